@@ -1,0 +1,242 @@
+"""ctypes binding of libgrainrecon_b200.so (the C ABI of include/grainrecon_b200.h).
+
+There is no fallback: if the shared library is missing or no sm_100 device is
+present, every call raises.  Arrays are passed as plain pointers; numpy arrays
+are host buffers, objects exposing ``data_ptr()`` (torch CUDA tensors) or
+``__cuda_array_interface__`` are device buffers.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+_PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_PKG, "libgrainrecon_b200.so")
+
+GRC_OK, GRC_EINVAL, GRC_ECAPACITY, GRC_ECUDA, GRC_ETIMEOUT, GRC_ENOMASK = 0, 1, 2, 3, 4, 5
+STATUS_NAMES = {0: "GRC_OK", 1: "GRC_EINVAL", 2: "GRC_ECAPACITY", 3: "GRC_ECUDA", 4: "GRC_ETIMEOUT",
+                5: "GRC_ENOMASK"}
+
+# Every symbol include/grainrecon_b200.h declares.
+EXPORTS = [
+    "grc_ctx_create", "grc_ctx_destroy", "grc_last_error", "grc_ctx_stream", "grc_sync", "grc_set_options",
+    "grc_upload_masks", "grc_upload_masks_device", "grc_set_geometry", "grc_forward_comp",
+    "grc_grow_indexed_region", "grc_forward_comp_compete", "grc_forward_comp_device", "grc_grow_device",
+    "grc_compete_device", "grc_last_stats", "grc_set_timing", "grc_mask_info", "grc_simulate_spots", "grc_edt",
+]
+
+
+class GrcError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{STATUS_NAMES.get(code, code)}: {msg}")
+        self.code = code
+
+
+class Stats(C.Structure):
+    _fields_ = [("trials", C.c_int64), ("refined", C.c_int64), ("kernel_launches", C.c_int64),
+                ("score_ms", C.c_double)]
+
+
+_lib = None
+
+
+def load(path: str | None = None):
+    """Load the library (building it first when sources are newer and nvcc exists)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    p = path or LIB_PATH
+    try:
+        from . import build as _b
+        if _b.needs_build():
+            _b.build()
+    except RuntimeError:
+        if not os.path.exists(p):
+            raise
+    if not os.path.exists(p):
+        raise OSError(f"{p} is missing: build it with `python -m grainrecon_b200.build`")
+    L = C.CDLL(p)
+    vp, i64, i, d, f = C.c_void_p, C.c_int64, C.c_int, C.c_double, C.c_void_p
+    sig = {
+        "grc_ctx_create": [C.POINTER(vp), i],
+        "grc_ctx_destroy": [vp],
+        "grc_last_error": [vp],
+        "grc_ctx_stream": [vp],
+        "grc_sync": [vp],
+        "grc_set_options": [vp, d, d, d],
+        "grc_upload_masks": [vp, f, i64, i64, i64],
+        "grc_upload_masks_device": [vp, f, i64, i64, i64],
+        "grc_set_geometry": [vp, f, f, f, f, f, f],
+        "grc_forward_comp": [vp, f, f, i64, f, f, f, f, f, f, f, f],
+        "grc_grow_indexed_region": [vp, f, i64, f, f, f, f, f, f, f, f, f, f],
+        "grc_forward_comp_compete": [vp, f, i64, f, i64, f, i64, f, f, f, f, f, f, f, f, f],
+        "grc_forward_comp_device": [vp, f, i64, f, i64, f],
+        "grc_grow_device": [vp, f, i64, f, f, f],
+        "grc_compete_device": [vp, f, i64, f, i64, f, i64, f, f, f],
+        "grc_last_stats": [vp, C.POINTER(Stats)],
+        "grc_set_timing": [vp, i],
+        "grc_mask_info": [vp, C.POINTER(i64), C.POINTER(i), C.POINTER(i64), C.POINTER(i64), C.POINTER(i64)],
+        "grc_simulate_spots": [vp, f, f, i64, f],
+        "grc_edt": [vp, f, i64, i64, i64, f],
+    }
+    for name, args in sig.items():
+        fn = getattr(L, name)
+        fn.argtypes = args
+        fn.restype = i
+    L.grc_last_error.restype = C.c_char_p
+    L.grc_ctx_stream.restype = vp
+    _lib = L
+    return L
+
+
+def _ptr(a):
+    """Raw address of a host numpy array, a torch tensor or a CUDA-array-interface object."""
+    if a is None:
+        return None
+    if isinstance(a, np.ndarray):
+        if not a.flags["C_CONTIGUOUS"]:
+            raise ValueError("array must be C-contiguous")
+        return a.ctypes.data
+    if hasattr(a, "data_ptr"):
+        if hasattr(a, "is_contiguous") and not a.is_contiguous():
+            raise ValueError("tensor must be contiguous")
+        return a.data_ptr()
+    if hasattr(a, "__cuda_array_interface__"):
+        return a.__cuda_array_interface__["data"][0]
+    if isinstance(a, int):
+        return a
+    raise TypeError(f"cannot take the address of {type(a)}")
+
+
+def f32(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.float32).reshape(-1)
+
+
+class Context:
+    """One device context of the scorer (owns the resident distance map and a stream)."""
+
+    def __init__(self, device: int = 0):
+        self.L = load()
+        h = C.c_void_p()
+        rc = self.L.grc_ctx_create(C.byref(h), device)
+        if rc != GRC_OK:
+            raise GrcError(rc, f"grc_ctx_create(device={device}) failed (no sm_100 GPU visible?)")
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.grc_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _check(self, rc: int):
+        if rc != GRC_OK:
+            raise GrcError(rc, self.L.grc_last_error(self.h).decode())
+
+    @property
+    def stream(self) -> int:
+        return int(self.L.grc_ctx_stream(self.h) or 0)
+
+    def sync(self):
+        self._check(self.L.grc_sync(self.h))
+
+    def set_options(self, dety0=float("nan"), detz0=float("nan"), hit_threshold=float("nan")):
+        self._check(self.L.grc_set_options(self.h, dety0, detz0, hit_threshold))
+
+    def upload_masks(self, proj_bin_bw, detzsize: int, detysize: int, nrot: int):
+        if isinstance(proj_bin_bw, np.ndarray):
+            proj_bin_bw = np.ascontiguousarray(proj_bin_bw, dtype=np.float32)
+        self._check(self.L.grc_upload_masks(self.h, _ptr(proj_bin_bw), detzsize, detysize, nrot))
+
+    def set_geometry(self, S, B, hkl, rot_angles, RotDet, param):
+        keep = [f32(x) for x in (S, B, hkl, rot_angles, RotDet, param)]
+        self._check(self.L.grc_set_geometry(self.h, *[_ptr(a) for a in keep]))
+
+    def forward_comp(self, pos, q, S, B, hkl, proj_bin_bw, rot_angles, RotDet, param, out=None):
+        """cuda_forward_comp: returns 4*n_q floats [Nr_simu Nr_intersect C dis_median]."""
+        q = f32(q)
+        n = q.size // 4
+        if out is None:
+            out = np.empty(4 * n, np.float32)
+        pb = None if proj_bin_bw is None else f32(proj_bin_bw)
+        keep = [f32(pos), q, f32(S), f32(B), f32(hkl), pb, f32(rot_angles), f32(RotDet), f32(param)]
+        p = [_ptr(a) for a in keep]
+        self._check(self.L.grc_forward_comp(self.h, p[0], p[1], n, p[2], p[3], p[4], p[5], p[6], p[7], p[8],
+                                            _ptr(out)))
+        return out
+
+    def grow_indexed_region(self, rows6, U, S, B, hkl, proj_bin_bw, rot_angles, RotDet, param, param1, out=None):
+        """cuda_grow_indexed_region: returns 7*m floats [x y z Nr_simu Nr_intersect dis_median flag]."""
+        rows6 = f32(rows6)
+        m = rows6.size // 6
+        if out is None:
+            out = np.empty(7 * m, np.float32)
+        pb = None if proj_bin_bw is None else f32(proj_bin_bw)
+        keep = [rows6, f32(U), f32(S), f32(B), f32(hkl), pb, f32(rot_angles), f32(RotDet), f32(param), f32(param1)]
+        p = [_ptr(a) for a in keep]
+        self._check(self.L.grc_grow_indexed_region(self.h, p[0], m, p[1], p[2], p[3], p[4], p[5], p[6], p[7], p[8],
+                                                   p[9], _ptr(out)))
+        return out
+
+    def forward_comp_compete(self, rows5, id_neigb, euler, S, B, hkl, proj_bin_bw, rot_angles, RotDet, param,
+                             param1, out=None):
+        """cuda_forward_comp_compete: returns 8*m floats [row phi1 PHI phi2 GrainId C Nr_intersect dis_median]."""
+        rows5, idn, eu = f32(rows5), f32(id_neigb), f32(euler)
+        m = rows5.size // 5
+        if out is None:
+            out = np.empty(8 * m, np.float32)
+        pb = None if proj_bin_bw is None else f32(proj_bin_bw)
+        keep = [rows5, idn, eu, f32(S), f32(B), f32(hkl), pb, f32(rot_angles), f32(RotDet), f32(param), f32(param1)]
+        p = [_ptr(a) for a in keep]
+        self._check(self.L.grc_forward_comp_compete(self.h, p[0], m, p[1], idn.size, p[2], eu.size // 3, p[3], p[4],
+                                                    p[5], p[6], p[7], p[8], p[9], p[10], _ptr(out)))
+        return out
+
+    # device-resident entries (torch CUDA tensors / device pointers)
+    def forward_comp_device(self, d_pos, n_vox: int, d_q, n_q: int, d_out):
+        self._check(self.L.grc_forward_comp_device(self.h, _ptr(d_pos), n_vox, _ptr(d_q), n_q, _ptr(d_out)))
+
+    def grow_device(self, d_rows6, m: int, U, param1, d_out):
+        u, p1 = f32(U), f32(param1)
+        self._check(self.L.grc_grow_device(self.h, _ptr(d_rows6), m, _ptr(u), _ptr(p1), _ptr(d_out)))
+
+    def compete_device(self, d_rows5, m: int, d_id, n_neigb: int, d_euler, n_grain: int, param1, d_out,
+                       d_trial_out=None):
+        p1 = f32(param1)
+        self._check(self.L.grc_compete_device(self.h, _ptr(d_rows5), m, _ptr(d_id), n_neigb, _ptr(d_euler),
+                                              n_grain, _ptr(p1), _ptr(d_out), _ptr(d_trial_out)))
+
+    def simulate_spots(self, d_pos, d_U, n: int, d_mask):
+        self._check(self.L.grc_simulate_spots(self.h, _ptr(d_pos), _ptr(d_U), n, _ptr(d_mask)))
+
+    def edt(self, d_mask, detzsize: int, detysize: int, nrot: int, d_map):
+        self._check(self.L.grc_edt(self.h, _ptr(d_mask), detzsize, detysize, nrot, _ptr(d_map)))
+
+    def set_timing(self, enable: bool):
+        self._check(self.L.grc_set_timing(self.h, int(bool(enable))))
+
+    def last_stats(self) -> dict:
+        s = Stats()
+        self._check(self.L.grc_last_stats(self.h, C.byref(s)))
+        return {"trials": s.trials, "refined": s.refined, "kernel_launches": s.kernel_launches,
+                "score_ms": s.score_ms}
+
+    def mask_info(self) -> dict:
+        nd, nz, ny, nr = C.c_int64(), C.c_int64(), C.c_int64(), C.c_int64()
+        bits = C.c_int()
+        self._check(self.L.grc_mask_info(self.h, C.byref(nd), C.byref(bits), C.byref(nz), C.byref(ny), C.byref(nr)))
+        return {"n_distinct": nd.value, "code_bits": bits.value, "detzsize": nz.value, "detysize": ny.value,
+                "nrot": nr.value}

@@ -1,0 +1,689 @@
+// grc_capi.cu -- the C ABI (include/grainrecon_b200.h): context, resident distance
+// map, geometry cache and the drop-in entries replacing GrainRecon's CUDA MEX calls.
+#include <cub/cub.cuh>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "grainrecon_b200.h"
+#include "grc_internal.h"
+
+namespace {
+
+struct DevBuf {
+    void *p = nullptr;
+    size_t cap = 0;
+};
+
+// Trials per work item of a seeding scan: one omega table serves this many orientations.
+constexpr int kSeedChunk = 16;
+
+}  // namespace
+
+struct grc_ctx {
+    int device = 0;
+    int num_sms = 0;
+    cudaStream_t stream = nullptr;
+    std::mutex mu;
+    std::string err;
+    double opt_dety0 = NAN, opt_detz0 = NAN, opt_thr = 0.5;
+    bool has_geo = false;
+    std::vector<float> geo_key;
+    grc::Geo geo{};
+    bool has_masks = false;
+    grc::MapCodes mc{};
+    int64_t mz = 0, my = 0, mrot = 0;
+    std::vector<float> h_vals;
+    DevBuf rot_cs, hkl, pos, U, res, in1, in2, in3, out, items, torient, counts, offsets, tmp, counter, p1, bad;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    bool timing = false;
+    bool timed_last = false;
+    grc_stats stats{};
+};
+
+namespace {
+
+int fail(grc_ctx *c, int code, const char *fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    if (c) c->err = buf;
+    return code;
+}
+
+#define CU(x)                                                                                      \
+    do {                                                                                           \
+        cudaError_t e_ = (x);                                                                      \
+        if (e_ != cudaSuccess) return fail(ctx, GRC_ECUDA, "%s: %s", #x, cudaGetErrorString(e_)); \
+    } while (0)
+
+#define TRY(x)                 \
+    do {                       \
+        int r_ = (x);          \
+        if (r_ != GRC_OK) return r_; \
+    } while (0)
+
+int ensure(grc_ctx *ctx, DevBuf &b, size_t bytes) {
+    if (bytes == 0) bytes = 16;
+    if (b.cap >= bytes) return GRC_OK;
+    const size_t want = std::max(bytes, b.cap + b.cap / 2);
+    CU(cudaStreamSynchronize(ctx->stream));
+    if (b.p) CU(cudaFree(b.p));
+    b.p = nullptr;
+    b.cap = 0;
+    cudaError_t e = cudaMalloc(&b.p, want);
+    if (e != cudaSuccess) return fail(ctx, GRC_ECUDA, "cudaMalloc(%zu bytes): %s", want, cudaGetErrorString(e));
+    b.cap = want;
+    return GRC_OK;
+}
+
+bool is_device_ptr(const void *p) {
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+bool is_int(float v) { return std::isfinite(v) && std::floor(v) == v; }
+
+void refresh_hit(grc_ctx *ctx) {
+    if (!ctx->has_masks) return;
+    const double thr = ctx->opt_thr;
+    size_t n = 0;
+    while (n < ctx->h_vals.size() && (double)ctx->h_vals[n] <= thr) ++n;
+    ctx->geo.n_hit = (uint32_t)n;
+    ctx->geo.n_vals = (uint32_t)std::max<int64_t>(1, ctx->mc.n_distinct);
+    int bits = 0;
+    while (bits < 32 && (int64_t(1) << bits) < ctx->mc.n_distinct) ++bits;
+    ctx->geo.code_bits = bits;
+}
+
+void apply_options(grc_ctx *ctx) {
+    grc::Geo &g = ctx->geo;
+    g.dety0 = std::isnan(ctx->opt_dety0) ? g.detysize / 2.0 + 0.5 : ctx->opt_dety0;
+    g.detz0 = std::isnan(ctx->opt_detz0) ? g.detzsize / 2.0 + 0.5 : ctx->opt_detz0;
+    refresh_hit(ctx);
+}
+
+int set_geometry(grc_ctx *ctx, const float *S, const float *B, const float *hkl, const float *rot,
+                 const float *R, const float *param) {
+    if (!S || !B || !hkl || !rot || !R || !param) return fail(ctx, GRC_EINVAL, "geometry: NULL argument");
+    for (int i = 0; i < 20; ++i)
+        if (!std::isfinite(param[i])) return fail(ctx, GRC_EINVAL, "param(%d) is not finite", i + 1);
+    if (!is_int(param[0]) || param[0] < 1) return fail(ctx, GRC_EINVAL, "param(1)=nr_hkl must be a positive integer");
+    if (!is_int(param[1]) || param[1] < 1) return fail(ctx, GRC_EINVAL, "param(2)=nr_rot must be a positive integer");
+    if (param[0] > GRC_MAX_NHKL)
+        return fail(ctx, GRC_ECAPACITY, "nr_hkl=%g exceeds GRC_MAX_NHKL=%d", param[0], GRC_MAX_NHKL);
+    if (param[1] > GRC_MAX_NROT)
+        return fail(ctx, GRC_ECAPACITY, "nr_rot=%g exceeds GRC_MAX_NROT=%d", param[1], GRC_MAX_NROT);
+    if (!is_int(param[10]) || !is_int(param[11]) || param[10] < 1 || param[11] < 1)
+        return fail(ctx, GRC_EINVAL, "detysize/detzsize must be positive integers");
+    if (!(param[8] > 0) || !(param[9] > 0)) return fail(ctx, GRC_EINVAL, "pixel sizes must be positive");
+    const int nhkl = (int)param[0], nrot = (int)param[1];
+    std::vector<float> key;
+    key.reserve(47 + 3 * nhkl + nrot);
+    key.insert(key.end(), S, S + 9);
+    key.insert(key.end(), B, B + 9);
+    key.insert(key.end(), R, R + 9);
+    key.insert(key.end(), param, param + 20);
+    key.insert(key.end(), hkl, hkl + 3 * nhkl);
+    key.insert(key.end(), rot, rot + nrot);
+    for (float v : key)
+        if (!std::isfinite(v)) return fail(ctx, GRC_EINVAL, "geometry array holds a non-finite value");
+    if (ctx->has_geo && key.size() == ctx->geo_key.size() &&
+        std::memcmp(key.data(), ctx->geo_key.data(), key.size() * sizeof(float)) == 0) {
+        apply_options(ctx);
+        return GRC_OK;
+    }
+    grc::Geo g{};
+    g.nhkl = nhkl;
+    g.nrot = nrot;
+    g.lss = param[2]; g.lsd = param[3]; g.p0y = param[4]; g.p0z = param[5];
+    g.dety00 = param[6]; g.detz00 = param[7]; g.pxy = param[8]; g.pxz = param[9];
+    g.detysize = (int)param[10]; g.detzsize = (int)param[11];
+    g.bsy0 = param[12]; g.bsy1 = param[13]; g.bsz0 = param[14]; g.bsz1 = param[15];
+    g.lmin = param[17]; g.lmax = param[18]; g.rao = param[19];
+    const double pi = 3.14159265358979323846;
+    const double bmax = (90.0 + (double)param[16] * 4.0) / 180.0 * pi;  // forward_comp.m:61
+    g.cbmax = bmax <= pi ? std::cos(bmax) : -2.0;
+    for (int i = 0; i < 9; ++i) {
+        g.S[i] = S[i];
+        g.B[i] = B[i];
+        g.R[i] = R[i];
+    }
+    g.plane = (int64_t)g.detysize * g.detzsize;
+    std::vector<double2> cs(nrot);
+    for (int i = 0; i < nrot; ++i) {
+        const double w = (double)rot[i] * pi / 180.0;  // forward_comp.m:19
+        cs[i] = make_double2(std::cos(w), std::sin(w));
+    }
+    std::vector<double> h(3 * nhkl);
+    for (int i = 0; i < 3 * nhkl; ++i) h[i] = hkl[i];
+    TRY(ensure(ctx, ctx->rot_cs, sizeof(double2) * nrot));
+    TRY(ensure(ctx, ctx->hkl, sizeof(double) * 3 * nhkl));
+    CU(cudaMemcpyAsync(ctx->rot_cs.p, cs.data(), sizeof(double2) * nrot, cudaMemcpyHostToDevice, ctx->stream));
+    CU(cudaMemcpyAsync(ctx->hkl.p, h.data(), sizeof(double) * 3 * nhkl, cudaMemcpyHostToDevice, ctx->stream));
+    CU(cudaStreamSynchronize(ctx->stream));
+    ctx->geo = g;
+    ctx->geo_key.swap(key);
+    ctx->has_geo = true;
+    apply_options(ctx);
+    return GRC_OK;
+}
+
+int upload_device_map(grc_ctx *ctx, const float *d_map, int64_t dz, int64_t dy, int64_t nrot) {
+    const int64_t n = dz * dy * nrot;
+    grc::MapCodes mc{};
+    int bad = 0;
+    cudaError_t e = grc::encode_map(d_map, n, ctx->stream, &mc, &bad);
+    if (e != cudaSuccess) return fail(ctx, GRC_ECUDA, "distance-map coding: %s", cudaGetErrorString(e));
+    if (bad) return fail(ctx, GRC_EINVAL, "distance map holds NaN values");
+    std::vector<float> hv((size_t)mc.n_distinct);
+    if (mc.n_distinct > 0) {
+        e = cudaMemcpy(hv.data(), mc.vals, sizeof(float) * mc.n_distinct, cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) {
+            cudaFree(mc.codes);
+            cudaFree(mc.vals);
+            return fail(ctx, GRC_ECUDA, "value table copy: %s", cudaGetErrorString(e));
+        }
+    }
+    if (ctx->has_masks) {
+        cudaFree(ctx->mc.codes);
+        cudaFree(ctx->mc.vals);
+    }
+    ctx->mc = mc;
+    ctx->h_vals.swap(hv);
+    ctx->mz = dz;
+    ctx->my = dy;
+    ctx->mrot = nrot;
+    ctx->has_masks = true;
+    refresh_hit(ctx);
+    return GRC_OK;
+}
+
+int upload_host_map(grc_ctx *ctx, const float *map, int64_t dz, int64_t dy, int64_t nrot) {
+    if (!map) return fail(ctx, GRC_EINVAL, "proj_bin_bw is NULL");
+    if (dz < 1 || dy < 1 || nrot < 1) return fail(ctx, GRC_EINVAL, "distance-map dimensions must be positive");
+    const int64_t n = dz * dy * nrot;
+    float *d_map = nullptr;
+    cudaError_t e = cudaMalloc(&d_map, sizeof(float) * n);
+    if (e != cudaSuccess) return fail(ctx, GRC_ECUDA, "cudaMalloc(map): %s", cudaGetErrorString(e));
+    // chunked copy keeps the pageable staging small
+    const int64_t chunk = int64_t(1) << 26;
+    for (int64_t s = 0; s < n && e == cudaSuccess; s += chunk) {
+        const int64_t c = std::min(chunk, n - s);
+        e = cudaMemcpyAsync(d_map + s, map + s, sizeof(float) * c, cudaMemcpyHostToDevice, ctx->stream);
+    }
+    if (e != cudaSuccess) {
+        cudaFree(d_map);
+        return fail(ctx, GRC_ECUDA, "map upload: %s", cudaGetErrorString(e));
+    }
+    int r = upload_device_map(ctx, d_map, dz, dy, nrot);
+    cudaStreamSynchronize(ctx->stream);
+    cudaFree(d_map);
+    return r;
+}
+
+int check_ready(grc_ctx *ctx) {
+    if (!ctx->has_geo) return fail(ctx, GRC_EINVAL, "no geometry set");
+    if (!ctx->has_masks) return fail(ctx, GRC_ENOMASK, "no distance map resident and none passed");
+    const grc::Geo &g = ctx->geo;
+    if (ctx->mz != g.detzsize || ctx->my != g.detysize || ctx->mrot != g.nrot)
+        return fail(ctx, GRC_EINVAL,
+                    "distance map is %lld x %lld x %lld (detz x dety x nrot) but param says %d x %d x %d",
+                    (long long)ctx->mz, (long long)ctx->my, (long long)ctx->mrot, g.detzsize, g.detysize, g.nrot);
+    return GRC_OK;
+}
+
+grc::ScoreBufs bufs(grc_ctx *ctx) {
+    grc::ScoreBufs b{};
+    b.rot_cs = (const double2 *)ctx->rot_cs.p;
+    b.hkl = (const double *)ctx->hkl.p;
+    b.vpos = (const double *)ctx->pos.p;
+    b.U = (const double *)ctx->U.p;
+    b.codes = ctx->mc.codes;
+    b.vals = ctx->mc.vals;
+    b.res = (grc::TrialRes *)ctx->res.p;
+    b.work_counter = (int *)ctx->counter.p;
+    return b;
+}
+
+int run_score(grc_ctx *ctx, const grc::Work &w, int64_t n_trials) {
+    TRY(ensure(ctx, ctx->counter, 8 * sizeof(int)));
+    int launches = 0;
+    cudaError_t e = grc::launch_score(ctx->geo, bufs(ctx), w, ctx->num_sms, ctx->stream,
+                                      ctx->timing ? ctx->ev0 : nullptr, ctx->timing ? ctx->ev1 : nullptr,
+                                      &launches);
+    if (e != cudaSuccess) return fail(ctx, GRC_ECUDA, "scorer launch: %s", cudaGetErrorString(e));
+    ctx->timed_last = ctx->timing;
+    ctx->stats.trials = n_trials;
+    ctx->stats.kernel_launches += launches;
+    return GRC_OK;
+}
+
+// Seeding batch on device buffers: n_vox voxels x n_q orientations.
+int forward_device(grc_ctx *ctx, const float *d_pos, int64_t n_vox, const float *d_q, int64_t n_q, float *d_out) {
+    TRY(check_ready(ctx));
+    ctx->stats = grc_stats{};
+    if (n_vox <= 0 || n_q <= 0) return GRC_OK;
+    TRY(ensure(ctx, ctx->U, sizeof(double) * 9 * n_q));
+    TRY(ensure(ctx, ctx->pos, sizeof(double) * 3 * n_vox));
+    TRY(ensure(ctx, ctx->res, sizeof(grc::TrialRes) * n_vox * n_q));
+    CU(grc::launch_quat_to_u(d_q, n_q, (double *)ctx->U.p, ctx->stream));
+    CU(grc::launch_pos_f3(d_pos, n_vox, (double *)ctx->pos.p, ctx->stream));
+    grc::Work w{};
+    w.n_or = n_q;
+    w.chunk = kSeedChunk;
+    w.chunks_per_voxel = (n_q + kSeedChunk - 1) / kSeedChunk;
+    w.n_items = n_vox * w.chunks_per_voxel;
+    TRY(run_score(ctx, w, n_vox * n_q));
+    CU(grc::launch_epi_forward((const grc::TrialRes *)ctx->res.p, n_vox * n_q, d_out, ctx->stream));
+    ctx->stats.kernel_launches += 3;
+    return GRC_OK;
+}
+
+int grow_device(grc_ctx *ctx, const float *d_rows6, int64_t m, const float *U9, const float *param1,
+                float *d_out) {
+    TRY(check_ready(ctx));
+    ctx->stats = grc_stats{};
+    if (!U9 || !param1) return fail(ctx, GRC_EINVAL, "grow: NULL U or param1");
+    if (m <= 0) return GRC_OK;
+    double p1[14];
+    for (int i = 0; i < 14; ++i) {
+        if (!std::isfinite(param1[i])) return fail(ctx, GRC_EINVAL, "param1(%d) is not finite", i + 1);
+        p1[i] = param1[i];
+    }
+    TRY(ensure(ctx, ctx->p1, sizeof(p1)));
+    TRY(ensure(ctx, ctx->in3, sizeof(float) * 9));
+    TRY(ensure(ctx, ctx->U, sizeof(double) * 9));
+    TRY(ensure(ctx, ctx->pos, sizeof(double) * 3 * m));
+    TRY(ensure(ctx, ctx->res, sizeof(grc::TrialRes) * m));
+    CU(cudaMemcpyAsync(ctx->p1.p, p1, sizeof(p1), cudaMemcpyHostToDevice, ctx->stream));
+    CU(cudaMemcpyAsync(ctx->in3.p, U9, sizeof(float) * 9, cudaMemcpyHostToDevice, ctx->stream));
+    CU(grc::launch_f9_to_u((const float *)ctx->in3.p, 1, (double *)ctx->U.p, ctx->stream));
+    CU(grc::launch_pos_rows(d_rows6, 6, m, (const double *)ctx->p1.p, (double *)ctx->pos.p, ctx->stream));
+    grc::Work w{};
+    w.n_or = 1;
+    w.chunk = 1;
+    w.chunks_per_voxel = 1;
+    w.n_items = m;
+    TRY(run_score(ctx, w, m));
+    CU(grc::launch_epi_grow((const grc::TrialRes *)ctx->res.p, d_rows6, m, (const double *)ctx->p1.p, d_out,
+                            ctx->stream));
+    ctx->stats.kernel_launches += 3;
+    return GRC_OK;
+}
+
+int compete_device(grc_ctx *ctx, const float *d_rows5, int64_t m, const float *d_id, int64_t n_neigb,
+                   const float *d_euler, int64_t n_grain, const float *param1, float *d_out, float *d_trial_out) {
+    TRY(check_ready(ctx));
+    ctx->stats = grc_stats{};
+    if (!param1) return fail(ctx, GRC_EINVAL, "compete: NULL param1");
+    if (m <= 0) return GRC_OK;
+    if (n_grain < 1 || n_grain > (int64_t)INT32_MAX) return fail(ctx, GRC_EINVAL, "compete: bad grain count");
+    double p1[14] = {0};
+    for (int i = 0; i < 11; ++i) {
+        if (!std::isfinite(param1[i])) return fail(ctx, GRC_EINVAL, "param1(%d) is not finite", i + 1);
+        p1[i] = param1[i];
+    }
+    TRY(ensure(ctx, ctx->p1, sizeof(p1)));
+    TRY(ensure(ctx, ctx->U, sizeof(double) * 9 * n_grain));
+    TRY(ensure(ctx, ctx->pos, sizeof(double) * 3 * m));
+    TRY(ensure(ctx, ctx->counts, sizeof(int64_t) * m));
+    TRY(ensure(ctx, ctx->offsets, sizeof(int64_t) * m));
+    TRY(ensure(ctx, ctx->items, sizeof(longlong4) * m));
+    TRY(ensure(ctx, ctx->bad, sizeof(int)));
+    CU(cudaMemcpyAsync(ctx->p1.p, p1, sizeof(p1), cudaMemcpyHostToDevice, ctx->stream));
+    CU(cudaMemsetAsync(ctx->bad.p, 0, sizeof(int), ctx->stream));
+    CU(grc::launch_euler_to_u(d_euler, n_grain, (double *)ctx->U.p, ctx->stream));
+    CU(grc::launch_pos_rows(d_rows5, 5, m, (const double *)ctx->p1.p, (double *)ctx->pos.p, ctx->stream));
+    CU(grc::launch_csr_counts(d_rows5, m, (int64_t *)ctx->counts.p, ctx->stream));
+    size_t tmp_bytes = 0;
+    CU(cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, (int64_t *)ctx->counts.p, (int64_t *)ctx->offsets.p, m,
+                                     ctx->stream));
+    TRY(ensure(ctx, ctx->tmp, tmp_bytes));
+    CU(cub::DeviceScan::ExclusiveSum(ctx->tmp.p, tmp_bytes, (int64_t *)ctx->counts.p, (int64_t *)ctx->offsets.p,
+                                     m, ctx->stream));
+    int64_t last_off = 0, last_cnt = 0;
+    CU(cudaMemcpyAsync(&last_off, (int64_t *)ctx->offsets.p + (m - 1), 8, cudaMemcpyDeviceToHost, ctx->stream));
+    CU(cudaMemcpyAsync(&last_cnt, (int64_t *)ctx->counts.p + (m - 1), 8, cudaMemcpyDeviceToHost, ctx->stream));
+    CU(cudaStreamSynchronize(ctx->stream));
+    const int64_t T = last_off + last_cnt;
+    TRY(ensure(ctx, ctx->torient, sizeof(int32_t) * (T > 0 ? T : 1)));
+    TRY(ensure(ctx, ctx->res, sizeof(grc::TrialRes) * (T > 0 ? T : 1)));
+    CU(grc::launch_csr_fill(d_rows5, m, (const int64_t *)ctx->offsets.p, d_id, n_neigb, n_grain,
+                            (longlong4 *)ctx->items.p, (int32_t *)ctx->torient.p, (int *)ctx->bad.p, ctx->stream));
+    int hbad = 0;
+    CU(cudaMemcpyAsync(&hbad, ctx->bad.p, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    CU(cudaStreamSynchronize(ctx->stream));
+    if (hbad & 1) return fail(ctx, GRC_EINVAL, "compete: a [first,last] range lies outside id_neigb_all");
+    if (hbad & 2) return fail(ctx, GRC_EINVAL, "compete: a grain id lies outside the Euler table");
+    if (T > 0) {
+        grc::Work w{};
+        w.items = (const longlong4 *)ctx->items.p;
+        w.trial_orient = (const int32_t *)ctx->torient.p;
+        w.n_items = m;
+        TRY(run_score(ctx, w, T));
+    }
+    CU(grc::launch_epi_compete((const grc::TrialRes *)ctx->res.p, (const longlong4 *)ctx->items.p,
+                               (const int32_t *)ctx->torient.p, m, d_euler, d_out, d_trial_out, ctx->stream));
+    ctx->stats.kernel_launches += 5;
+    return GRC_OK;
+}
+
+// Copy a host array into a workspace buffer (or use it directly when already on the device).
+int stage_in(grc_ctx *ctx, DevBuf &b, const float *src, int64_t n, const float **dst) {
+    if (n <= 0) {
+        *dst = nullptr;
+        TRY(ensure(ctx, b, 16));
+        *dst = (const float *)b.p;
+        return GRC_OK;
+    }
+    if (!src) return fail(ctx, GRC_EINVAL, "NULL input array");
+    if (is_device_ptr(src)) {
+        *dst = src;
+        return GRC_OK;
+    }
+    TRY(ensure(ctx, b, sizeof(float) * n));
+    CU(cudaMemcpyAsync(b.p, src, sizeof(float) * n, cudaMemcpyHostToDevice, ctx->stream));
+    *dst = (const float *)b.p;
+    return GRC_OK;
+}
+
+struct Lock {
+    grc_ctx *c;
+    std::lock_guard<std::mutex> g;
+    explicit Lock(grc_ctx *ctx) : c(ctx), g(ctx->mu) { cudaSetDevice(ctx->device); }
+};
+
+}  // namespace
+
+extern "C" {
+
+int grc_ctx_create(grc_ctx **out, int device) {
+    if (!out) return GRC_EINVAL;
+    *out = nullptr;
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+        cudaGetLastError();
+        return GRC_ECUDA;
+    }
+    if (device < 0 || device >= n) return GRC_EINVAL;
+    grc_ctx *ctx = new grc_ctx();
+    ctx->device = device;
+    cudaSetDevice(device);
+    cudaDeviceProp p;
+    if (cudaGetDeviceProperties(&p, device) != cudaSuccess) {
+        delete ctx;
+        return GRC_ECUDA;
+    }
+    if (p.major < 10) {
+        delete ctx;
+        return GRC_ECUDA;  // built for sm_100a only
+    }
+    ctx->num_sms = p.multiProcessorCount;
+    if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreate(&ctx->ev0) != cudaSuccess || cudaEventCreate(&ctx->ev1) != cudaSuccess) {
+        delete ctx;
+        return GRC_ECUDA;
+    }
+    *out = ctx;
+    return GRC_OK;
+}
+
+int grc_ctx_destroy(grc_ctx *ctx) {
+    if (!ctx) return GRC_EINVAL;
+    {
+        Lock l(ctx);
+        cudaStreamSynchronize(ctx->stream);
+        DevBuf *all[] = {&ctx->rot_cs, &ctx->hkl, &ctx->pos, &ctx->U, &ctx->res, &ctx->in1, &ctx->in2,
+                         &ctx->in3, &ctx->out, &ctx->items, &ctx->torient, &ctx->counts, &ctx->offsets,
+                         &ctx->tmp, &ctx->counter, &ctx->p1, &ctx->bad};
+        for (DevBuf *b : all) cudaFree(b->p);
+        if (ctx->has_masks) {
+            cudaFree(ctx->mc.codes);
+            cudaFree(ctx->mc.vals);
+        }
+        cudaEventDestroy(ctx->ev0);
+        cudaEventDestroy(ctx->ev1);
+        cudaStreamDestroy(ctx->stream);
+    }
+    delete ctx;
+    return GRC_OK;
+}
+
+const char *grc_last_error(const grc_ctx *ctx) { return ctx ? ctx->err.c_str() : "NULL context"; }
+
+void *grc_ctx_stream(grc_ctx *ctx) { return ctx ? (void *)ctx->stream : nullptr; }
+
+int grc_sync(grc_ctx *ctx) {
+    if (!ctx) return GRC_EINVAL;
+    Lock l(ctx);
+    CU(cudaStreamSynchronize(ctx->stream));
+    return GRC_OK;
+}
+
+int grc_set_options(grc_ctx *ctx, double dety0, double detz0, double thr) {
+    if (!ctx) return GRC_EINVAL;
+    Lock l(ctx);
+    ctx->opt_dety0 = dety0;
+    ctx->opt_detz0 = detz0;
+    ctx->opt_thr = std::isnan(thr) ? 0.5 : thr;
+    if (ctx->has_geo) apply_options(ctx);
+    return GRC_OK;
+}
+
+int grc_upload_masks(grc_ctx *ctx, const float *map, int64_t dz, int64_t dy, int64_t nrot) {
+    if (!ctx) return GRC_EINVAL;
+    Lock l(ctx);
+    if (map && is_device_ptr(map)) return upload_device_map(ctx, map, dz, dy, nrot);
+    return upload_host_map(ctx, map, dz, dy, nrot);
+}
+
+int grc_upload_masks_device(grc_ctx *ctx, const float *d_map, int64_t dz, int64_t dy, int64_t nrot) {
+    if (!ctx) return GRC_EINVAL;
+    Lock l(ctx);
+    if (!d_map) return fail(ctx, GRC_EINVAL, "proj_bin_bw is NULL");
+    if (dz < 1 || dy < 1 || nrot < 1) return fail(ctx, GRC_EINVAL, "distance-map dimensions must be positive");
+    return upload_device_map(ctx, d_map, dz, dy, nrot);
+}
+
+int grc_set_geometry(grc_ctx *ctx, const float *S, const float *B, const float *hkl, const float *rot,
+                     const float *R, const float *param) {
+    if (!ctx) return GRC_EINVAL;
+    Lock l(ctx);
+    return set_geometry(ctx, S, B, hkl, rot, R, param);
+}
+
+int grc_forward_comp(grc_ctx *ctx, const float *pos, const float *q, int64_t n_q, const float *S, const float *B,
+                     const float *hkl, const float *map, const float *rot, const float *R, const float *param,
+                     float *out) {
+    if (!ctx) return GRC_EINVAL;
+    Lock l(ctx);
+    if (!pos || !out || (n_q > 0 && !q)) return fail(ctx, GRC_EINVAL, "forward_comp: NULL argument");
+    if (n_q < 0) return fail(ctx, GRC_EINVAL, "forward_comp: negative orientation count");
+    TRY(set_geometry(ctx, S, B, hkl, rot, R, param));
+    if (map) TRY(upload_host_map(ctx, map, ctx->geo.detzsize, ctx->geo.detysize, ctx->geo.nrot));
+    TRY(check_ready(ctx));
+    if (n_q == 0) return GRC_OK;
+    const float *d_pos = nullptr, *d_q = nullptr;
+    TRY(stage_in(ctx, ctx->in1, pos, 3, &d_pos));
+    TRY(stage_in(ctx, ctx->in2, q, 4 * n_q, &d_q));
+    const bool dev_out = is_device_ptr(out);
+    float *d_out = out;
+    if (!dev_out) {
+        TRY(ensure(ctx, ctx->out, sizeof(float) * 4 * n_q));
+        d_out = (float *)ctx->out.p;
+    }
+    TRY(forward_device(ctx, d_pos, 1, d_q, n_q, d_out));
+    if (!dev_out) CU(cudaMemcpyAsync(out, d_out, sizeof(float) * 4 * n_q, cudaMemcpyDeviceToHost, ctx->stream));
+    CU(cudaStreamSynchronize(ctx->stream));
+    CU(cudaGetLastError());
+    return GRC_OK;
+}
+
+int grc_grow_indexed_region(grc_ctx *ctx, const float *rows6, int64_t m, const float *U, const float *S,
+                            const float *B, const float *hkl, const float *map, const float *rot, const float *R,
+                            const float *param, const float *param1, float *out) {
+    if (!ctx) return GRC_EINVAL;
+    Lock l(ctx);
+    if (!U || !param1 || !out || (m > 0 && !rows6)) return fail(ctx, GRC_EINVAL, "grow: NULL argument");
+    if (m < 0) return fail(ctx, GRC_EINVAL, "grow: negative row count");
+    TRY(set_geometry(ctx, S, B, hkl, rot, R, param));
+    if (map) TRY(upload_host_map(ctx, map, ctx->geo.detzsize, ctx->geo.detysize, ctx->geo.nrot));
+    TRY(check_ready(ctx));
+    if (m == 0) return GRC_OK;
+    const float *d_rows = nullptr;
+    TRY(stage_in(ctx, ctx->in1, rows6, 6 * m, &d_rows));
+    const bool dev_out = is_device_ptr(out);
+    float *d_out = out;
+    if (!dev_out) {
+        TRY(ensure(ctx, ctx->out, sizeof(float) * 7 * m));
+        d_out = (float *)ctx->out.p;
+    }
+    TRY(grow_device(ctx, d_rows, m, U, param1, d_out));
+    if (!dev_out) CU(cudaMemcpyAsync(out, d_out, sizeof(float) * 7 * m, cudaMemcpyDeviceToHost, ctx->stream));
+    CU(cudaStreamSynchronize(ctx->stream));
+    CU(cudaGetLastError());
+    return GRC_OK;
+}
+
+int grc_forward_comp_compete(grc_ctx *ctx, const float *rows5, int64_t m, const float *id_neigb, int64_t n_neigb,
+                             const float *euler, int64_t n_grain, const float *S, const float *B, const float *hkl,
+                             const float *map, const float *rot, const float *R, const float *param,
+                             const float *param1, float *out) {
+    if (!ctx) return GRC_EINVAL;
+    Lock l(ctx);
+    if (!param1 || !out || (m > 0 && (!rows5 || !euler))) return fail(ctx, GRC_EINVAL, "compete: NULL argument");
+    if (m < 0 || n_neigb < 0 || n_grain < 0) return fail(ctx, GRC_EINVAL, "compete: negative size");
+    TRY(set_geometry(ctx, S, B, hkl, rot, R, param));
+    if (map) TRY(upload_host_map(ctx, map, ctx->geo.detzsize, ctx->geo.detysize, ctx->geo.nrot));
+    TRY(check_ready(ctx));
+    if (m == 0) return GRC_OK;
+    const float *d_rows = nullptr, *d_id = nullptr, *d_eu = nullptr;
+    TRY(stage_in(ctx, ctx->in1, rows5, 5 * m, &d_rows));
+    TRY(stage_in(ctx, ctx->in2, id_neigb, n_neigb, &d_id));
+    TRY(stage_in(ctx, ctx->in3, euler, 3 * n_grain, &d_eu));
+    const bool dev_out = is_device_ptr(out);
+    float *d_out = out;
+    if (!dev_out) {
+        TRY(ensure(ctx, ctx->out, sizeof(float) * 8 * m));
+        d_out = (float *)ctx->out.p;
+    }
+    TRY(compete_device(ctx, d_rows, m, d_id, n_neigb, d_eu, n_grain, param1, d_out, nullptr));
+    if (!dev_out) CU(cudaMemcpyAsync(out, d_out, sizeof(float) * 8 * m, cudaMemcpyDeviceToHost, ctx->stream));
+    CU(cudaStreamSynchronize(ctx->stream));
+    CU(cudaGetLastError());
+    return GRC_OK;
+}
+
+int grc_forward_comp_device(grc_ctx *ctx, const float *d_pos, int64_t n_vox, const float *d_q, int64_t n_q,
+                            float *d_out) {
+    if (!ctx) return GRC_EINVAL;
+    Lock l(ctx);
+    if (n_vox < 0 || n_q < 0) return fail(ctx, GRC_EINVAL, "negative size");
+    if (n_vox > 0 && n_q > 0 && (!d_pos || !d_q || !d_out)) return fail(ctx, GRC_EINVAL, "NULL device buffer");
+    return forward_device(ctx, d_pos, n_vox, d_q, n_q, d_out);
+}
+
+int grc_grow_device(grc_ctx *ctx, const float *d_rows6, int64_t m, const float *U, const float *param1,
+                    float *d_out) {
+    if (!ctx) return GRC_EINVAL;
+    Lock l(ctx);
+    if (m < 0) return fail(ctx, GRC_EINVAL, "negative size");
+    if (m > 0 && (!d_rows6 || !d_out)) return fail(ctx, GRC_EINVAL, "NULL device buffer");
+    return grow_device(ctx, d_rows6, m, U, param1, d_out);
+}
+
+int grc_compete_device(grc_ctx *ctx, const float *d_rows5, int64_t m, const float *d_id, int64_t n_neigb,
+                       const float *d_euler, int64_t n_grain, const float *param1, float *d_out,
+                       float *d_trial_out) {
+    if (!ctx) return GRC_EINVAL;
+    Lock l(ctx);
+    if (m < 0 || n_neigb < 0 || n_grain < 0) return fail(ctx, GRC_EINVAL, "negative size");
+    if (m > 0 && (!d_rows5 || !d_out || !d_euler)) return fail(ctx, GRC_EINVAL, "NULL device buffer");
+    return compete_device(ctx, d_rows5, m, d_id, n_neigb, d_euler, n_grain, param1, d_out, d_trial_out);
+}
+
+int grc_last_stats(grc_ctx *ctx, grc_stats *out) {
+    if (!ctx || !out) return GRC_EINVAL;
+    Lock l(ctx);
+    CU(cudaStreamSynchronize(ctx->stream));
+    if (ctx->counter.p) {
+        int c[8];
+        CU(cudaMemcpy(c, ctx->counter.p, sizeof c, cudaMemcpyDeviceToHost));
+        ctx->stats.refined = c[4];
+    }
+    ctx->stats.score_ms = 0;
+    if (ctx->timed_last) {
+        float ms = 0;
+        if (cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1) == cudaSuccess) ctx->stats.score_ms = ms;
+        cudaGetLastError();
+    }
+    *out = ctx->stats;
+    return GRC_OK;
+}
+
+int grc_set_timing(grc_ctx *ctx, int enable) {
+    if (!ctx) return GRC_EINVAL;
+    Lock l(ctx);
+    ctx->timing = enable != 0;
+    return GRC_OK;
+}
+
+int grc_mask_info(grc_ctx *ctx, int64_t *n_distinct, int *code_bits, int64_t *dz, int64_t *dy, int64_t *nrot) {
+    if (!ctx) return GRC_EINVAL;
+    Lock l(ctx);
+    if (!ctx->has_masks) return fail(ctx, GRC_ENOMASK, "no distance map resident");
+    if (n_distinct) *n_distinct = ctx->mc.n_distinct;
+    if (code_bits) *code_bits = ctx->mc.n_distinct <= 65536 ? 16 : 32;
+    if (dz) *dz = ctx->mz;
+    if (dy) *dy = ctx->my;
+    if (nrot) *nrot = ctx->mrot;
+    return GRC_OK;
+}
+
+int grc_simulate_spots(grc_ctx *ctx, const float *d_pos, const float *d_U, int64_t n, uint8_t *d_mask) {
+    if (!ctx) return GRC_EINVAL;
+    Lock l(ctx);
+    if (!ctx->has_geo) return fail(ctx, GRC_EINVAL, "no geometry set");
+    if (n < 0) return fail(ctx, GRC_EINVAL, "negative size");
+    if (n == 0) return GRC_OK;
+    if (!d_pos || !d_U || !d_mask) return fail(ctx, GRC_EINVAL, "NULL device buffer");
+    TRY(ensure(ctx, ctx->U, sizeof(double) * 9 * n));
+    TRY(ensure(ctx, ctx->pos, sizeof(double) * 3 * n));
+    TRY(ensure(ctx, ctx->counter, 8 * sizeof(int)));
+    CU(grc::launch_f9_to_u(d_U, n, (double *)ctx->U.p, ctx->stream));
+    CU(grc::launch_pos_f3(d_pos, n, (double *)ctx->pos.p, ctx->stream));
+    grc::Work w{};
+    w.n_or = 1;
+    w.chunk = 1;
+    w.chunks_per_voxel = 1;
+    w.n_items = n;
+    w.diag = 1;
+    CU(grc::launch_simulate_work(ctx->geo, bufs(ctx), w, ctx->num_sms, d_mask, ctx->stream));
+    CU(cudaStreamSynchronize(ctx->stream));
+    return GRC_OK;
+}
+
+int grc_edt(grc_ctx *ctx, const uint8_t *d_mask, int64_t dz, int64_t dy, int64_t nrot, float *d_map) {
+    if (!ctx) return GRC_EINVAL;
+    Lock l(ctx);
+    if (!d_mask || !d_map) return fail(ctx, GRC_EINVAL, "NULL device buffer");
+    if (dz < 1 || dy < 1 || nrot < 1) return fail(ctx, GRC_EINVAL, "dimensions must be positive");
+    CU(grc::launch_edt(d_mask, dz, dy, nrot, d_map, ctx->stream));
+    return GRC_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,107 @@
+// grc_internal.h -- types shared by the scorer kernels and the C-ABI layer.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace grc {
+
+// Histogram width of the first scoring pass: distance-map codes below kHistBins
+// are counted exactly in shared memory; a trial whose median rank falls on a
+// larger code is finished by the radix refine kernel.
+constexpr int kHistBins = 1024;
+constexpr int kThreads = 256;
+constexpr int kWarps = kThreads / 32;
+constexpr int kQueueCap = 32 + 32 * 4;  // one 32-item batch in flight + 4 reflection slots per lane
+
+// Scalar geometry of one scorer call, FP64 (promoted from the float32 MEX
+// arguments).  Field names follow forward_comp.m.
+struct Geo {
+    double lss, lsd, p0y, p0z, dety00, detz00, pxy, pxz, rao;
+    double dety0, detz0;
+    double lmin, lmax;       // wavelength window [A]
+    double cbmax;            // cos((90+4*thetamax) deg), or -2 when that angle is >= 180 deg
+    double bsy0, bsy1, bsz0, bsz1;
+    double S[9], B[9], R[9]; // row-major
+    int nhkl, nrot, detysize, detzsize;
+    uint32_t n_hit;          // codes [0, n_hit) are "dis <= threshold"
+    uint32_t n_vals;         // entries of the code -> value table
+    int code_bits;           // bits of the largest code (radix passes of the refine kernel)
+    int64_t plane;           // detysize * detzsize
+};
+
+// Per-trial result of the scoring pass.  median is NaN while the exact radix
+// refine pass still has to produce it.
+struct TrialRes {
+    int32_t simu;
+    int32_t inter;
+    double median;
+};
+
+// Work enumeration.  Explicit: items[i] = {voxel, t_begin, t_end} and
+// trial_orient[t] = orientation index.  Implicit (items == nullptr):
+// n_vox voxels x n_or orientations in chunks of `chunk`, trial t = v*n_or + o.
+// diag != 0: trial t uses orientation t (one orientation per voxel).
+struct Work {
+    const longlong4 *items;
+    const int32_t *trial_orient;
+    int64_t n_items;
+    int64_t n_or;
+    int64_t chunks_per_voxel;
+    int32_t chunk;
+    int32_t diag;
+};
+
+struct ScoreBufs {
+    const double2 *rot_cs;    // cos/sin of every omega
+    const double *hkl;        // 3*nhkl
+    const double *vpos;       // 3 per voxel [mm]
+    const double *U;          // 9 per orientation
+    const void *codes;        // rank codes of the distance map
+    const float *vals;        // code -> distance value
+    TrialRes *res;
+    int *work_counter;        // 8 ints: [0..1] main-pass item counter (u64), [2..3] refine-pass
+                              // item counter (u64), [4] trials left for the refine pass
+};
+
+size_t score_smem_bytes(int nrot, int nhkl);
+size_t refine_smem_bytes(int nrot, int nhkl);
+// Enqueue the scoring pass (+ refine pass) on `s`.  Returns a cudaError_t.
+cudaError_t launch_score(const Geo &g, const ScoreBufs &b, const Work &w, int num_sms, cudaStream_t s,
+                         cudaEvent_t ev0, cudaEvent_t ev1, int *launches);
+
+// Orientation / position preparation kernels.
+cudaError_t launch_quat_to_u(const float *q, int64_t n, double *U, cudaStream_t s);
+cudaError_t launch_euler_to_u(const float *e, int64_t n, double *U, cudaStream_t s);
+cudaError_t launch_f9_to_u(const float *u9, int64_t n, double *U, cudaStream_t s);
+cudaError_t launch_pos_f3(const float *p, int64_t n, double *vpos, cudaStream_t s);
+cudaError_t launch_pos_rows(const float *rows, int stride, int64_t n, const double *p1, double *vpos,
+                            cudaStream_t s);
+
+// Epilogues: TrialRes -> MEX output layouts.
+cudaError_t launch_epi_forward(const TrialRes *res, int64_t n, float *out4, cudaStream_t s);
+cudaError_t launch_epi_grow(const TrialRes *res, const float *rows6, int64_t m, const double *p1, float *out7,
+                            cudaStream_t s);
+// CSR set-up for compete: counts from rows5 -> items / trial_orient.
+cudaError_t launch_csr_counts(const float *rows5, int64_t m, int64_t *counts, cudaStream_t s);
+cudaError_t launch_csr_fill(const float *rows5, int64_t m, const int64_t *offsets, const float *id_neigb,
+                            int64_t n_neigb, int64_t n_grain, longlong4 *items, int32_t *trial_orient,
+                            int *bad, cudaStream_t s);
+cudaError_t launch_epi_compete(const TrialRes *res, const longlong4 *items, const int32_t *trial_orient,
+                               int64_t m, const float *euler, float *out8, float *trial_out4, cudaStream_t s);
+
+// Distance-map rank coding.
+struct MapCodes {
+    void *codes;
+    float *vals;
+    int64_t n_distinct;
+    int code_bits;
+};
+// Encodes d_map (n floats) into codes; allocates codes/vals with cudaMalloc.
+cudaError_t encode_map(const float *d_map, int64_t n, cudaStream_t s, MapCodes *out, int *bad_nan);
+
+// Synthetic-data kernels.
+cudaError_t launch_simulate_work(const Geo &g, const ScoreBufs &b, const Work &w, int num_sms, uint8_t *mask,
+                                 cudaStream_t s);
+cudaError_t launch_edt(const uint8_t *mask, int64_t nz, int64_t ny, int64_t nrot, float *map, cudaStream_t s);
+
+}  // namespace grc

@@ -1,0 +1,587 @@
+// grc_score.cu -- the (voxel, orientation) completeness scorer for sm_100a.
+//
+// One kernel scores trials = (voxel, orientation) pairs; the seeding scan
+// (cuda_forward_comp), the grower (cuda_grow_indexed_region) and the
+// candidate competition (cuda_forward_comp_compete) are work lists over it.
+//
+// Per trial the reference (forward_comp.m:18-82) walks every projection omega
+// and every reflection hkl.  Here one CTA owns one trial at a time:
+//   * per work item (one voxel, a run of its trials) the CTA builds an omega
+//     table in shared memory: FP64 constants of the cone-beam geometry that do
+//     not depend on the orientation, plus the FP32 incident direction rotated
+//     back into the sample frame (k_w = Omega^T k_in);
+//   * warps take omegas round-robin, lanes take reflections (up to 4 per lane,
+//     the trial's G = S*U*B*h held in registers), and an FP32 prefilter
+//     -(k_w . G) in (lambda_min |G|^2/4pi, lambda_max |G|^2/4pi), widened by a
+//     margin far above its rounding error, drops the ~80% of reflections that
+//     miss the energy window after 3 FMAs;
+//   * survivors are compacted through a per-warp shared-memory queue and
+//     evaluated 32 at a time with every lane busy: the exact FP64 window test,
+//     the Bragg/cone-beam landing point and the tilted-detector intersection,
+//     round-half-away pixel, detector and beam-stop tests;
+//   * a selected reflection reads one rank code of the distance map; counts go
+//     to warp registers, the code to a shared-memory histogram, from which the
+//     exact median (MATLAB even-count rule) is read after the trial.  Medians
+//     whose rank lies above the histogram are finished by refine_kernel with
+//     10-bit radix passes.
+#include <cuda_runtime.h>
+#include <math_constants.h>
+#include <stdint.h>
+
+#include "grc_internal.h"
+
+namespace grc {
+namespace {
+
+constexpr unsigned kFull = 0xffffffffu;
+
+struct __align__(16) OmegaRow {
+    double kx, ky, kz, L2;  // unit incident direction (lab), L2 of forward_comp.m:42
+    double ax, ay, az, num; // center - SamposW; t-numerator of forward_comp.m:51
+    double r2d, r3d, c, s;  // RotDet(:,2).d, RotDet(:,3).d with d = SamposW - D0; cos/sin omega
+};
+static_assert(sizeof(OmegaRow) == 96, "OmegaRow layout");
+
+__device__ __forceinline__ size_t align16(size_t x) { return (x + 15) & ~size_t(15); }
+
+// forward_comp.m:17-26,42,51 for one voxel and every omega (FP64).
+__device__ void build_rows(const Geo &g, const double2 *__restrict__ rot_cs, const double *__restrict__ vp,
+                           OmegaRow *trow, float4 *kw) {
+    const double px = vp[0], py = vp[1] - g.rao, pz = vp[2];
+    const double spx = g.S[0] * px + g.S[1] * py + g.S[2] * pz;
+    const double spy = g.S[3] * px + g.S[4] * py + g.S[5] * pz;
+    const double spz = g.S[6] * px + g.S[7] * py + g.S[8] * pz;
+    const double L = g.lss + g.lsd;
+    for (int iw = threadIdx.x; iw < g.nrot; iw += blockDim.x) {
+        const double2 cs = rot_cs[iw];
+        const double c = cs.x, s = cs.y;
+        const double swx = c * spx - s * spy, swy = s * spx + c * spy, swz = spz;
+        const double gx = g.lss + swx, gy = swy - g.p0y + g.rao, gz = swz - g.p0z;
+        const double ngp = sqrt(gx * gx + gy * gy + gz * gz);
+        OmegaRow r;
+        r.kx = gx / ngp;
+        r.ky = gy / ngp;
+        r.kz = gz / ngp;
+        r.L2 = (g.lsd - swx) * ngp / gx;  // (Lsd - SamposW_x) / cos(alpha)
+        r.ax = g.lsd - swx;
+        r.ay = gy * L / gx - swy;
+        r.az = gz * L / gx - swz;
+        const double dx = swx - g.lsd, dy = swy - g.dety00 + g.rao, dz = swz - g.detz00;
+        r.num = -(g.R[0] * dx + g.R[3] * dy + g.R[6] * dz);
+        r.r2d = g.R[1] * dx + g.R[4] * dy + g.R[7] * dz;
+        r.r3d = g.R[2] * dx + g.R[5] * dy + g.R[8] * dz;
+        r.c = c;
+        r.s = s;
+        trow[iw] = r;
+        kw[iw] = make_float4((float)(c * r.kx + s * r.ky), (float)(-s * r.kx + c * r.ky), (float)r.kz, 0.f);
+    }
+}
+
+// Gw = S*U*B*h and |Gw| for every reflection of one trial (forward_comp.m:15-16).
+__device__ void build_gw(const Geo &g, const double *__restrict__ hkl, const double *__restrict__ U, double *gw) {
+    const int ih = threadIdx.x;
+    if (ih >= g.nhkl) return;
+    double SU[9], SUB[9];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j)
+            SU[3 * i + j] = g.S[3 * i] * U[j] + g.S[3 * i + 1] * U[3 + j] + g.S[3 * i + 2] * U[6 + j];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j)
+            SUB[3 * i + j] = SU[3 * i] * g.B[j] + SU[3 * i + 1] * g.B[3 + j] + SU[3 * i + 2] * g.B[6 + j];
+    const double h = hkl[3 * ih], k = hkl[3 * ih + 1], l = hkl[3 * ih + 2];
+    const double x = SUB[0] * h + SUB[1] * k + SUB[2] * l;
+    const double y = SUB[3] * h + SUB[4] * k + SUB[5] * l;
+    const double z = SUB[6] * h + SUB[7] * k + SUB[8] * l;
+    gw[4 * ih] = x;
+    gw[4 * ih + 1] = y;
+    gw[4 * ih + 2] = z;
+    gw[4 * ih + 3] = sqrt(x * x + y * y + z * z);
+}
+
+// Exact FP64 evaluation of one reflection (omega row iw, reflection ih):
+// returns the linear map index of its pixel, or -1 when select3 of
+// forward_comp.m:61-65 rejects it.  Algebraic form of forward_comp.m:28-59:
+// sin(theta) = -cos(beta), cos(theta) = sin(beta), sin(phiy) expanded, and the
+// ray/plane intersection without normalising K_out.
+__device__ __forceinline__ int64_t landing_index(const Geo &g, const OmegaRow &r, const double *gw, int iw,
+                                                 int ih) {
+    const double gxw = gw[4 * ih], gyw = gw[4 * ih + 1], gzw = gw[4 * ih + 2], G = gw[4 * ih + 3];
+    const double Gtx = r.c * gxw - r.s * gyw, Gty = r.s * gxw + r.c * gyw, Gtz = gzw;
+    const double x = (r.kx * Gtx + r.ky * Gty + r.kz * Gtz) / G;  // cos(beta)
+    const double lam = 2.0 * (2.0 * CUDART_PI / G) * (-x);        // 2 d sin(theta)
+    if (!(x < 0.0 && x > g.cbmax && lam > g.lmin && lam < g.lmax)) return -1;
+    const double st = -x, ct = sqrt(1.0 - x * x);
+    const double s2 = 2.0 * st * ct, c2 = 1.0 - 2.0 * st * st;
+    const double konst = sqrt(Gty * Gty + Gtz * Gtz);
+    const double gy = Gty / konst, gz = Gtz / konst;
+    const double cphx = gy * r.ky + gz * r.kz;
+    const double sphx = sqrt(fmax(0.0, 1.0 - cphx * cphx));
+    const double sphy = sphx * c2 - cphx * s2;
+    const double diff = r.L2 * s2 / sphy;
+    const double Kx = r.ax, Ky = r.ay + diff * gy, Kz = r.az + diff * gz;
+    const double nK = g.R[0] * Kx + g.R[3] * Ky + g.R[6] * Kz;
+    const double f = r.num / nK;
+    const double y2 = f * (g.R[1] * Kx + g.R[4] * Ky + g.R[7] * Kz) + r.r2d;
+    const double z2 = f * (g.R[2] * Kx + g.R[5] * Ky + g.R[8] * Kz) + r.r3d;
+    const double u = g.dety0 - y2 / g.pxy, v = g.detz0 - z2 / g.pxz;
+    // 1 <= round(u) <= detysize  <=>  0.5 <= u < detysize + 0.5 (round half away from zero)
+    if (!(u >= 0.5 && u < g.detysize + 0.5 && v >= 0.5 && v < g.detzsize + 0.5)) return -1;
+    const double ru = round(u), rv = round(v);
+    if (ru >= g.bsy0 && ru <= g.bsy1 && rv >= g.bsz0 && rv <= g.bsz1) return -1;
+    return (int64_t)iw * g.plane + (int64_t)(ru - 1.0) * g.detzsize + (int64_t)(rv - 1.0);
+}
+
+// Counts + histogram of codes below kHistBins (scoring pass).
+template <typename CodeT>
+struct HistSink {
+    const CodeT *codes;
+    uint32_t *hist;
+    uint32_t n_hit;
+    int simu, inter, over;
+    __device__ __forceinline__ void on(int64_t idx) {
+        const bool ok = idx >= 0;
+        uint32_t code = 0;
+        if (ok) code = (uint32_t)__ldg(codes + idx);
+        const bool inr = ok && code < (uint32_t)kHistBins;
+        if (inr) atomicAdd(&hist[code], 1u);
+        const unsigned mo = __ballot_sync(kFull, ok);
+        const unsigned mh = __ballot_sync(kFull, ok && code < n_hit);
+        const unsigned mi = __ballot_sync(kFull, inr);
+        simu += __popc(mo);
+        inter += __popc(mh);
+        over += __popc(mo & ~mi);
+    }
+};
+
+// One 10-bit radix digit pass for two target ranks (refine pass).
+template <typename CodeT>
+struct RadixSink {
+    const CodeT *codes;
+    uint32_t *ha, *hb;
+    uint32_t pa, pb;
+    int digit_shift, prefix_shift;
+    uint32_t digit_mask;
+    __device__ __forceinline__ void on(int64_t idx) {
+        if (idx < 0) return;
+        const uint32_t code = (uint32_t)__ldg(codes + idx);
+        const uint32_t pre = prefix_shift >= 32 ? 0u : (code >> prefix_shift);
+        const uint32_t d = (code >> digit_shift) & digit_mask;
+        if (pre == pa) atomicAdd(&ha[d], 1u);
+        if (pre == pb) atomicAdd(&hb[d], 1u);
+    }
+};
+
+// Marks landing pixels (synthetic spot simulation).
+struct MarkSink {
+    uint8_t *mask;
+    __device__ __forceinline__ void on(int64_t idx) {
+        if (idx >= 0) mask[idx] = 1;
+    }
+};
+
+// Walk every (omega, reflection) of one trial; the sink sees each selected pixel.
+template <int HPL, typename Sink>
+__device__ __forceinline__ void run_trial(const Geo &g, const OmegaRow *trow, const float4 *kw, const double *gw,
+                                          uint32_t *wq, Sink &sink) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const unsigned lt = (1u << lane) - 1u;
+    float pfx[HPL], pfy[HPL], pfz[HPL], plo[HPL], phi[HPL];
+    const double inv4pi = 0.25 / CUDART_PI;
+#pragma unroll
+    for (int j = 0; j < HPL; ++j) {
+        const int ih = lane + 32 * j;
+        if (ih < g.nhkl) {
+            const double G = gw[4 * ih + 3], G2 = G * G;
+            double lo = g.lmin * G2 * inv4pi, hi = g.lmax * G2 * inv4pi;
+            if (g.cbmax > -1.0) hi = fmin(hi, -g.cbmax * G);
+            lo = fmax(lo, 0.0);
+            const double m = 1e-5 * G;  // >> FP32 error of k_w . G (~4e-7 |G|)
+            plo[j] = (float)(lo - m);
+            phi[j] = (float)(hi + m);
+            pfx[j] = (float)gw[4 * ih];
+            pfy[j] = (float)gw[4 * ih + 1];
+            pfz[j] = (float)gw[4 * ih + 2];
+        } else {
+            plo[j] = CUDART_INF_F;
+            phi[j] = -CUDART_INF_F;
+            pfx[j] = pfy[j] = pfz[j] = 0.f;
+        }
+    }
+    int qn = 0;
+    for (int iw = warp; iw < g.nrot; iw += kWarps) {
+        const float4 k = kw[iw];
+#pragma unroll
+        for (int j = 0; j < HPL; ++j) {
+            const float t = -fmaf(k.x, pfx[j], fmaf(k.y, pfy[j], k.z * pfz[j]));
+            const bool pass = (t > plo[j]) && (t < phi[j]);
+            const unsigned m = __ballot_sync(kFull, pass);
+            if (pass) wq[qn + __popc(m & lt)] = ((uint32_t)iw << 8) | (uint32_t)(lane + 32 * j);
+            qn += __popc(m);
+        }
+        __syncwarp();
+        while (qn >= 32) {
+            qn -= 32;
+            const uint32_t item = wq[qn + lane];
+            __syncwarp();
+            const int iwi = (int)(item >> 8), ihi = (int)(item & 255u);
+            sink.on(landing_index(g, trow[iwi], gw, iwi, ihi));
+        }
+    }
+    if (qn > 0) {
+        const bool valid = lane < qn;
+        const uint32_t item = valid ? wq[lane] : 0u;
+        __syncwarp();
+        int64_t idx = -1;
+        if (valid) {
+            const int iwi = (int)(item >> 8), ihi = (int)(item & 255u);
+            idx = landing_index(g, trow[iwi], gw, iwi, ihi);
+        }
+        sink.on(idx);
+    }
+    __syncwarp();
+}
+
+struct Smem {
+    OmegaRow *trow;
+    float4 *kw;
+    double *gw;
+    uint32_t *h0, *h1;
+    uint32_t *queue;
+};
+
+__device__ __forceinline__ Smem carve(unsigned char *base, const Geo &g, int nhist) {
+    Smem s;
+    size_t off = 0;
+    s.trow = (OmegaRow *)(base + off);
+    off = align16(off + sizeof(OmegaRow) * g.nrot);
+    s.kw = (float4 *)(base + off);
+    off = align16(off + sizeof(float4) * g.nrot);
+    s.gw = (double *)(base + off);
+    off = align16(off + sizeof(double) * 4 * g.nhkl);
+    s.h0 = (uint32_t *)(base + off);
+    off += sizeof(uint32_t) * kHistBins;
+    s.h1 = nhist > 1 ? (uint32_t *)(base + off) : nullptr;
+    off += nhist > 1 ? sizeof(uint32_t) * kHistBins : 0;
+    s.queue = (uint32_t *)(base + off);
+    return s;
+}
+
+__device__ __forceinline__ bool next_item(const Work &w, unsigned long long *counter, int64_t *s_item,
+                                          int64_t &v, int64_t &t0, int64_t &t1) {
+    if (threadIdx.x == 0) *s_item = (int64_t)atomicAdd(counter, 1ull);
+    __syncthreads();
+    const int64_t it = *s_item;
+    __syncthreads();
+    if (it >= w.n_items) return false;
+    if (w.items) {
+        const longlong4 e = w.items[it];
+        v = e.x;
+        t0 = e.y;
+        t1 = e.z;
+    } else {
+        v = it / w.chunks_per_voxel;
+        const int64_t c = it % w.chunks_per_voxel;
+        t0 = v * w.n_or + c * w.chunk;
+        const int64_t end = (v + 1) * w.n_or;
+        t1 = t0 + w.chunk < end ? t0 + w.chunk : end;
+    }
+    return true;
+}
+
+__device__ __forceinline__ int64_t orient_of(const Work &w, int64_t t, int64_t v) {
+    if (w.trial_orient) return (int64_t)w.trial_orient[t];
+    return w.diag ? t : (t - v * w.n_or);
+}
+
+// Block-wide search of the smallest bins with cumulative count >= ra and >= rb.
+__device__ void find_two_ranks(const uint32_t *hist, int ra, int rb, int *s_code, uint32_t *s_wsum) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    constexpr int per = kHistBins / kThreads;
+    const int base = threadIdx.x * per;
+    uint32_t c[per];
+    uint32_t local = 0;
+#pragma unroll
+    for (int i = 0; i < per; ++i) {
+        c[i] = hist[base + i];
+        local += c[i];
+    }
+    uint32_t incl = local;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(kFull, incl, o);
+        if (lane >= o) incl += y;
+    }
+    if (lane == 31) s_wsum[warp] = incl;
+    __syncthreads();
+    uint32_t woff = 0;
+    for (int i = 0; i < warp; ++i) woff += s_wsum[i];
+    const uint32_t excl = incl - local + woff;
+    const uint32_t r2[2] = {(uint32_t)ra, (uint32_t)rb};
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+        const uint32_t r = r2[q];
+        if (excl < r && r <= excl + local) {
+            uint32_t cum = excl;
+#pragma unroll
+            for (int i = 0; i < per; ++i) {
+                cum += c[i];
+                if (cum >= r) {
+                    s_code[q] = base + i;
+                    break;
+                }
+            }
+        }
+    }
+}
+
+template <int HPL, typename CodeT>
+__global__ void __launch_bounds__(kThreads, 2) score_kernel(Geo g, ScoreBufs b, Work w) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const Smem sm = carve(smem_raw, g, 1);
+    __shared__ int64_t s_item;
+    __shared__ int s_simu, s_inter, s_over;
+    __shared__ int s_code[2];
+    __shared__ uint32_t s_wsum[kWarps];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    uint32_t *wq = sm.queue + warp * kQueueCap;
+    const CodeT *codes = (const CodeT *)b.codes;
+    unsigned long long *counter = (unsigned long long *)b.work_counter;
+    int64_t v, t0, t1;
+    while (next_item(w, counter, &s_item, v, t0, t1)) {
+        if (t0 >= t1) continue;
+        build_rows(g, b.rot_cs, b.vpos + 3 * v, sm.trow, sm.kw);
+        for (int64_t t = t0; t < t1; ++t) {
+            const int64_t o = orient_of(w, t, v);
+            build_gw(g, b.hkl, b.U + 9 * o, sm.gw);
+            for (int i = threadIdx.x; i < kHistBins; i += kThreads) sm.h0[i] = 0;
+            if (threadIdx.x == 0) {
+                s_simu = s_inter = s_over = 0;
+                s_code[0] = s_code[1] = -1;
+            }
+            __syncthreads();
+            HistSink<CodeT> sink{codes, sm.h0, g.n_hit, 0, 0, 0};
+            run_trial<HPL>(g, sm.trow, sm.kw, sm.gw, wq, sink);
+            if (lane == 0) {
+                atomicAdd(&s_simu, sink.simu);
+                atomicAdd(&s_inter, sink.inter);
+                atomicAdd(&s_over, sink.over);
+            }
+            __syncthreads();
+            const int n = s_simu, inr = n - s_over;
+            const int ra = (n + 1) / 2, rb = n / 2 + 1;
+            const bool direct = n > 0 && rb <= inr;
+            if (direct) find_two_ranks(sm.h0, ra, rb, s_code, s_wsum);
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                TrialRes r;
+                r.simu = n;
+                r.inter = s_inter;
+                if (n == 0) {
+                    r.median = 2000.0;  // forward_comp.m:89
+                } else if (direct) {
+                    const uint32_t ca = min((uint32_t)s_code[0], g.n_vals - 1u), cb = min((uint32_t)s_code[1], g.n_vals - 1u);
+                    r.median = ((double)b.vals[ca] + (double)b.vals[cb]) / 2.0;
+                } else {
+                    r.median = CUDART_NAN;
+                    atomicAdd(b.work_counter + 4, 1);
+                }
+                b.res[t] = r;
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// Exact median for trials whose median rank lies beyond the histogram: radix
+// select over the code bits, two ranks at once, one full trial walk per digit.
+template <int HPL, typename CodeT>
+__global__ void __launch_bounds__(kThreads, 2) refine_kernel(Geo g, ScoreBufs b, Work w) {
+    if (b.work_counter[4] == 0) return;  // nothing to refine
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const Smem sm = carve(smem_raw, g, 2);
+    __shared__ int64_t s_item;
+    __shared__ int s_any;
+    __shared__ uint32_t s_pa, s_pb, s_ra, s_rb;
+    const int warp = threadIdx.x >> 5;
+    uint32_t *wq = sm.queue + warp * kQueueCap;
+    const CodeT *codes = (const CodeT *)b.codes;
+    unsigned long long *counter = (unsigned long long *)(b.work_counter + 2);
+    int64_t v, t0, t1;
+    while (next_item(w, counter, &s_item, v, t0, t1)) {
+        if (threadIdx.x == 0) s_any = 0;
+        __syncthreads();
+        for (int64_t t = t0 + threadIdx.x; t < t1; t += kThreads)
+            if (isnan(b.res[t].median)) s_any = 1;
+        __syncthreads();
+        if (!s_any) continue;
+        build_rows(g, b.rot_cs, b.vpos + 3 * v, sm.trow, sm.kw);
+        __syncthreads();
+        for (int64_t t = t0; t < t1; ++t) {
+            if (!isnan(b.res[t].median)) continue;  // uniform: every thread reads the same value
+            const int64_t o = orient_of(w, t, v);
+            build_gw(g, b.hkl, b.U + 9 * o, sm.gw);
+            const int n = b.res[t].simu;
+            if (threadIdx.x == 0) {
+                s_pa = s_pb = 0;
+                s_ra = (uint32_t)((n + 1) / 2);
+                s_rb = (uint32_t)(n / 2 + 1);
+            }
+            int pos = g.code_bits;
+            while (pos > 0) {
+                const int width = pos < 10 ? pos : 10;
+                pos -= width;
+                for (int i = threadIdx.x; i < kHistBins; i += kThreads) sm.h0[i] = sm.h1[i] = 0;
+                __syncthreads();
+                RadixSink<CodeT> sink{codes, sm.h0, sm.h1, s_pa, s_pb, pos, pos + width, (1u << width) - 1u};
+                run_trial<HPL>(g, sm.trow, sm.kw, sm.gw, wq, sink);
+                __syncthreads();
+                if (threadIdx.x == 0) {
+                    uint32_t cum = 0;
+                    for (uint32_t d = 0; d < (1u << width); ++d) {
+                        if (cum + sm.h0[d] >= s_ra) {
+                            s_ra -= cum;
+                            s_pa = (s_pa << width) | d;
+                            break;
+                        }
+                        cum += sm.h0[d];
+                    }
+                    cum = 0;
+                    for (uint32_t d = 0; d < (1u << width); ++d) {
+                        if (cum + sm.h1[d] >= s_rb) {
+                            s_rb -= cum;
+                            s_pb = (s_pb << width) | d;
+                            break;
+                        }
+                        cum += sm.h1[d];
+                    }
+                }
+                __syncthreads();
+            }
+            if (threadIdx.x == 0) {
+                const uint32_t ca = min(s_pa, g.n_vals - 1u), cb = min(s_pb, g.n_vals - 1u);
+                b.res[t].median = ((double)b.vals[ca] + (double)b.vals[cb]) / 2.0;
+            }
+            __syncthreads();
+        }
+    }
+}
+
+// Synthetic spot simulation: every trial marks its selected landing pixels.
+template <int HPL>
+__global__ void __launch_bounds__(kThreads, 2) mark_kernel(Geo g, ScoreBufs b, Work w, uint8_t *mask) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const Smem sm = carve(smem_raw, g, 1);
+    __shared__ int64_t s_item;
+    const int warp = threadIdx.x >> 5;
+    uint32_t *wq = sm.queue + warp * kQueueCap;
+    unsigned long long *counter = (unsigned long long *)b.work_counter;
+    int64_t v, t0, t1;
+    while (next_item(w, counter, &s_item, v, t0, t1)) {
+        if (t0 >= t1) continue;
+        build_rows(g, b.rot_cs, b.vpos + 3 * v, sm.trow, sm.kw);
+        for (int64_t t = t0; t < t1; ++t) {
+            build_gw(g, b.hkl, b.U + 9 * orient_of(w, t, v), sm.gw);
+            __syncthreads();
+            MarkSink sink{mask};
+            run_trial<HPL>(g, sm.trow, sm.kw, sm.gw, wq, sink);
+            __syncthreads();
+        }
+    }
+}
+
+template <typename K>
+cudaError_t prep_launch(K kern, size_t smem, int num_sms, int64_t n_items, int *grid_out) {
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    int per_sm = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kThreads, smem);
+    if (e != cudaSuccess) return e;
+    if (per_sm < 1) return cudaErrorInvalidConfiguration;
+    int64_t grid = (int64_t)per_sm * num_sms;
+    if (grid > n_items) grid = n_items;
+    if (grid < 1) grid = 1;
+    *grid_out = (int)grid;
+    return cudaSuccess;
+}
+
+template <int HPL, typename CodeT>
+cudaError_t launch_score_t(const Geo &g, const ScoreBufs &b, const Work &w, int num_sms, cudaStream_t s,
+                           cudaEvent_t ev0, cudaEvent_t ev1, int *launches) {
+    const size_t smem = score_smem_bytes(g.nrot, g.nhkl);
+    const size_t smem_r = refine_smem_bytes(g.nrot, g.nhkl);
+    int grid = 0, grid_r = 0;
+    cudaError_t e = prep_launch(score_kernel<HPL, CodeT>, smem, num_sms, w.n_items, &grid);
+    if (e != cudaSuccess) return e;
+    e = prep_launch(refine_kernel<HPL, CodeT>, smem_r, num_sms, w.n_items, &grid_r);
+    if (e != cudaSuccess) return e;
+    // counters: [0..1] main work (u64), [2..3] refine work (u64), [4] refine needed
+    e = cudaMemsetAsync(b.work_counter, 0, 8 * sizeof(int), s);
+    if (e != cudaSuccess) return e;
+    if (ev0) cudaEventRecord(ev0, s);
+    score_kernel<HPL, CodeT><<<grid, kThreads, smem, s>>>(g, b, w);
+    if (ev1) cudaEventRecord(ev1, s);
+    refine_kernel<HPL, CodeT><<<grid_r, kThreads, smem_r, s>>>(g, b, w);
+    *launches += 2;
+    return cudaGetLastError();
+}
+
+template <int HPL>
+cudaError_t launch_mark_t(const Geo &g, const ScoreBufs &b, const Work &w, int num_sms, uint8_t *mask,
+                          cudaStream_t s) {
+    const size_t smem = score_smem_bytes(g.nrot, g.nhkl);
+    int grid = 0;
+    cudaError_t e = prep_launch(mark_kernel<HPL>, smem, num_sms, w.n_items, &grid);
+    if (e != cudaSuccess) return e;
+    e = cudaMemsetAsync(b.work_counter, 0, 8 * sizeof(int), s);
+    if (e != cudaSuccess) return e;
+    mark_kernel<HPL><<<grid, kThreads, smem, s>>>(g, b, w, mask);
+    return cudaGetLastError();
+}
+
+}  // namespace
+
+size_t score_smem_bytes(int nrot, int nhkl) {
+    size_t off = 0;
+    off = (off + sizeof(OmegaRow) * nrot + 15) & ~size_t(15);
+    off = (off + sizeof(float4) * nrot + 15) & ~size_t(15);
+    off = (off + sizeof(double) * 4 * nhkl + 15) & ~size_t(15);
+    off += sizeof(uint32_t) * kHistBins;
+    off += sizeof(uint32_t) * kWarps * kQueueCap;
+    return off;
+}
+
+size_t refine_smem_bytes(int nrot, int nhkl) { return score_smem_bytes(nrot, nhkl) + sizeof(uint32_t) * kHistBins; }
+
+cudaError_t launch_score(const Geo &g, const ScoreBufs &b, const Work &w, int num_sms, cudaStream_t s,
+                         cudaEvent_t ev0, cudaEvent_t ev1, int *launches) {
+    const int hpl = (g.nhkl + 31) / 32;
+    const bool c16 = g.code_bits <= 16;
+#define GRC_DISPATCH(H)                                                                        \
+    if (hpl == H)                                                                              \
+        return c16 ? launch_score_t<H, uint16_t>(g, b, w, num_sms, s, ev0, ev1, launches)     \
+                   : launch_score_t<H, uint32_t>(g, b, w, num_sms, s, ev0, ev1, launches);
+    GRC_DISPATCH(1)
+    GRC_DISPATCH(2)
+    GRC_DISPATCH(3)
+    GRC_DISPATCH(4)
+#undef GRC_DISPATCH
+    return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_simulate_work(const Geo &g, const ScoreBufs &b, const Work &w, int num_sms, uint8_t *mask,
+                                 cudaStream_t s) {
+    const int hpl = (g.nhkl + 31) / 32;
+    switch (hpl) {
+        case 1: return launch_mark_t<1>(g, b, w, num_sms, mask, s);
+        case 2: return launch_mark_t<2>(g, b, w, num_sms, mask, s);
+        case 3: return launch_mark_t<3>(g, b, w, num_sms, mask, s);
+        case 4: return launch_mark_t<4>(g, b, w, num_sms, mask, s);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+}  // namespace grc

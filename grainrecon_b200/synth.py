@@ -1,0 +1,241 @@
+"""Seeded synthetic samples, spot masks and distance maps.
+
+The reference's example data (spot .mat files, ground-truth h5, 1-degree grids) is
+not available, so benchmarks and tests run on synthetic samples with the shapes of
+the reference's configurations:
+
+* a cylinder of voxels split into grains by a seeded (power-weighted) Voronoi
+  tessellation, one uniformly random orientation per grain;
+* spot masks forward-simulated from that ground truth with the point-voxel model
+  of forward_comp.m (a pixel is a spot pixel when some voxel of some grain lands a
+  selected reflection on it);
+* the distance map ``proj_bin_bw = bwdist(mask)`` of GrainMapping_fun.m:73-75, i.e.
+  the Euclidean distance of every pixel to the nearest spot pixel (0 on spots).
+
+Everything here is host-side numpy; large volumes use the library's device-side
+spot simulator and EDT instead (``grainrecon_b200.forward.simulate_masks``).
+"""
+from __future__ import annotations
+
+import dataclasses
+
+import numpy as np
+
+from . import geometry as G
+
+
+@dataclasses.dataclass
+class Sample:
+    geom: G.Geometry
+    vol: G.Volume
+    cell: tuple
+    space_group: int
+    B: np.ndarray                 # 3x3
+    hkl: np.ndarray               # nhkl x 3
+    S: np.ndarray                 # 3x3
+    grain_id: np.ndarray          # Dim int32 (0 = outside the cylinder)
+    grain_q: np.ndarray           # ngrain x 4 ground-truth quaternions (row g-1 = grain g)
+    seed: int = 0
+
+    @property
+    def nhkl(self) -> int:
+        return int(self.hkl.shape[0])
+
+    def voxel_indices(self) -> np.ndarray:
+        """1-based (x,y,z) indices of every voxel inside the sample, in C order."""
+        idx = np.argwhere(self.grain_id > 0) + 1
+        return idx.astype(np.int64)
+
+    def mex_arrays(self):
+        """(S9, B9, hkl_flat, rot_angles, RotDet9, param20) as the MATLAB wrappers build them."""
+        return (G.flat_rowmajor(self.S), G.flat_rowmajor(self.B), G.flat_hkl(self.hkl),
+                np.asarray(self.geom.rot_angles, np.float32), G.flat_rowmajor(self.geom.rot_det),
+                self.geom.param20(self.nhkl))
+
+
+def voronoi_cylinder(dim: int, n_grains: int, seed: int, lognormal_sigma: float = 0.0) -> np.ndarray:
+    """Grain-id volume (dim^3, int32) of a cylinder along z split by a seeded Voronoi.
+
+    With ``lognormal_sigma > 0`` each site gets a log-normal weight and voxels go to
+    the site minimising |x-c|^2 - w^2 (a power diagram), which spreads grain sizes.
+    """
+    rng = np.random.default_rng(seed)
+    r = dim / 2.0
+    ax = np.arange(dim) + 0.5
+    X, Y, Z = np.meshgrid(ax, ax, ax, indexing="ij")
+    inside = (X - r) ** 2 + (Y - r) ** 2 <= r * r
+    # sites inside the cylinder
+    sites = []
+    while len(sites) < n_grains:
+        p = rng.random(3) * dim
+        if (p[0] - r) ** 2 + (p[1] - r) ** 2 <= r * r:
+            sites.append(p)
+    sites = np.array(sites)
+    mean_d = dim / max(n_grains, 1) ** (1 / 3)
+    w2 = np.zeros(n_grains)
+    if lognormal_sigma > 0:
+        w = rng.lognormal(mean=0.0, sigma=lognormal_sigma, size=n_grains) * mean_d * 0.5
+        w2 = w * w
+    pts = np.stack([X[inside], Y[inside], Z[inside]], axis=1)
+    best = np.zeros(len(pts), np.int32)
+    bestd = np.full(len(pts), np.inf)
+    chunk = 1 << 16
+    for s in range(0, len(pts), chunk):
+        p = pts[s:s + chunk]
+        d = ((p[:, None, :] - sites[None, :, :]) ** 2).sum(-1) - w2[None, :]
+        best[s:s + chunk] = np.argmin(d, axis=1).astype(np.int32) + 1
+    gid = np.zeros((dim, dim, dim), np.int32)
+    gid[inside] = best
+    return gid
+
+
+def make_sample(kind: str = "fe_small", seed: int = 1, **over) -> Sample:
+    """Named synthetic samples.
+
+    ``fe6``   : BCC Fe a=2.8665, 6 grains, 100 um cylinder at 5 um (20^3 grid, ~6.3k voxels),
+                6 families (86 reflections), 1024^2 detector at 0.0672 mm, Lss=Lsd=11 mm,
+                tilts U(-0.5,0.5) deg, 181 projections 0:2:360, E 10-70 keV.
+    ``al400`` : FCC Al a=4.0495, 400 grains log-normal (sigma 0.4), 400 um cylinder at 2.5 um
+                (160^3 grid, ~3.2M voxels), 6 families (64 reflections), 2048^2 detector at
+                0.0336 mm, 361 projections 0:1:360.
+    ``fe_small``: the fe6 set-up shrunk for fast CPU tests (12^3 grid, 256^2 detector at
+                0.2688 mm, 37 projections 0:10:360).
+    """
+    rng = np.random.default_rng(seed + 1000)
+    tilt = tuple(rng.uniform(-0.5, 0.5, 3))
+    if kind in ("fe6", "fe_small", "fe_tiny"):
+        cell = (2.8665, 2.8665, 2.8665, 90, 90, 90)
+        sg = 229
+        if kind == "fe6":
+            dim, ng, det, px, rot = 20, 6, 1024, 0.0672, np.arange(0, 361, 2.0)
+        elif kind == "fe_small":
+            dim, ng, det, px, rot = 12, 6, 256, 0.2688, np.arange(0, 361, 10.0)
+        else:
+            dim, ng, det, px, rot = 8, 3, 128, 0.5376, np.arange(0, 361, 30.0)
+        vox = 0.1 / dim
+        sigma = 0.0
+    elif kind in ("al400", "al_small"):
+        cell = (4.0495, 4.0495, 4.0495, 90, 90, 90)
+        sg = 225
+        if kind == "al400":
+            dim, ng, det, px, rot = 160, 400, 2048, 0.0336, np.arange(0, 361, 1.0)
+        else:
+            dim, ng, det, px, rot = 24, 20, 512, 0.1344, np.arange(0, 361, 5.0)
+        vox = 0.4 / dim
+        sigma = 0.4
+    else:
+        raise ValueError(kind)
+    geom = G.Geometry(pxy=px, pxz=px, detysize=det, detzsize=det, tilt=tilt, rot_angles=rot)
+    for k, v in over.items():
+        setattr(geom, k, v)
+    vol = G.Volume(rec_volume_pixel=(1, 1, 1), simap=1, vox_size=vox, center=(0.0, 0.0, 0.0),
+                   dimension=(dim, dim, dim))
+    gid = voronoi_cylinder(dim, ng, seed, sigma)
+    q = G.cubic_fz_orientations(ng, seed + 7)
+    hkl = G.gen_hkl(sg, 6)
+    return Sample(geom=geom, vol=vol, cell=cell, space_group=sg, B=G.form_b(cell), hkl=hkl, S=np.eye(3),
+                  grain_id=gid, grain_q=q, seed=seed)
+
+
+def landing_pixels(sample: Sample, pos: np.ndarray, U: np.ndarray, dety0=None, detz0=None):
+    """Selected landing pixels of many (pos, U) trials -- algebraic form, float64.
+
+    ``pos``: n x 3 [mm]; ``U``: n x 3 x 3.  Returns (iw, dety, detz) int arrays (1-based
+    pixel indices) of every selected reflection.  Used only to synthesise masks.
+    """
+    g = sample.geom
+    f = lambda a: np.asarray(np.asarray(a, np.float32), np.float64)
+    S = f(G.flat_rowmajor(sample.S)).reshape(3, 3)
+    B = f(G.flat_rowmajor(sample.B)).reshape(3, 3)
+    R = f(G.flat_rowmajor(g.rot_det)).reshape(3, 3)
+    p = f(g.param20(sample.nhkl))
+    lss, lsd, p0y, p0z, y00, z00, pxy, pxz = p[2:10]
+    ny, nz = int(p[10]), int(p[11])
+    bs = p[12:16]
+    tmax, lmin, lmax, rao = p[16:20]
+    dety0 = ny / 2 + 0.5 if dety0 is None else dety0
+    detz0 = nz / 2 + 0.5 if detz0 is None else detz0
+    hkl = f(sample.hkl)
+    pos = f(pos).copy()
+    pos[:, 1] -= rao
+    Sp = pos @ S.T
+    Gw = np.einsum("ij,njk,kl,hl->nhi", S, f(U), B, hkl)          # n x nhkl x 3
+    Glen = np.linalg.norm(Gw, axis=-1)
+    cbmax = np.cos(np.radians(90 + 4 * tmax)) if 90 + 4 * tmax < 180 else -2.0
+    out = []
+    for iw, w in enumerate(f(g.rot_angles)):
+        c, s = np.cos(np.radians(w)), np.sin(np.radians(w))
+        SW = np.stack([c * Sp[:, 0] - s * Sp[:, 1], s * Sp[:, 0] + c * Sp[:, 1], Sp[:, 2]], 1)
+        gp = np.stack([lss + SW[:, 0], SW[:, 1] - p0y + rao, SW[:, 2] - p0z], 1)
+        ngp = np.linalg.norm(gp, axis=1)
+        k = gp / ngp[:, None]
+        L2 = (lsd - SW[:, 0]) * ngp / gp[:, 0]
+        L = lss + lsd
+        a = np.stack([lsd - SW[:, 0], gp[:, 1] * L / gp[:, 0] - SW[:, 1], gp[:, 2] * L / gp[:, 0] - SW[:, 2]], 1)
+        dv = np.stack([SW[:, 0] - lsd, SW[:, 1] - y00 + rao, SW[:, 2] - z00], 1)
+        num = -(dv @ R[:, 0])
+        Gt = np.stack([c * Gw[..., 0] - s * Gw[..., 1], s * Gw[..., 0] + c * Gw[..., 1], Gw[..., 2]], -1)
+        x = np.einsum("ni,nhi->nh", k, Gt) / Glen
+        lam = -2 * (2 * np.pi / Glen) * x
+        ok = (x < 0) & (x > cbmax) & (lam > lmin) & (lam < lmax)
+        if not ok.any():
+            continue
+        ni, hi = np.nonzero(ok)
+        xs = x[ni, hi]
+        st = -xs
+        ct = np.sqrt(1 - xs * xs)
+        s2, c2 = 2 * st * ct, 1 - 2 * st * st
+        gt = Gt[ni, hi]
+        konst = np.hypot(gt[:, 1], gt[:, 2])
+        gy, gz = gt[:, 1] / konst, gt[:, 2] / konst
+        kk = k[ni]
+        cphx = gy * kk[:, 1] + gz * kk[:, 2]
+        sphx = np.sqrt(np.maximum(0, 1 - cphx * cphx))
+        with np.errstate(divide="ignore", invalid="ignore"):
+            diff = L2[ni] * s2 / (sphx * c2 - cphx * s2)
+            K = a[ni] + np.stack([np.zeros_like(diff), diff * gy, diff * gz], 1)
+            fK = num[ni] / (K @ R[:, 0])
+            y2 = fK * (K @ R[:, 1]) + dv[ni] @ R[:, 1]
+            z2 = fK * (K @ R[:, 2]) + dv[ni] @ R[:, 2]
+            u = dety0 - y2 / pxy
+            v = detz0 - z2 / pxz
+        iu, iv = np.floor(u + 0.5), np.floor(v + 0.5)
+        sel = (iu >= 1) & (iu <= ny) & (iv >= 1) & (iv <= nz) & ~(
+            (iu >= bs[0]) & (iu <= bs[1]) & (iv >= bs[2]) & (iv <= bs[3]))
+        out.append((np.full(int(sel.sum()), iw), iu[sel].astype(np.int64), iv[sel].astype(np.int64)))
+    if not out:
+        z = np.zeros(0, np.int64)
+        return z, z, z
+    return tuple(np.concatenate([o[i] for o in out]) for i in range(3))
+
+
+def simulate_mask(sample: Sample, stride: int = 1, chunk: int = 2048) -> np.ndarray:
+    """Boolean spot mask (nrot, detysize, detzsize) from the ground-truth grains."""
+    g = sample.geom
+    mask = np.zeros((g.nrot, g.detysize, g.detzsize), bool)
+    idx = sample.voxel_indices()[::stride]
+    gid = sample.grain_id[idx[:, 0] - 1, idx[:, 1] - 1, idx[:, 2] - 1]
+    pos = sample.vol.pos_of_index(idx)
+    Us = np.stack([G.quat_to_u(q) for q in sample.grain_q])[gid - 1]
+    for s in range(0, len(idx), chunk):
+        iw, iy, iz = landing_pixels(sample, pos[s:s + chunk], Us[s:s + chunk])
+        mask[iw, iy - 1, iz - 1] = True
+    return mask
+
+
+def distance_map(mask: np.ndarray) -> np.ndarray:
+    """bwdist per projection: Euclidean distance to the nearest spot pixel (float32).
+
+    Layout (nrot, dety, detz) in C order, which is the MATLAB (detz, dety, nrot)
+    column-major array flattened by ``reshape(proj_bin_bw,1,[])``.  A projection
+    with no spot pixel is all +Inf, as bwdist returns.
+    """
+    from scipy.ndimage import distance_transform_edt
+
+    out = np.empty(mask.shape, np.float32)
+    for i in range(mask.shape[0]):
+        if mask[i].any():
+            out[i] = distance_transform_edt(~mask[i]).astype(np.float32)
+        else:
+            out[i] = np.inf
+    return out

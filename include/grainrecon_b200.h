@@ -1,0 +1,184 @@
+/*
+ * grainrecon_b200.h -- C ABI of the B200 completeness scorer / grain grower.
+ *
+ * Drop-in boundary for GrainRecon's CUDA MEX functions.  The three drop-in
+ * entries take exactly the arrays the MATLAB wrappers build (float32, matrices
+ * flattened row by row as reshape(M',1,9), the distance map flattened
+ * column-major as reshape(proj_bin_bw,1,[])) in the same order, and write the
+ * same output layout into a caller-owned buffer (host or device memory).
+ *
+ * Index base: voxel indices in rows6/rows5 and the CSR ranges are 1-based
+ * floats, as in the reference.  Every function returns a GRC_* status; no
+ * exception or abort crosses this boundary.  The message of the last failure
+ * is available from grc_last_error().  One context = one CUDA device + one
+ * stream; calls on one context are serialised by an internal mutex.
+ */
+#ifndef GRAINRECON_B200_H
+#define GRAINRECON_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GRC_OK 0
+#define GRC_EINVAL 1     /* bad argument (NULL, size, NaN in the map, ...) */
+#define GRC_ECAPACITY 2  /* a size beyond a documented limit */
+#define GRC_ECUDA 3      /* a CUDA runtime error (message says which) */
+#define GRC_ETIMEOUT 4   /* a device-side wait gave up (bounded spin) */
+#define GRC_ENOMASK 5    /* no distance map resident and none passed */
+
+/* Documented limits. */
+#define GRC_MAX_NHKL 128
+#define GRC_MAX_NROT 1800
+
+typedef struct grc_ctx grc_ctx;
+
+/* ---- context ------------------------------------------------------------ */
+int grc_ctx_create(grc_ctx **out, int device);
+int grc_ctx_destroy(grc_ctx *ctx);
+const char *grc_last_error(const grc_ctx *ctx);
+/* The context's cudaStream_t (as void*), for callers that enqueue their own work. */
+void *grc_ctx_stream(grc_ctx *ctx);
+int grc_sync(grc_ctx *ctx);
+
+/*
+ * Options the MEX argument list does not carry.  The reference GPU kernels
+ * receive neither dety0/detz0 nor minEucDis; the defaults here are the values
+ * the reference uses when it re-checks GPU results on the CPU
+ * (revise_all_unindexed_voxel_cuda.m:41-42): dety0 = detysize/2+0.5,
+ * detz0 = detzsize/2+0.5, hit when dis <= 0.5 pixel.  Pass NaN to keep a default.
+ */
+int grc_set_options(grc_ctx *ctx, double dety0, double detz0, double hit_threshold_px);
+
+/*
+ * Make a distance map resident on the device (replaces the per-call upload of
+ * ForwardCalc_OR_space_comp_cuda.m:22 / grow_indexed_region_cuda.m:88).
+ * proj_bin_bw: host float32, detzsize*detysize*nrot values, column-major
+ * (detz fastest).  The map is rank-coded on the device (16- or 32-bit codes)
+ * so the median is exact; NaN values are rejected.
+ */
+int grc_upload_masks(grc_ctx *ctx, const float *proj_bin_bw, int64_t detzsize, int64_t detysize, int64_t nrot);
+/* Same, from device memory (float32, same layout). */
+int grc_upload_masks_device(grc_ctx *ctx, const float *d_proj_bin_bw, int64_t detzsize, int64_t detysize,
+                            int64_t nrot);
+
+/*
+ * Geometry shared by all scorer calls: S, B, RotDet (9 floats, row-major),
+ * hkl (3*nhkl floats), rot_angles (nrot floats, degrees) and the 20-float
+ * param vector [nhkl nrot Lsam2sou Lsam2det P0y P0z dety00 detz00 pixelysize
+ * pixelzsize detysize detzsize BeamStopY(1:2) BeamStopZ(1:2) thetamax
+ * lambda_min lambda_max RotAxisOffset] (ForwardCalc_OR_space_comp_cuda.m:25-27).
+ */
+int grc_set_geometry(grc_ctx *ctx, const float *S, const float *B, const float *hkl, const float *rot_angles,
+                     const float *RotDet, const float *param);
+
+/* ---- drop-in entries (host buffers in, caller-owned output) ------------- */
+
+/*
+ * Replaces cuda_forward_comp(pos, q, S, B, hkl, proj_bin_bw, rot_angles,
+ * RotDet, param) called at ForwardCalc_OR_space_comp_cuda.m:32-33 (also
+ * fit_OR_constrain_with_local_comp_cuda.m:47, forward_calc_gridding_OR.m:17).
+ * pos: 3 floats [mm]; q: 4*n_q floats [q0 q1 q2 q3] per orientation.
+ * out: 4*n_q floats [Nr_simu Nr_intersect completeness dis_median] per
+ * orientation (completeness = NaN when Nr_simu = 0; dis_median = 2000 when
+ * nothing is simulated).  proj_bin_bw may be NULL when a map is resident;
+ * when non-NULL it is uploaded first (the reference's per-call behaviour).
+ * No nrot*nhkl capacity limit (the reference stops at 181*80).
+ */
+int grc_forward_comp(grc_ctx *ctx, const float *pos, const float *q, int64_t n_q, const float *S, const float *B,
+                     const float *hkl, const float *proj_bin_bw, const float *rot_angles, const float *RotDet,
+                     const float *param, float *out);
+
+/*
+ * Replaces cuda_grow_indexed_region(rows6, U, S, B, hkl, proj_bin_bw,
+ * rot_angles, RotDet, param, param1) called at grow_indexed_region_cuda.m:105-107
+ * and Forward_calc_comp_allvoxel_cuda.m:57-59.
+ * rows6: 6*m floats [x y z I mask DisMedian] (x,y,z 1-based voxel indices);
+ * U: 9 floats row-major; param1: 14 floats [RecVolumePixel(:,1)'(3) simap
+ * VoxSize Center'(3) Dimension(3) seed_comp drop_off maxDmedian].
+ * out: 7*m floats [x y z Nr_simu Nr_intersect dis_median growth_flag].  Every
+ * row is scored; growth_flag = 1 when mask > 0 and C > I and dis_median <=
+ * min(DisMedian, maxDmedian) and C >= seed_comp*(1-drop_off)
+ * (grow_indexed_region_parallel.m:78-88 without the Ninter clause, which needs
+ * a column the MEX rows do not carry).
+ */
+int grc_grow_indexed_region(grc_ctx *ctx, const float *rows6, int64_t m, const float *U, const float *S,
+                            const float *B, const float *hkl, const float *proj_bin_bw, const float *rot_angles,
+                            const float *RotDet, const float *param, const float *param1, float *out);
+
+/*
+ * Replaces cuda_forward_comp_compete(rows5, id_neigb_all, Euler, S, B, hkl,
+ * proj_bin_bw, rot_angles, RotDet, param, param1) called at
+ * grow_unindexed_compete_comp_cuda.m:39-41.  rows5: 5*m floats [x y z first
+ * last], first/last a 1-based inclusive range into id_neigb (n_neigb floats,
+ * 1-based grain ids); euler: 3*n_grain floats (degrees, Bunge ZXZ); param1:
+ * the first 11 floats of the grow param1.  out: 8*m floats [row phi1 PHI phi2
+ * GrainId completeness Nr_intersect dis_median] of the first candidate with the
+ * largest completeness (NaN ignored); a row without candidates gives
+ * [row 0 0 0 0 0 0 2000].
+ */
+int grc_forward_comp_compete(grc_ctx *ctx, const float *rows5, int64_t m, const float *id_neigb, int64_t n_neigb,
+                             const float *euler, int64_t n_grain, const float *S, const float *B, const float *hkl,
+                             const float *proj_bin_bw, const float *rot_angles, const float *RotDet,
+                             const float *param, const float *param1, float *out);
+
+/* ---- device-resident entries (enqueue on the context stream, no sync) --- */
+
+/*
+ * Seeding batch: every voxel of d_pos (3*n_vox floats, mm) against every
+ * orientation of d_q (4*n_q floats).  d_out: 4*n_vox*n_q floats, voxel-major,
+ * same per-trial layout as grc_forward_comp.  Geometry and map must be set.
+ */
+int grc_forward_comp_device(grc_ctx *ctx, const float *d_pos, int64_t n_vox, const float *d_q, int64_t n_q,
+                            float *d_out);
+
+/* Grow on device buffers: d_rows6 (6*m), host U[9] and param1[14], d_out (7*m). */
+int grc_grow_device(grc_ctx *ctx, const float *d_rows6, int64_t m, const float *U, const float *param1,
+                    float *d_out);
+
+/*
+ * Batched grow / compete on a device CSR work list: voxel i (d_rows5 row, 1-based
+ * indices) scores candidates id_neigb[first-1 .. last-1] (grain ids into d_euler).
+ * d_out: 8*m floats as grc_forward_comp_compete.  When d_trial_out is non-NULL it
+ * also receives 4 floats [Nr_simu Nr_intersect C dis_median] per candidate, in
+ * CSR order.
+ */
+int grc_compete_device(grc_ctx *ctx, const float *d_rows5, int64_t m, const float *d_id_neigb, int64_t n_neigb,
+                       const float *d_euler, int64_t n_grain, const float *param1, float *d_out,
+                       float *d_trial_out);
+
+/* Statistics of the last scorer launch on this context. */
+typedef struct {
+    int64_t trials;          /* (voxel, orientation) pairs scored */
+    int64_t refined;         /* trials whose median needed the exact refine pass */
+    int64_t kernel_launches; /* kernels enqueued by the call */
+    double score_ms;         /* device time of the scoring kernel (CUDA events), 0 if not timed */
+} grc_stats;
+int grc_last_stats(grc_ctx *ctx, grc_stats *out);
+/* 1 = record CUDA events around the scoring kernel of each call (for benchmarks). */
+int grc_set_timing(grc_ctx *ctx, int enable);
+
+/* Counts of selected reflections per trial are exact; this reports the codes of the
+ * resident map: number of distinct values, code width in bits. */
+int grc_mask_info(grc_ctx *ctx, int64_t *n_distinct, int *code_bits, int64_t *detzsize, int64_t *detysize,
+                  int64_t *nrot);
+
+/*
+ * Synthetic-data helpers (device-side mask preparation).
+ * grc_simulate_spots: every voxel (d_pos, 3*n floats mm) with its orientation
+ * (d_U, 9*n floats row-major) lands its selected reflections; the landing
+ * pixels are OR-ed into d_mask (uint8, nrot*detysize*detzsize, detz fastest).
+ * grc_edt: exact Euclidean distance transform per projection (bwdist
+ * semantics: distance to the nearest nonzero mask pixel, +Inf for a projection
+ * with none) into d_map (float32, same layout).
+ */
+int grc_simulate_spots(grc_ctx *ctx, const float *d_pos, const float *d_U, int64_t n, uint8_t *d_mask);
+int grc_edt(grc_ctx *ctx, const uint8_t *d_mask, int64_t detzsize, int64_t detysize, int64_t nrot, float *d_map);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
