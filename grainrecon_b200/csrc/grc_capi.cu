@@ -41,7 +41,8 @@ struct grc_ctx {
     grc::MapCodes mc{};
     int64_t mz = 0, my = 0, mrot = 0;
     std::vector<float> h_vals;
-    DevBuf rot_cs, hkl, pos, U, res, in1, in2, in3, out, items, torient, counts, offsets, tmp, counter, p1, bad;
+    DevBuf geo_dev, rot_cs, hkl, pos, U, res, in1, in2, in3, out, items, torient, counts, offsets, tmp, counter, p1, bad;
+    grc::Geo *geo_pinned = nullptr;  // staging of the per-launch geometry copy
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     bool timing = false;
     bool timed_last = false;
@@ -113,6 +114,15 @@ void apply_options(grc_ctx *ctx) {
     grc::Geo &g = ctx->geo;
     g.dety0 = std::isnan(ctx->opt_dety0) ? g.detysize / 2.0 + 0.5 : ctx->opt_dety0;
     g.detz0 = std::isnan(ctx->opt_detz0) ? g.detzsize / 2.0 + 0.5 : ctx->opt_detz0;
+    for (int i = 0; i < 9; ++i) g.Rf[i] = (float)g.R[i];
+    g.dety0f = (float)g.dety0;
+    g.detz0f = (float)g.detz0;
+    g.rpxyf = (float)(1.0 / g.pxy);
+    g.rpxzf = (float)(1.0 / g.pxz);
+    g.bsy0f = (float)g.bsy0;
+    g.bsy1f = (float)g.bsy1;
+    g.bsz0f = (float)g.bsz0;
+    g.bsz1f = (float)g.bsz1;
     refresh_hit(ctx);
 }
 
@@ -248,6 +258,7 @@ int check_ready(grc_ctx *ctx) {
 
 grc::ScoreBufs bufs(grc_ctx *ctx) {
     grc::ScoreBufs b{};
+    b.geo = (const grc::Geo *)ctx->geo_dev.p;
     b.rot_cs = (const double2 *)ctx->rot_cs.p;
     b.hkl = (const double *)ctx->hkl.p;
     b.vpos = (const double *)ctx->pos.p;
@@ -259,8 +270,17 @@ grc::ScoreBufs bufs(grc_ctx *ctx) {
     return b;
 }
 
+int stage_geo(grc_ctx *ctx) {
+    TRY(ensure(ctx, ctx->geo_dev, sizeof(grc::Geo)));
+    CU(cudaStreamSynchronize(ctx->stream));  // the pinned staging copy may still be read by an earlier call
+    *ctx->geo_pinned = ctx->geo;
+    CU(cudaMemcpyAsync(ctx->geo_dev.p, ctx->geo_pinned, sizeof(grc::Geo), cudaMemcpyHostToDevice, ctx->stream));
+    return GRC_OK;
+}
+
 int run_score(grc_ctx *ctx, const grc::Work &w, int64_t n_trials) {
     TRY(ensure(ctx, ctx->counter, 8 * sizeof(int)));
+    TRY(stage_geo(ctx));
     int launches = 0;
     cudaError_t e = grc::launch_score(ctx->geo, bufs(ctx), w, ctx->num_sms, ctx->stream,
                                       ctx->timing ? ctx->ev0 : nullptr, ctx->timing ? ctx->ev1 : nullptr,
@@ -434,6 +454,7 @@ int grc_ctx_create(grc_ctx **out, int device) {
     }
     ctx->num_sms = p.multiProcessorCount;
     if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaHostAlloc((void **)&ctx->geo_pinned, sizeof(grc::Geo), cudaHostAllocDefault) != cudaSuccess ||
         cudaEventCreate(&ctx->ev0) != cudaSuccess || cudaEventCreate(&ctx->ev1) != cudaSuccess) {
         delete ctx;
         return GRC_ECUDA;
@@ -447,7 +468,8 @@ int grc_ctx_destroy(grc_ctx *ctx) {
     {
         Lock l(ctx);
         cudaStreamSynchronize(ctx->stream);
-        DevBuf *all[] = {&ctx->rot_cs, &ctx->hkl, &ctx->pos, &ctx->U, &ctx->res, &ctx->in1, &ctx->in2,
+        cudaFreeHost(ctx->geo_pinned);
+        DevBuf *all[] = {&ctx->geo_dev, &ctx->rot_cs, &ctx->hkl, &ctx->pos, &ctx->U, &ctx->res, &ctx->in1, &ctx->in2,
                          &ctx->in3, &ctx->out, &ctx->items, &ctx->torient, &ctx->counts, &ctx->offsets,
                          &ctx->tmp, &ctx->counter, &ctx->p1, &ctx->bad};
         for (DevBuf *b : all) cudaFree(b->p);
@@ -666,6 +688,7 @@ int grc_simulate_spots(grc_ctx *ctx, const float *d_pos, const float *d_U, int64
     TRY(ensure(ctx, ctx->counter, 8 * sizeof(int)));
     CU(grc::launch_f9_to_u(d_U, n, (double *)ctx->U.p, ctx->stream));
     CU(grc::launch_pos_f3(d_pos, n, (double *)ctx->pos.p, ctx->stream));
+    TRY(stage_geo(ctx));
     grc::Work w{};
     w.n_or = 1;
     w.chunk = 1;

@@ -12,6 +12,7 @@ constexpr int kHistBins = 1024;
 constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
 constexpr int kQueueCap = 32 + 32 * 4;  // one 32-item batch in flight + 4 reflection slots per lane
+constexpr int kFallbackCap = 64;       // ambiguous items awaiting the FP64 path (< 32 + 32)
 
 // Scalar geometry of one scorer call, FP64 (promoted from the float32 MEX
 // arguments).  Field names follow forward_comp.m.
@@ -22,6 +23,10 @@ struct Geo {
     double cbmax;            // cos((90+4*thetamax) deg), or -2 when that angle is >= 180 deg
     double bsy0, bsy1, bsz0, bsz1;
     double S[9], B[9], R[9]; // row-major
+    // FP32 copies for the fast landing chain
+    float Rf[9];
+    float dety0f, detz0f, rpxyf, rpxzf;
+    float bsy0f, bsy1f, bsz0f, bsz1f;
     int nhkl, nrot, detysize, detzsize;
     uint32_t n_hit;          // codes [0, n_hit) are "dis <= threshold"
     uint32_t n_vals;         // entries of the code -> value table
@@ -52,6 +57,7 @@ struct Work {
 };
 
 struct ScoreBufs {
+    const Geo *geo;           // device copy of the kernel's Geo (read by the exact FP64 path)
     const double2 *rot_cs;    // cos/sin of every omega
     const double *hkl;        // 3*nhkl
     const double *vpos;       // 3 per voxel [mm]

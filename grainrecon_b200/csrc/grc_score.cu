@@ -30,58 +30,87 @@
 
 #include "grc_internal.h"
 
+// Resident CTAs per SM the scoring kernel is compiled for (register budget).
+#ifndef GRC_MIN_BLOCKS
+#define GRC_MIN_BLOCKS 4
+#endif
+
 namespace grc {
 namespace {
 
 constexpr unsigned kFull = 0xffffffffu;
 
-struct __align__(16) OmegaRow {
+// FP64 constants of one (voxel, omega) pair, forward_comp.m:17-26,42,51.
+struct OmegaRow {
     double kx, ky, kz, L2;  // unit incident direction (lab), L2 of forward_comp.m:42
     double ax, ay, az, num; // center - SamposW; t-numerator of forward_comp.m:51
     double r2d, r3d, c, s;  // RotDet(:,2).d, RotDet(:,3).d with d = SamposW - D0; cos/sin omega
 };
-static_assert(sizeof(OmegaRow) == 96, "OmegaRow layout");
+
+// The same row rounded to FP32 plus k_w = Omega^T k_in (prefilter), kept in shared memory.
+struct __align__(16) RowF {
+    float kx, ky, kz, L2;
+    float ax, ay, az, num;
+    float r2d, r3d, c, s;
+    float wx, wy, wz, pad;
+};
+static_assert(sizeof(RowF) == 64, "RowF layout");
+
+// Pixel-rounding ambiguity band of the FP32 landing chain.  Its error against the
+// FP64 chain stays below 1.4e-3 px on the 1024^2 / 2048^2 geometries (measured over
+// 3.4e5 landings); landings closer than this to a half-pixel boundary are recomputed
+// in FP64, so every decision equals the FP64 one.
+constexpr float kAmbigPx = 0.0125f;
 
 __device__ __forceinline__ size_t align16(size_t x) { return (x + 15) & ~size_t(15); }
 
-// forward_comp.m:17-26,42,51 for one voxel and every omega (FP64).
-__device__ void build_rows(const Geo &g, const double2 *__restrict__ rot_cs, const double *__restrict__ vp,
-                           OmegaRow *trow, float4 *kw) {
+__device__ __forceinline__ OmegaRow omega_row(const Geo &g, const double2 cs, const double *__restrict__ vp) {
     const double px = vp[0], py = vp[1] - g.rao, pz = vp[2];
     const double spx = g.S[0] * px + g.S[1] * py + g.S[2] * pz;
     const double spy = g.S[3] * px + g.S[4] * py + g.S[5] * pz;
     const double spz = g.S[6] * px + g.S[7] * py + g.S[8] * pz;
     const double L = g.lss + g.lsd;
+    const double c = cs.x, s = cs.y;
+    const double swx = c * spx - s * spy, swy = s * spx + c * spy, swz = spz;
+    const double gx = g.lss + swx, gy = swy - g.p0y + g.rao, gz = swz - g.p0z;
+    const double ngp = sqrt(gx * gx + gy * gy + gz * gz);
+    OmegaRow r;
+    r.kx = gx / ngp;
+    r.ky = gy / ngp;
+    r.kz = gz / ngp;
+    r.L2 = (g.lsd - swx) * ngp / gx;  // (Lsd - SamposW_x) / cos(alpha)
+    r.ax = g.lsd - swx;
+    r.ay = gy * L / gx - swy;
+    r.az = gz * L / gx - swz;
+    const double dx = swx - g.lsd, dy = swy - g.dety00 + g.rao, dz = swz - g.detz00;
+    r.num = -(g.R[0] * dx + g.R[3] * dy + g.R[6] * dz);
+    r.r2d = g.R[1] * dx + g.R[4] * dy + g.R[7] * dz;
+    r.r3d = g.R[2] * dx + g.R[5] * dy + g.R[8] * dz;
+    r.c = c;
+    r.s = s;
+    return r;
+}
+
+// Omega table of one voxel in shared memory (all threads of the CTA).
+__device__ void build_rows(const Geo &g, const double2 *__restrict__ rot_cs, const double *__restrict__ vp,
+                           RowF *rows) {
     for (int iw = threadIdx.x; iw < g.nrot; iw += blockDim.x) {
-        const double2 cs = rot_cs[iw];
-        const double c = cs.x, s = cs.y;
-        const double swx = c * spx - s * spy, swy = s * spx + c * spy, swz = spz;
-        const double gx = g.lss + swx, gy = swy - g.p0y + g.rao, gz = swz - g.p0z;
-        const double ngp = sqrt(gx * gx + gy * gy + gz * gz);
-        OmegaRow r;
-        r.kx = gx / ngp;
-        r.ky = gy / ngp;
-        r.kz = gz / ngp;
-        r.L2 = (g.lsd - swx) * ngp / gx;  // (Lsd - SamposW_x) / cos(alpha)
-        r.ax = g.lsd - swx;
-        r.ay = gy * L / gx - swy;
-        r.az = gz * L / gx - swz;
-        const double dx = swx - g.lsd, dy = swy - g.dety00 + g.rao, dz = swz - g.detz00;
-        r.num = -(g.R[0] * dx + g.R[3] * dy + g.R[6] * dz);
-        r.r2d = g.R[1] * dx + g.R[4] * dy + g.R[7] * dz;
-        r.r3d = g.R[2] * dx + g.R[5] * dy + g.R[8] * dz;
-        r.c = c;
-        r.s = s;
-        trow[iw] = r;
-        kw[iw] = make_float4((float)(c * r.kx + s * r.ky), (float)(-s * r.kx + c * r.ky), (float)r.kz, 0.f);
+        const OmegaRow r = omega_row(g, rot_cs[iw], vp);
+        RowF f;
+        f.kx = (float)r.kx; f.ky = (float)r.ky; f.kz = (float)r.kz; f.L2 = (float)r.L2;
+        f.ax = (float)r.ax; f.ay = (float)r.ay; f.az = (float)r.az; f.num = (float)r.num;
+        f.r2d = (float)r.r2d; f.r3d = (float)r.r3d; f.c = (float)r.c; f.s = (float)r.s;
+        f.wx = (float)(r.c * r.kx + r.s * r.ky);
+        f.wy = (float)(-r.s * r.kx + r.c * r.ky);
+        f.wz = (float)r.kz;
+        f.pad = 0.f;
+        rows[iw] = f;
     }
 }
 
-// Gw = S*U*B*h and |Gw| for every reflection of one trial (forward_comp.m:15-16).
-__device__ void build_gw(const Geo &g, const double *__restrict__ hkl, const double *__restrict__ U, double *gw) {
-    const int ih = threadIdx.x;
-    if (ih >= g.nhkl) return;
-    double SU[9], SUB[9];
+// SUB = S*U*B (FP64, 9 values) of one trial.
+__device__ __forceinline__ void sub_matrix(const Geo &g, const double *__restrict__ U, double *SUB) {
+    double SU[9];
 #pragma unroll
     for (int i = 0; i < 3; ++i)
 #pragma unroll
@@ -92,24 +121,35 @@ __device__ void build_gw(const Geo &g, const double *__restrict__ hkl, const dou
 #pragma unroll
         for (int j = 0; j < 3; ++j)
             SUB[3 * i + j] = SU[3 * i] * g.B[j] + SU[3 * i + 1] * g.B[3 + j] + SU[3 * i + 2] * g.B[6 + j];
+}
+
+// Gw = S*U*B*h and |Gw| (forward_comp.m:15-16): FP32 table in shared memory plus the
+// FP64 SUB matrix kept for the exact recomputation of ambiguous reflections.
+__device__ __forceinline__ float4 window_of(const Geo &g, float G_f);
+
+__device__ void build_gw(const Geo &g, const double *__restrict__ hkl, const double *__restrict__ U, float4 *gw,
+                         float4 *win, double *sub) {
+    const int ih = threadIdx.x;
+    if (ih >= g.nhkl) return;
+    double SUB[9];
+    sub_matrix(g, U, SUB);
+    if (ih < 9) sub[ih] = SUB[ih];
     const double h = hkl[3 * ih], k = hkl[3 * ih + 1], l = hkl[3 * ih + 2];
     const double x = SUB[0] * h + SUB[1] * k + SUB[2] * l;
     const double y = SUB[3] * h + SUB[4] * k + SUB[5] * l;
     const double z = SUB[6] * h + SUB[7] * k + SUB[8] * l;
-    gw[4 * ih] = x;
-    gw[4 * ih + 1] = y;
-    gw[4 * ih + 2] = z;
-    gw[4 * ih + 3] = sqrt(x * x + y * y + z * z);
+    const float G = (float)sqrt(x * x + y * y + z * z);
+    gw[ih] = make_float4((float)x, (float)y, (float)z, G);
+    win[ih] = window_of(g, G);
 }
 
-// Exact FP64 evaluation of one reflection (omega row iw, reflection ih):
-// returns the linear map index of its pixel, or -1 when select3 of
-// forward_comp.m:61-65 rejects it.  Algebraic form of forward_comp.m:28-59:
-// sin(theta) = -cos(beta), cos(theta) = sin(beta), sin(phiy) expanded, and the
-// ray/plane intersection without normalising K_out.
-__device__ __forceinline__ int64_t landing_index(const Geo &g, const OmegaRow &r, const double *gw, int iw,
-                                                 int ih) {
-    const double gxw = gw[4 * ih], gyw = gw[4 * ih + 1], gzw = gw[4 * ih + 2], G = gw[4 * ih + 3];
+// Exact FP64 evaluation of one reflection: the linear map index of its pixel, or -1
+// when select3 of forward_comp.m:61-65 rejects it.  Algebraic form of
+// forward_comp.m:28-59: sin(theta) = -cos(beta), cos(theta) = sin(beta), sin(phiy)
+// expanded, and the ray/plane intersection without normalising K_out.
+__device__ __forceinline__ int64_t landing_fp64(const Geo &g, const OmegaRow &r, double gxw, double gyw,
+                                                double gzw, int iw) {
+    const double G = sqrt(gxw * gxw + gyw * gyw + gzw * gzw);
     const double Gtx = r.c * gxw - r.s * gyw, Gty = r.s * gxw + r.c * gyw, Gtz = gzw;
     const double x = (r.kx * Gtx + r.ky * Gty + r.kz * Gtz) / G;  // cos(beta)
     const double lam = 2.0 * (2.0 * CUDART_PI / G) * (-x);        // 2 d sin(theta)
@@ -133,6 +173,70 @@ __device__ __forceinline__ int64_t landing_index(const Geo &g, const OmegaRow &r
     const double ru = round(u), rv = round(v);
     if (ru >= g.bsy0 && ru <= g.bsy1 && rv >= g.bsz0 && rv <= g.bsz1) return -1;
     return (int64_t)iw * g.plane + (int64_t)(ru - 1.0) * g.detzsize + (int64_t)(rv - 1.0);
+}
+
+// The exact path for one ambiguous item: FP64 omega row and Gw rebuilt from the inputs.
+// Kept out of line (rarely taken) and reads the geometry from its global-memory copy.
+__device__ __noinline__ int64_t landing_exact(const Geo *__restrict__ gd, const double2 *__restrict__ rot_cs,
+                                              const double *__restrict__ vp, const double *__restrict__ hkl,
+                                              const double *sub, int iw, int ih) {
+    const Geo &g = *gd;
+    const OmegaRow r = omega_row(g, rot_cs[iw], vp);
+    const double h = hkl[3 * ih], k = hkl[3 * ih + 1], l = hkl[3 * ih + 2];
+    const double x = sub[0] * h + sub[1] * k + sub[2] * l;
+    const double y = sub[3] * h + sub[4] * k + sub[5] * l;
+    const double z = sub[6] * h + sub[7] * k + sub[8] * l;
+    return landing_fp64(g, r, x, y, z, iw);
+}
+
+// Window thresholds of one reflection on t = -(k_w . Gw) = |G|^2 lambda / (4 pi):
+// lambda in (lambda_min, lambda_max) and cos(beta) > cos(beta_max).  Returned as
+// (lo, hi) = the interval widened by the FP32 margin (prefilter) and (lo_in, hi_in)
+// = narrowed by it (inside, the FP32 decision is certain).
+__device__ __forceinline__ float4 window_of(const Geo &g, float G_f) {
+    const double G = G_f, G2 = G * G;
+    const double inv4pi = 0.25 / CUDART_PI;
+    double lo = g.lmin * G2 * inv4pi, hi = g.lmax * G2 * inv4pi;
+    if (g.cbmax > -1.0) hi = fmin(hi, -g.cbmax * G);
+    lo = fmax(lo, 0.0);
+    const double m = 1e-5 * G;  // >> FP32 error of k_w . G (~4e-7 |G|)
+    return make_float4((float)(lo - m), (float)(hi + m), (float)(lo + m), (float)(hi - m));
+}
+
+// FP32 landing chain (same algebra as landing_fp64).  Returns the map index, -1 for a
+// certain rejection, or -2 when the item lies within the ambiguity band of a
+// decision boundary and must be decided by landing_exact.
+__device__ __forceinline__ int64_t landing_fp32(const Geo &g, const RowF &r, const float4 gw, float lo_in, float hi_in,
+                                                int iw) {
+    const float Gtx = r.c * gw.x - r.s * gw.y, Gty = r.s * gw.x + r.c * gw.y, Gtz = gw.z;
+    const float dot = r.kx * Gtx + r.ky * Gty + r.kz * Gtz;
+    const float t = -dot;
+    if (!(t > lo_in && t < hi_in)) return -2;  // near the wavelength / Bragg-angle window edge
+    const float x = dot / gw.w;
+    const float st = -x, ct = sqrtf(1.0f - x * x);
+    const float s2 = 2.0f * st * ct, c2 = 1.0f - 2.0f * st * st;
+    const float rk = rsqrtf(Gty * Gty + Gtz * Gtz);
+    const float gy = Gty * rk, gz = Gtz * rk;
+    const float cphx = gy * r.ky + gz * r.kz;
+    const float sphx = sqrtf(fmaxf(0.0f, 1.0f - cphx * cphx));
+    const float sphy = sphx * c2 - cphx * s2;
+    const float diff = r.L2 * s2 / sphy;
+    const float Kx = r.ax, Ky = r.ay + diff * gy, Kz = r.az + diff * gz;
+    const float nK = g.Rf[0] * Kx + g.Rf[3] * Ky + g.Rf[6] * Kz;
+    const float f = r.num / nK;
+    const float y2 = f * (g.Rf[1] * Kx + g.Rf[4] * Ky + g.Rf[7] * Kz) + r.r2d;
+    const float z2 = f * (g.Rf[2] * Kx + g.Rf[5] * Ky + g.Rf[8] * Kz) + r.r3d;
+    const float u = g.dety0f - y2 * g.rpxyf, v = g.detz0f - z2 * g.rpxzf;
+    if (!(fabsf(u) < 1e6f && fabsf(v) < 1e6f)) {
+        // far off the detector (or NaN): certain rejection only for finite values
+        return (isfinite(u) && isfinite(v)) ? -1 : -2;
+    }
+    const float fu = u - floorf(u), fv = v - floorf(v);
+    if (fabsf(fu - 0.5f) < kAmbigPx || fabsf(fv - 0.5f) < kAmbigPx) return -2;
+    const float ru = floorf(u + 0.5f), rv = floorf(v + 0.5f);  // exact away from the half-pixel band
+    if (!(ru >= 1.0f && ru <= (float)g.detysize && rv >= 1.0f && rv <= (float)g.detzsize)) return -1;
+    if (ru >= g.bsy0f && ru <= g.bsy1f && rv >= g.bsz0f && rv <= g.bsz1f) return -1;
+    return (int64_t)iw * g.plane + (int64_t)(ru - 1.0f) * g.detzsize + (int64_t)(rv - 1.0f);
 }
 
 // Counts + histogram of codes below kHistBins (scoring pass).
@@ -183,40 +287,70 @@ struct MarkSink {
     }
 };
 
+// Per-trial context handed to run_trial.
+struct TrialCtx {
+    const RowF *rows;        // shared: omega table of the voxel
+    const float4 *gw;        // shared: FP32 Gw table of the trial
+    const float4 *win;       // shared: window thresholds per reflection (window_of)
+    const double *sub;       // shared: FP64 S*U*B of the trial
+    const double *vp;        // global: voxel position (FP64)
+    const double2 *rot_cs;   // global
+    const double *hkl;       // global
+    const Geo *geo;          // global copy of the geometry (exact path)
+    uint32_t *wq;            // shared: this warp's candidate queue (kQueueCap)
+    uint32_t *fq;            // shared: this warp's ambiguous-item queue (kFallbackCap)
+};
+
 // Walk every (omega, reflection) of one trial; the sink sees each selected pixel.
 template <int HPL, typename Sink>
-__device__ __forceinline__ void run_trial(const Geo &g, const OmegaRow *trow, const float4 *kw, const double *gw,
-                                          uint32_t *wq, Sink &sink) {
+__device__ __forceinline__ void run_trial(const Geo &g, const TrialCtx &tc, Sink &sink) {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const unsigned lt = (1u << lane) - 1u;
     float pfx[HPL], pfy[HPL], pfz[HPL], plo[HPL], phi[HPL];
-    const double inv4pi = 0.25 / CUDART_PI;
 #pragma unroll
     for (int j = 0; j < HPL; ++j) {
         const int ih = lane + 32 * j;
         if (ih < g.nhkl) {
-            const double G = gw[4 * ih + 3], G2 = G * G;
-            double lo = g.lmin * G2 * inv4pi, hi = g.lmax * G2 * inv4pi;
-            if (g.cbmax > -1.0) hi = fmin(hi, -g.cbmax * G);
-            lo = fmax(lo, 0.0);
-            const double m = 1e-5 * G;  // >> FP32 error of k_w . G (~4e-7 |G|)
-            plo[j] = (float)(lo - m);
-            phi[j] = (float)(hi + m);
-            pfx[j] = (float)gw[4 * ih];
-            pfy[j] = (float)gw[4 * ih + 1];
-            pfz[j] = (float)gw[4 * ih + 2];
+            const float4 gv = tc.gw[ih];
+            const float4 w = tc.win[ih];
+            plo[j] = w.x;
+            phi[j] = w.y;
+            pfx[j] = gv.x;
+            pfy[j] = gv.y;
+            pfz[j] = gv.z;
         } else {
             plo[j] = CUDART_INF_F;
             phi[j] = -CUDART_INF_F;
             pfx[j] = pfy[j] = pfz[j] = 0.f;
         }
     }
-    int qn = 0;
+    uint32_t *wq = tc.wq, *fq = tc.fq;
+    int qn = 0, fn = 0;
+    auto fast = [&](uint32_t item, bool valid) {
+        const int iwi = (int)(item >> 8), ihi = (int)(item & 255u);
+        int64_t r = -1;
+        if (valid) {
+            const float4 gv = tc.gw[ihi];
+            const float4 w = tc.win[ihi];
+            r = landing_fp32(g, tc.rows[iwi], gv, w.z, w.w, iwi);
+        }
+        const bool amb = r == -2;
+        const unsigned m = __ballot_sync(kFull, amb);
+        if (amb) fq[fn + __popc(m & lt)] = item;
+        fn += __popc(m);
+        sink.on(r >= 0 ? r : -1);
+    };
+    auto exact = [&](uint32_t item, bool valid) {
+        int64_t r = -1;
+        if (valid) r = landing_exact(tc.geo, tc.rot_cs, tc.vp, tc.hkl, tc.sub, (int)(item >> 8), (int)(item & 255u));
+        sink.on(r);
+    };
     for (int iw = warp; iw < g.nrot; iw += kWarps) {
-        const float4 k = kw[iw];
+        const RowF &row = tc.rows[iw];
+        const float kx = row.wx, ky = row.wy, kz = row.wz;
 #pragma unroll
         for (int j = 0; j < HPL; ++j) {
-            const float t = -fmaf(k.x, pfx[j], fmaf(k.y, pfy[j], k.z * pfz[j]));
+            const float t = -fmaf(kx, pfx[j], fmaf(ky, pfy[j], kz * pfz[j]));
             const bool pass = (t > plo[j]) && (t < phi[j]);
             const unsigned m = __ballot_sync(kFull, pass);
             if (pass) wq[qn + __popc(m & lt)] = ((uint32_t)iw << 8) | (uint32_t)(lane + 32 * j);
@@ -227,46 +361,63 @@ __device__ __forceinline__ void run_trial(const Geo &g, const OmegaRow *trow, co
             qn -= 32;
             const uint32_t item = wq[qn + lane];
             __syncwarp();
-            const int iwi = (int)(item >> 8), ihi = (int)(item & 255u);
-            sink.on(landing_index(g, trow[iwi], gw, iwi, ihi));
+            fast(item, true);
+            __syncwarp();
+            while (fn >= 32) {
+                fn -= 32;
+                const uint32_t it2 = fq[fn + lane];
+                __syncwarp();
+                exact(it2, true);
+                __syncwarp();
+            }
         }
     }
     if (qn > 0) {
         const bool valid = lane < qn;
         const uint32_t item = valid ? wq[lane] : 0u;
         __syncwarp();
-        int64_t idx = -1;
-        if (valid) {
-            const int iwi = (int)(item >> 8), ihi = (int)(item & 255u);
-            idx = landing_index(g, trow[iwi], gw, iwi, ihi);
-        }
-        sink.on(idx);
+        fast(item, valid);
+        __syncwarp();
     }
-    __syncwarp();
+    while (fn > 0) {
+        const int take = fn < 32 ? fn : 32;
+        fn -= take;
+        const bool valid = lane < take;
+        const uint32_t item = valid ? fq[fn + lane] : 0u;
+        __syncwarp();
+        exact(item, valid);
+        __syncwarp();
+    }
 }
 
 struct Smem {
-    OmegaRow *trow;
-    float4 *kw;
-    double *gw;
+    RowF *rows;
+    float4 *gw;
+    float4 *win;
+    double *sub;
     uint32_t *h0, *h1;
     uint32_t *queue;
+    uint32_t *fqueue;
 };
 
 __device__ __forceinline__ Smem carve(unsigned char *base, const Geo &g, int nhist) {
     Smem s;
     size_t off = 0;
-    s.trow = (OmegaRow *)(base + off);
-    off = align16(off + sizeof(OmegaRow) * g.nrot);
-    s.kw = (float4 *)(base + off);
-    off = align16(off + sizeof(float4) * g.nrot);
-    s.gw = (double *)(base + off);
-    off = align16(off + sizeof(double) * 4 * g.nhkl);
+    s.rows = (RowF *)(base + off);
+    off = align16(off + sizeof(RowF) * g.nrot);
+    s.gw = (float4 *)(base + off);
+    off = align16(off + sizeof(float4) * g.nhkl);
+    s.win = (float4 *)(base + off);
+    off = align16(off + sizeof(float4) * g.nhkl);
+    s.sub = (double *)(base + off);
+    off = align16(off + sizeof(double) * 9);
     s.h0 = (uint32_t *)(base + off);
     off += sizeof(uint32_t) * kHistBins;
     s.h1 = nhist > 1 ? (uint32_t *)(base + off) : nullptr;
     off += nhist > 1 ? sizeof(uint32_t) * kHistBins : 0;
     s.queue = (uint32_t *)(base + off);
+    off += sizeof(uint32_t) * kWarps * kQueueCap;
+    s.fqueue = (uint32_t *)(base + off);
     return s;
 }
 
@@ -339,7 +490,7 @@ __device__ void find_two_ranks(const uint32_t *hist, int ra, int rb, int *s_code
 }
 
 template <int HPL, typename CodeT>
-__global__ void __launch_bounds__(kThreads, 2) score_kernel(Geo g, ScoreBufs b, Work w) {
+__global__ void __launch_bounds__(kThreads, GRC_MIN_BLOCKS) score_kernel(Geo g, ScoreBufs b, Work w) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const Smem sm = carve(smem_raw, g, 1);
     __shared__ int64_t s_item;
@@ -348,15 +499,17 @@ __global__ void __launch_bounds__(kThreads, 2) score_kernel(Geo g, ScoreBufs b, 
     __shared__ uint32_t s_wsum[kWarps];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     uint32_t *wq = sm.queue + warp * kQueueCap;
+    uint32_t *fq = sm.fqueue + warp * kFallbackCap;
     const CodeT *codes = (const CodeT *)b.codes;
     unsigned long long *counter = (unsigned long long *)b.work_counter;
     int64_t v, t0, t1;
     while (next_item(w, counter, &s_item, v, t0, t1)) {
         if (t0 >= t1) continue;
-        build_rows(g, b.rot_cs, b.vpos + 3 * v, sm.trow, sm.kw);
+        build_rows(g, b.rot_cs, b.vpos + 3 * v, sm.rows);
+        const TrialCtx tc{sm.rows, sm.gw, sm.win, sm.sub, b.vpos + 3 * v, b.rot_cs, b.hkl, b.geo, wq, fq};
         for (int64_t t = t0; t < t1; ++t) {
             const int64_t o = orient_of(w, t, v);
-            build_gw(g, b.hkl, b.U + 9 * o, sm.gw);
+            build_gw(g, b.hkl, b.U + 9 * o, sm.gw, sm.win, sm.sub);
             for (int i = threadIdx.x; i < kHistBins; i += kThreads) sm.h0[i] = 0;
             if (threadIdx.x == 0) {
                 s_simu = s_inter = s_over = 0;
@@ -364,7 +517,7 @@ __global__ void __launch_bounds__(kThreads, 2) score_kernel(Geo g, ScoreBufs b, 
             }
             __syncthreads();
             HistSink<CodeT> sink{codes, sm.h0, g.n_hit, 0, 0, 0};
-            run_trial<HPL>(g, sm.trow, sm.kw, sm.gw, wq, sink);
+            run_trial<HPL>(g, tc, sink);
             if (lane == 0) {
                 atomicAdd(&s_simu, sink.simu);
                 atomicAdd(&s_inter, sink.inter);
@@ -408,6 +561,7 @@ __global__ void __launch_bounds__(kThreads, 2) refine_kernel(Geo g, ScoreBufs b,
     __shared__ uint32_t s_pa, s_pb, s_ra, s_rb;
     const int warp = threadIdx.x >> 5;
     uint32_t *wq = sm.queue + warp * kQueueCap;
+    uint32_t *fq = sm.fqueue + warp * kFallbackCap;
     const CodeT *codes = (const CodeT *)b.codes;
     unsigned long long *counter = (unsigned long long *)(b.work_counter + 2);
     int64_t v, t0, t1;
@@ -418,12 +572,14 @@ __global__ void __launch_bounds__(kThreads, 2) refine_kernel(Geo g, ScoreBufs b,
             if (isnan(b.res[t].median)) s_any = 1;
         __syncthreads();
         if (!s_any) continue;
-        build_rows(g, b.rot_cs, b.vpos + 3 * v, sm.trow, sm.kw);
+        build_rows(g, b.rot_cs, b.vpos + 3 * v, sm.rows);
         __syncthreads();
+        const TrialCtx tc{sm.rows, sm.gw, sm.win, sm.sub, b.vpos + 3 * v, b.rot_cs, b.hkl, b.geo, wq, fq};
         for (int64_t t = t0; t < t1; ++t) {
             if (!isnan(b.res[t].median)) continue;  // uniform: every thread reads the same value
             const int64_t o = orient_of(w, t, v);
-            build_gw(g, b.hkl, b.U + 9 * o, sm.gw);
+            __syncthreads();
+            build_gw(g, b.hkl, b.U + 9 * o, sm.gw, sm.win, sm.sub);
             const int n = b.res[t].simu;
             if (threadIdx.x == 0) {
                 s_pa = s_pb = 0;
@@ -437,7 +593,7 @@ __global__ void __launch_bounds__(kThreads, 2) refine_kernel(Geo g, ScoreBufs b,
                 for (int i = threadIdx.x; i < kHistBins; i += kThreads) sm.h0[i] = sm.h1[i] = 0;
                 __syncthreads();
                 RadixSink<CodeT> sink{codes, sm.h0, sm.h1, s_pa, s_pb, pos, pos + width, (1u << width) - 1u};
-                run_trial<HPL>(g, sm.trow, sm.kw, sm.gw, wq, sink);
+                run_trial<HPL>(g, tc, sink);
                 __syncthreads();
                 if (threadIdx.x == 0) {
                     uint32_t cum = 0;
@@ -478,16 +634,18 @@ __global__ void __launch_bounds__(kThreads, 2) mark_kernel(Geo g, ScoreBufs b, W
     __shared__ int64_t s_item;
     const int warp = threadIdx.x >> 5;
     uint32_t *wq = sm.queue + warp * kQueueCap;
+    uint32_t *fq = sm.fqueue + warp * kFallbackCap;
     unsigned long long *counter = (unsigned long long *)b.work_counter;
     int64_t v, t0, t1;
     while (next_item(w, counter, &s_item, v, t0, t1)) {
         if (t0 >= t1) continue;
-        build_rows(g, b.rot_cs, b.vpos + 3 * v, sm.trow, sm.kw);
+        build_rows(g, b.rot_cs, b.vpos + 3 * v, sm.rows);
+        const TrialCtx tc{sm.rows, sm.gw, sm.win, sm.sub, b.vpos + 3 * v, b.rot_cs, b.hkl, b.geo, wq, fq};
         for (int64_t t = t0; t < t1; ++t) {
-            build_gw(g, b.hkl, b.U + 9 * orient_of(w, t, v), sm.gw);
+            build_gw(g, b.hkl, b.U + 9 * orient_of(w, t, v), sm.gw, sm.win, sm.sub);
             __syncthreads();
             MarkSink sink{mask};
-            run_trial<HPL>(g, sm.trow, sm.kw, sm.gw, wq, sink);
+            run_trial<HPL>(g, tc, sink);
             __syncthreads();
         }
     }
@@ -546,11 +704,12 @@ cudaError_t launch_mark_t(const Geo &g, const ScoreBufs &b, const Work &w, int n
 
 size_t score_smem_bytes(int nrot, int nhkl) {
     size_t off = 0;
-    off = (off + sizeof(OmegaRow) * nrot + 15) & ~size_t(15);
-    off = (off + sizeof(float4) * nrot + 15) & ~size_t(15);
-    off = (off + sizeof(double) * 4 * nhkl + 15) & ~size_t(15);
+    off = (off + sizeof(RowF) * nrot + 15) & ~size_t(15);
+    off = (off + sizeof(float4) * nhkl + 15) & ~size_t(15);
+    off = (off + sizeof(float4) * nhkl + 15) & ~size_t(15);
+    off = (off + sizeof(double) * 9 + 15) & ~size_t(15);
     off += sizeof(uint32_t) * kHistBins;
-    off += sizeof(uint32_t) * kWarps * kQueueCap;
+    off += sizeof(uint32_t) * kWarps * (kQueueCap + kFallbackCap);
     return off;
 }
 

@@ -12,8 +12,8 @@ the reference's configurations:
 * the distance map ``proj_bin_bw = bwdist(mask)`` of GrainMapping_fun.m:73-75, i.e.
   the Euclidean distance of every pixel to the nearest spot pixel (0 on spots).
 
-Everything here is host-side numpy; large volumes use the library's device-side
-spot simulator and EDT instead (``grainrecon_b200.forward.simulate_masks``).
+Small samples are synthesised with host-side numpy; large volumes use the library's
+device-side spot simulator and EDT instead (``device_maps``).
 """
 from __future__ import annotations
 
@@ -130,7 +130,18 @@ def make_sample(kind: str = "fe_small", seed: int = 1, **over) -> Sample:
         setattr(geom, k, v)
     vol = G.Volume(rec_volume_pixel=(1, 1, 1), simap=1, vox_size=vox, center=(0.0, 0.0, 0.0),
                    dimension=(dim, dim, dim))
-    gid = voronoi_cylinder(dim, ng, seed, sigma)
+    if dim >= 64:
+        try:
+            import torch
+            use_torch = torch.cuda.is_available()
+        except ImportError:
+            use_torch = False
+    else:
+        use_torch = False
+    if use_torch:
+        gid = voronoi_cylinder_torch(dim, ng, seed, sigma).cpu().numpy()
+    else:
+        gid = voronoi_cylinder(dim, ng, seed, sigma)
     q = G.cubic_fz_orientations(ng, seed + 7)
     hkl = G.gen_hkl(sg, 6)
     return Sample(geom=geom, vol=vol, cell=cell, space_group=sg, B=G.form_b(cell), hkl=hkl, S=np.eye(3),
@@ -239,3 +250,66 @@ def distance_map(mask: np.ndarray) -> np.ndarray:
         else:
             out[i] = np.inf
     return out
+
+
+def voronoi_cylinder_torch(dim: int, n_grains: int, seed: int, lognormal_sigma: float = 0.0, device="cuda"):
+    """``voronoi_cylinder`` evaluated with torch on ``device`` (same sites and weights)."""
+    import torch
+
+    rng = np.random.default_rng(seed)
+    r = dim / 2.0
+    sites = []
+    while len(sites) < n_grains:
+        p = rng.random(3) * dim
+        if (p[0] - r) ** 2 + (p[1] - r) ** 2 <= r * r:
+            sites.append(p)
+    sites = torch.tensor(np.array(sites), dtype=torch.float64, device=device)
+    mean_d = dim / max(n_grains, 1) ** (1 / 3)
+    w2 = torch.zeros(n_grains, dtype=torch.float64, device=device)
+    if lognormal_sigma > 0:
+        w = rng.lognormal(mean=0.0, sigma=lognormal_sigma, size=n_grains) * mean_d * 0.5
+        w2 = torch.tensor(w * w, dtype=torch.float64, device=device)
+    ax = torch.arange(dim, dtype=torch.float64, device=device) + 0.5
+    gid = torch.zeros((dim, dim, dim), dtype=torch.int32, device=device)
+    for ix in range(dim):
+        Y, Z = torch.meshgrid(ax, ax, indexing="ij")
+        X = torch.full_like(Y, float(ax[ix]))
+        inside = (X - r) ** 2 + (Y - r) ** 2 <= r * r
+        pts = torch.stack([X[inside], Y[inside], Z[inside]], 1)
+        if pts.shape[0] == 0:
+            continue
+        d = ((pts[:, None, :] - sites[None, :, :]) ** 2).sum(-1) - w2[None, :]
+        sl = gid[ix]
+        sl[inside] = (torch.argmin(d, dim=1) + 1).to(torch.int32)
+    return gid
+
+
+def device_maps(sample: Sample, ctx, keep_host_map: bool = False):
+    """Simulate the spot masks and their distance map on the GPU and make the map resident.
+
+    Uses the library's device spot simulator (the same point-voxel model as
+    ``simulate_mask``) and exact EDT, then ``grc_upload_masks_device``.  Returns the
+    host float32 map (nrot, dety, detz) when ``keep_host_map``, else None.
+    """
+    import torch
+
+    g = sample.geom
+    S9, B9, hkl, rot, R9, p = sample.mex_arrays()
+    ctx.set_geometry(S9, B9, hkl, rot, R9, p)
+    idx = sample.voxel_indices()
+    gid = sample.grain_id[idx[:, 0] - 1, idx[:, 1] - 1, idx[:, 2] - 1]
+    pos = sample.vol.pos_of_index(idx).astype(np.float32)
+    Ug = np.stack([G.flat_rowmajor(G.quat_to_u(q)) for q in sample.grain_q])
+    d_U = torch.from_numpy(Ug).cuda()[torch.from_numpy(gid - 1).long().cuda()].reshape(-1).contiguous()
+    n = g.nrot * g.detysize * g.detzsize
+    d_mask = torch.zeros(n, dtype=torch.uint8, device="cuda")
+    ctx.simulate_spots(torch.from_numpy(pos.reshape(-1)).cuda(), d_U, len(idx), d_mask)
+    del d_U
+    d_map = torch.empty(n, dtype=torch.float32, device="cuda")
+    ctx.edt(d_mask, g.detzsize, g.detysize, g.nrot, d_map)
+    del d_mask
+    ctx.upload_masks(d_map, g.detzsize, g.detysize, g.nrot)
+    host = d_map.cpu().numpy().reshape(g.nrot, g.detysize, g.detzsize) if keep_host_map else None
+    del d_map
+    torch.cuda.empty_cache()
+    return host
