@@ -24,7 +24,8 @@ EXPORTS = [
     "grc_ctx_create", "grc_ctx_destroy", "grc_last_error", "grc_ctx_stream", "grc_sync", "grc_set_options",
     "grc_upload_masks", "grc_upload_masks_device", "grc_set_geometry", "grc_forward_comp",
     "grc_grow_indexed_region", "grc_forward_comp_compete", "grc_forward_comp_device", "grc_grow_device",
-    "grc_compete_device", "grc_last_stats", "grc_set_timing", "grc_mask_info", "grc_simulate_spots", "grc_edt",
+    "grc_compete_device", "grc_last_stats", "grc_set_timing", "grc_set_path", "grc_mask_info", "grc_simulate_spots",
+    "grc_edt",
 ]
 
 
@@ -36,7 +37,8 @@ class GrcError(RuntimeError):
 
 class Stats(C.Structure):
     _fields_ = [("trials", C.c_int64), ("refined", C.c_int64), ("kernel_launches", C.c_int64),
-                ("score_ms", C.c_double)]
+                ("score_ms", C.c_double), ("path", C.c_int64), ("audit_checked", C.c_int64),
+                ("audit_mismatch", C.c_int64)]
 
 
 _lib = None
@@ -77,6 +79,7 @@ def load(path: str | None = None):
         "grc_compete_device": [vp, f, i64, f, i64, f, i64, f, f, f],
         "grc_last_stats": [vp, C.POINTER(Stats)],
         "grc_set_timing": [vp, i],
+        "grc_set_path": [vp, i],
         "grc_mask_info": [vp, C.POINTER(i64), C.POINTER(i), C.POINTER(i64), C.POINTER(i64), C.POINTER(i64)],
         "grc_simulate_spots": [vp, f, f, i64, f],
         "grc_edt": [vp, f, i64, i64, i64, f],
@@ -228,11 +231,16 @@ class Context:
     def set_timing(self, enable: bool):
         self._check(self.L.grc_set_timing(self.h, int(bool(enable))))
 
+    def set_path(self, path: int):
+        """0 = by size, 1 = per-trial kernel, 2 = projection-window sweep."""
+        self._check(self.L.grc_set_path(self.h, int(path)))
+
     def last_stats(self) -> dict:
         s = Stats()
         self._check(self.L.grc_last_stats(self.h, C.byref(s)))
         return {"trials": s.trials, "refined": s.refined, "kernel_launches": s.kernel_launches,
-                "score_ms": s.score_ms}
+                "score_ms": s.score_ms, "path": s.path, "audit_checked": s.audit_checked,
+                "audit_mismatch": s.audit_mismatch}
 
     def mask_info(self) -> dict:
         nd, nz, ny, nr = C.c_int64(), C.c_int64(), C.c_int64(), C.c_int64()

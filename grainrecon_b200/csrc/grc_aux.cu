@@ -104,7 +104,7 @@ __global__ void csr_counts_k(const float *rows5, int64_t m, int64_t *counts) {
 }
 
 __global__ void csr_fill_k(const float *rows5, int64_t m, const int64_t *off, const float *id_neigb, int64_t n_neigb,
-                           int64_t n_grain, longlong4 *items, int32_t *trial_orient, int *bad) {
+                           int64_t n_grain, longlong4 *items, int32_t *trial_orient, int32_t *trial_voxel, int *bad) {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < m; i += (int64_t)gridDim.x * blockDim.x) {
         const int64_t first = (int64_t)rows5[5 * i + 3], last = (int64_t)rows5[5 * i + 4];
         const int64_t o = off[i];
@@ -120,6 +120,7 @@ __global__ void csr_fill_k(const float *rows5, int64_t m, const int64_t *off, co
                 gid = 1;
             }
             trial_orient[o + j] = (int32_t)(gid - 1);
+            trial_voxel[o + j] = (int32_t)i;
         }
         items[i] = make_longlong4(i, o, o + cnt, 0);
     }
@@ -212,11 +213,14 @@ __global__ void values_k(const uint32_t *bitmap, const uint32_t *prefix, int64_t
 }
 
 template <typename CodeT>
-__global__ void codes_k(const float *map, int64_t n, const uint32_t *bitmap, const uint32_t *prefix, CodeT *codes) {
+__global__ void codes_k(const float *map, int64_t n, const uint32_t *bitmap, const uint32_t *prefix, CodeT *codes,
+                        uint8_t *codes8) {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
         const uint32_t k = ordered_key(map[i]);
         const uint32_t w = k >> 5, b = k & 31;
-        codes[i] = (CodeT)(prefix[w] + __popc(bitmap[w] & ((1u << b) - 1u)));
+        const uint32_t c = prefix[w] + __popc(bitmap[w] & ((1u << b) - 1u));
+        codes[i] = (CodeT)c;
+        codes8[i] = (uint8_t)(c < 255u ? c : 255u);
     }
 }
 
@@ -305,9 +309,10 @@ cudaError_t launch_csr_counts(const float *rows5, int64_t m, int64_t *counts, cu
     return cudaGetLastError();
 }
 cudaError_t launch_csr_fill(const float *rows5, int64_t m, const int64_t *offsets, const float *id_neigb,
-                            int64_t n_neigb, int64_t n_grain, longlong4 *items, int32_t *trial_orient, int *bad,
-                            cudaStream_t s) {
-    csr_fill_k<<<blocks_for(m), kB, 0, s>>>(rows5, m, offsets, id_neigb, n_neigb, n_grain, items, trial_orient, bad);
+                            int64_t n_neigb, int64_t n_grain, longlong4 *items, int32_t *trial_orient,
+                            int32_t *trial_voxel, int *bad, cudaStream_t s) {
+    csr_fill_k<<<blocks_for(m), kB, 0, s>>>(rows5, m, offsets, id_neigb, n_neigb, n_grain, items, trial_orient,
+                                            trial_voxel, bad);
     return cudaGetLastError();
 }
 cudaError_t launch_epi_compete(const TrialRes *res, const longlong4 *items, const int32_t *trial_orient, int64_t m,
@@ -324,6 +329,7 @@ cudaError_t encode_map(const float *d_map, int64_t n, cudaStream_t s, MapCodes *
     size_t tmp_bytes = 0;
     cudaError_t e;
     out->codes = nullptr;
+    out->codes8 = nullptr;
     out->vals = nullptr;
 #define CK(x)                    \
     do {                         \
@@ -361,14 +367,16 @@ cudaError_t encode_map(const float *d_map, int64_t n, cudaStream_t s, MapCodes *
         CK(cudaMalloc(&out->vals, sizeof(float) * (nd > 0 ? nd : 1)));
         values_k<<<blocks_for(nw), kB, 0, s>>>(bitmap, prefix, nw, out->vals);
         CK(cudaGetLastError());
+        CK(cudaMalloc(&out->codes8, sizeof(uint8_t) * (n > 0 ? n : 1)));
+        out->code_bits = bits;
         if (nd <= 65536) {
-            out->code_bits = bits;
             CK(cudaMalloc(&out->codes, sizeof(uint16_t) * (n > 0 ? n : 1)));
-            codes_k<uint16_t><<<blocks_for(n, kB * 8), kB, 0, s>>>(d_map, n, bitmap, prefix, (uint16_t *)out->codes);
+            codes_k<uint16_t><<<blocks_for(n, kB * 8), kB, 0, s>>>(d_map, n, bitmap, prefix, (uint16_t *)out->codes,
+                                                                  out->codes8);
         } else {
-            out->code_bits = bits;
             CK(cudaMalloc(&out->codes, sizeof(uint32_t) * (n > 0 ? n : 1)));
-            codes_k<uint32_t><<<blocks_for(n, kB * 8), kB, 0, s>>>(d_map, n, bitmap, prefix, (uint32_t *)out->codes);
+            codes_k<uint32_t><<<blocks_for(n, kB * 8), kB, 0, s>>>(d_map, n, bitmap, prefix, (uint32_t *)out->codes,
+                                                                  out->codes8);
         }
         CK(cudaGetLastError());
         CK(cudaStreamSynchronize(s));
@@ -382,8 +390,10 @@ done:
     cudaFree(tmp);
     if (e != cudaSuccess || *bad_nan) {
         cudaFree(out->codes);
+        cudaFree(out->codes8);
         cudaFree(out->vals);
         out->codes = nullptr;
+        out->codes8 = nullptr;
         out->vals = nullptr;
     }
     return e;

@@ -41,11 +41,12 @@ struct grc_ctx {
     grc::MapCodes mc{};
     int64_t mz = 0, my = 0, mrot = 0;
     std::vector<float> h_vals;
-    DevBuf geo_dev, rot_cs, hkl, pos, U, res, in1, in2, in3, out, items, torient, counts, offsets, tmp, counter, p1, bad;
+    DevBuf geo_dev, rot_cs, hkl, pos, U, res, tvoxel, rlist, in1, in2, in3, out, items, torient, counts, offsets, tmp, counter, p1, bad;
     grc::Geo *geo_pinned = nullptr;  // staging of the per-launch geometry copy
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     bool timing = false;
     bool timed_last = false;
+    int force_path = 0;  // 0 = by size, 1 = per-trial kernel, 2 = projection-window sweep
     grc_stats stats{};
 };
 
@@ -123,6 +124,9 @@ void apply_options(grc_ctx *ctx) {
     g.bsy1f = (float)g.bsy1;
     g.bsz0f = (float)g.bsz0;
     g.bsz1f = (float)g.bsz1;
+    g.lo4pif = (float)(g.lmin * 0.25 / 3.14159265358979323846);
+    g.hi4pif = (float)(g.lmax * 0.25 / 3.14159265358979323846);
+    g.cbmaxf = (float)g.cbmax;
     refresh_hit(ctx);
 }
 
@@ -204,12 +208,14 @@ int upload_device_map(grc_ctx *ctx, const float *d_map, int64_t dz, int64_t dy, 
         e = cudaMemcpy(hv.data(), mc.vals, sizeof(float) * mc.n_distinct, cudaMemcpyDeviceToHost);
         if (e != cudaSuccess) {
             cudaFree(mc.codes);
+            cudaFree(mc.codes8);
             cudaFree(mc.vals);
             return fail(ctx, GRC_ECUDA, "value table copy: %s", cudaGetErrorString(e));
         }
     }
     if (ctx->has_masks) {
         cudaFree(ctx->mc.codes);
+        cudaFree(ctx->mc.codes8);
         cudaFree(ctx->mc.vals);
     }
     ctx->mc = mc;
@@ -264,7 +270,9 @@ grc::ScoreBufs bufs(grc_ctx *ctx) {
     b.vpos = (const double *)ctx->pos.p;
     b.U = (const double *)ctx->U.p;
     b.codes = ctx->mc.codes;
+    b.codes8 = ctx->mc.codes8;
     b.vals = ctx->mc.vals;
+    b.refine_list = (int64_t *)ctx->rlist.p;
     b.res = (grc::TrialRes *)ctx->res.p;
     b.work_counter = (int *)ctx->counter.p;
     return b;
@@ -282,9 +290,18 @@ int run_score(grc_ctx *ctx, const grc::Work &w, int64_t n_trials) {
     TRY(ensure(ctx, ctx->counter, 8 * sizeof(int)));
     TRY(stage_geo(ctx));
     int launches = 0;
-    cudaError_t e = grc::launch_score(ctx->geo, bufs(ctx), w, ctx->num_sms, ctx->stream,
-                                      ctx->timing ? ctx->ev0 : nullptr, ctx->timing ? ctx->ev1 : nullptr,
-                                      &launches);
+    cudaEvent_t e0 = ctx->timing ? ctx->ev0 : nullptr, e1 = ctx->timing ? ctx->ev1 : nullptr;
+    const int64_t round = ctx->force_path == 1 ? 0 : grc::sweep_round_trials(ctx->geo, ctx->num_sms);
+    cudaError_t e;
+    if (round > 0 && (ctx->force_path == 2 || n_trials * 2 >= round)) {
+        // projection-window sweep (L2-resident map windows) for large trial counts
+        TRY(ensure(ctx, ctx->rlist, sizeof(int64_t) * n_trials));
+        e = grc::launch_sweep(ctx->geo, bufs(ctx), w, n_trials, ctx->num_sms, ctx->stream, e0, e1, &launches);
+        ctx->stats.path = 2;
+    } else {
+        e = grc::launch_score(ctx->geo, bufs(ctx), w, ctx->num_sms, ctx->stream, e0, e1, &launches);
+        ctx->stats.path = 1;
+    }
     if (e != cudaSuccess) return fail(ctx, GRC_ECUDA, "scorer launch: %s", cudaGetErrorString(e));
     ctx->timed_last = ctx->timing;
     ctx->stats.trials = n_trials;
@@ -381,9 +398,11 @@ int compete_device(grc_ctx *ctx, const float *d_rows5, int64_t m, const float *d
     CU(cudaStreamSynchronize(ctx->stream));
     const int64_t T = last_off + last_cnt;
     TRY(ensure(ctx, ctx->torient, sizeof(int32_t) * (T > 0 ? T : 1)));
+    TRY(ensure(ctx, ctx->tvoxel, sizeof(int32_t) * (T > 0 ? T : 1)));
     TRY(ensure(ctx, ctx->res, sizeof(grc::TrialRes) * (T > 0 ? T : 1)));
     CU(grc::launch_csr_fill(d_rows5, m, (const int64_t *)ctx->offsets.p, d_id, n_neigb, n_grain,
-                            (longlong4 *)ctx->items.p, (int32_t *)ctx->torient.p, (int *)ctx->bad.p, ctx->stream));
+                            (longlong4 *)ctx->items.p, (int32_t *)ctx->torient.p, (int32_t *)ctx->tvoxel.p,
+                            (int *)ctx->bad.p, ctx->stream));
     int hbad = 0;
     CU(cudaMemcpyAsync(&hbad, ctx->bad.p, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
     CU(cudaStreamSynchronize(ctx->stream));
@@ -393,6 +412,7 @@ int compete_device(grc_ctx *ctx, const float *d_rows5, int64_t m, const float *d
         grc::Work w{};
         w.items = (const longlong4 *)ctx->items.p;
         w.trial_orient = (const int32_t *)ctx->torient.p;
+        w.trial_voxel = (const int32_t *)ctx->tvoxel.p;
         w.n_items = m;
         TRY(run_score(ctx, w, T));
     }
@@ -469,12 +489,13 @@ int grc_ctx_destroy(grc_ctx *ctx) {
         Lock l(ctx);
         cudaStreamSynchronize(ctx->stream);
         cudaFreeHost(ctx->geo_pinned);
-        DevBuf *all[] = {&ctx->geo_dev, &ctx->rot_cs, &ctx->hkl, &ctx->pos, &ctx->U, &ctx->res, &ctx->in1, &ctx->in2,
+        DevBuf *all[] = {&ctx->tvoxel, &ctx->rlist, &ctx->geo_dev, &ctx->rot_cs, &ctx->hkl, &ctx->pos, &ctx->U, &ctx->res, &ctx->in1, &ctx->in2,
                          &ctx->in3, &ctx->out, &ctx->items, &ctx->torient, &ctx->counts, &ctx->offsets,
                          &ctx->tmp, &ctx->counter, &ctx->p1, &ctx->bad};
         for (DevBuf *b : all) cudaFree(b->p);
         if (ctx->has_masks) {
             cudaFree(ctx->mc.codes);
+            cudaFree(ctx->mc.codes8);
             cudaFree(ctx->mc.vals);
         }
         cudaEventDestroy(ctx->ev0);
@@ -646,6 +667,10 @@ int grc_last_stats(grc_ctx *ctx, grc_stats *out) {
         int c[8];
         CU(cudaMemcpy(c, ctx->counter.p, sizeof c, cudaMemcpyDeviceToHost));
         ctx->stats.refined = c[4];
+        ctx->stats.audit_mismatch = c[5];
+        int64_t checked = 0;
+        std::memcpy(&checked, c + 6, sizeof checked);
+        ctx->stats.audit_checked = checked;
     }
     ctx->stats.score_ms = 0;
     if (ctx->timed_last) {
@@ -654,6 +679,13 @@ int grc_last_stats(grc_ctx *ctx, grc_stats *out) {
         cudaGetLastError();
     }
     *out = ctx->stats;
+    return GRC_OK;
+}
+
+int grc_set_path(grc_ctx *ctx, int path) {
+    if (!ctx || path < 0 || path > 2) return GRC_EINVAL;
+    Lock l(ctx);
+    ctx->force_path = path;
     return GRC_OK;
 }
 

@@ -27,6 +27,7 @@ struct Geo {
     float Rf[9];
     float dety0f, detz0f, rpxyf, rpxzf;
     float bsy0f, bsy1f, bsz0f, bsz1f;
+    float lo4pif, hi4pif, cbmaxf;   // lambda_min/(4 pi), lambda_max/(4 pi), cos(beta_max)
     int nhkl, nrot, detysize, detzsize;
     uint32_t n_hit;          // codes [0, n_hit) are "dis <= threshold"
     uint32_t n_vals;         // entries of the code -> value table
@@ -49,6 +50,7 @@ struct TrialRes {
 struct Work {
     const longlong4 *items;
     const int32_t *trial_orient;
+    const int32_t *trial_voxel;   // explicit voxel per trial (sweep kernel), or nullptr
     int64_t n_items;
     int64_t n_or;
     int64_t chunks_per_voxel;
@@ -63,7 +65,9 @@ struct ScoreBufs {
     const double *vpos;       // 3 per voxel [mm]
     const double *U;          // 9 per orientation
     const void *codes;        // rank codes of the distance map
+    const uint8_t *codes8;    // the same codes saturated at 255 (sweep kernel)
     const float *vals;        // code -> distance value
+    int64_t *refine_list;     // trials whose median needs the exact refine pass (sweep kernel)
     TrialRes *res;
     int *work_counter;        // 8 ints: [0..1] main-pass item counter (u64), [2..3] refine-pass
                               // item counter (u64), [4] trials left for the refine pass
@@ -74,6 +78,12 @@ size_t refine_smem_bytes(int nrot, int nhkl);
 // Enqueue the scoring pass (+ refine pass) on `s`.  Returns a cudaError_t.
 cudaError_t launch_score(const Geo &g, const ScoreBufs &b, const Work &w, int num_sms, cudaStream_t s,
                          cudaEvent_t ev0, cudaEvent_t ev1, int *launches);
+// Trials one round of the projection-window sweep holds (grid x slots); 0 if the sweep
+// cannot serve this geometry.
+int64_t sweep_round_trials(const Geo &g, int num_sms);
+// Enqueue the projection-window sweep over n_trials trials (+ the list refine pass).
+cudaError_t launch_sweep(const Geo &g, const ScoreBufs &b, const Work &w, int64_t n_trials, int num_sms,
+                         cudaStream_t s, cudaEvent_t ev0, cudaEvent_t ev1, int *launches);
 
 // Orientation / position preparation kernels.
 cudaError_t launch_quat_to_u(const float *q, int64_t n, double *U, cudaStream_t s);
@@ -91,13 +101,14 @@ cudaError_t launch_epi_grow(const TrialRes *res, const float *rows6, int64_t m, 
 cudaError_t launch_csr_counts(const float *rows5, int64_t m, int64_t *counts, cudaStream_t s);
 cudaError_t launch_csr_fill(const float *rows5, int64_t m, const int64_t *offsets, const float *id_neigb,
                             int64_t n_neigb, int64_t n_grain, longlong4 *items, int32_t *trial_orient,
-                            int *bad, cudaStream_t s);
+                            int32_t *trial_voxel, int *bad, cudaStream_t s);
 cudaError_t launch_epi_compete(const TrialRes *res, const longlong4 *items, const int32_t *trial_orient,
                                int64_t m, const float *euler, float *out8, float *trial_out4, cudaStream_t s);
 
 // Distance-map rank coding.
 struct MapCodes {
     void *codes;
+    uint8_t *codes8;
     float *vals;
     int64_t n_distinct;
     int code_bits;

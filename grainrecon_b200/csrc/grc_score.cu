@@ -34,6 +34,9 @@
 #ifndef GRC_MIN_BLOCKS
 #define GRC_MIN_BLOCKS 4
 #endif
+#ifndef GRC_SWEEP_BLOCKS
+#define GRC_SWEEP_BLOCKS 3
+#endif
 
 namespace grc {
 namespace {
@@ -60,7 +63,10 @@ static_assert(sizeof(RowF) == 64, "RowF layout");
 // FP64 chain stays below 1.4e-3 px on the 1024^2 / 2048^2 geometries (measured over
 // 3.4e5 landings); landings closer than this to a half-pixel boundary are recomputed
 // in FP64, so every decision equals the FP64 one.
-constexpr float kAmbigPx = 0.0125f;
+#ifndef GRC_AMBIG_PX
+#define GRC_AMBIG_PX 0.0125f
+#endif
+constexpr float kAmbigPx = GRC_AMBIG_PX;
 
 __device__ __forceinline__ size_t align16(size_t x) { return (x + 15) & ~size_t(15); }
 
@@ -138,9 +144,9 @@ __device__ void build_gw(const Geo &g, const double *__restrict__ hkl, const dou
     const double x = SUB[0] * h + SUB[1] * k + SUB[2] * l;
     const double y = SUB[3] * h + SUB[4] * k + SUB[5] * l;
     const double z = SUB[6] * h + SUB[7] * k + SUB[8] * l;
-    const float G = (float)sqrt(x * x + y * y + z * z);
-    gw[ih] = make_float4((float)x, (float)y, (float)z, G);
-    win[ih] = window_of(g, G);
+    const double Gd = sqrt(x * x + y * y + z * z);
+    gw[ih] = make_float4((float)x, (float)y, (float)z, (float)(1.0 / Gd));
+    win[ih] = window_of(g, (float)Gd);
 }
 
 // Exact FP64 evaluation of one reflection: the linear map index of its pixel, or -1
@@ -212,18 +218,22 @@ __device__ __forceinline__ int64_t landing_fp32(const Geo &g, const RowF &r, con
     const float dot = r.kx * Gtx + r.ky * Gty + r.kz * Gtz;
     const float t = -dot;
     if (!(t > lo_in && t < hi_in)) return -2;  // near the wavelength / Bragg-angle window edge
-    const float x = dot / gw.w;
-    const float st = -x, ct = sqrtf(1.0f - x * x);
+    // gw.w holds 1/|G|; reciprocal and square-root intrinsics (a few ulp) stay far inside
+    // the ambiguity band
+    const float x = dot * gw.w;
+    const float q = fmaxf(1.0f - x * x, 0.0f);
+    const float st = -x, ct = q * rsqrtf(q);
     const float s2 = 2.0f * st * ct, c2 = 1.0f - 2.0f * st * st;
     const float rk = rsqrtf(Gty * Gty + Gtz * Gtz);
     const float gy = Gty * rk, gz = Gtz * rk;
     const float cphx = gy * r.ky + gz * r.kz;
-    const float sphx = sqrtf(fmaxf(0.0f, 1.0f - cphx * cphx));
+    const float p = fmaxf(1.0f - cphx * cphx, 0.0f);
+    const float sphx = p * rsqrtf(p);
     const float sphy = sphx * c2 - cphx * s2;
-    const float diff = r.L2 * s2 / sphy;
+    const float diff = __fdividef(r.L2 * s2, sphy);
     const float Kx = r.ax, Ky = r.ay + diff * gy, Kz = r.az + diff * gz;
     const float nK = g.Rf[0] * Kx + g.Rf[3] * Ky + g.Rf[6] * Kz;
-    const float f = r.num / nK;
+    const float f = __fdividef(r.num, nK);
     const float y2 = f * (g.Rf[1] * Kx + g.Rf[4] * Ky + g.Rf[7] * Kz) + r.r2d;
     const float z2 = f * (g.Rf[2] * Kx + g.Rf[5] * Ky + g.Rf[8] * Kz) + r.r3d;
     const float u = g.dety0f - y2 * g.rpxyf, v = g.detz0f - z2 * g.rpxzf;
@@ -651,6 +661,411 @@ __global__ void __launch_bounds__(kThreads, 2) mark_kernel(Geo g, ScoreBufs b, W
     }
 }
 
+// ---------------------------------------------------------------------------------
+// Projection-window sweep.  One launch = one round: each CTA holds kSlots trials in
+// shared memory (counters, a 256-bin histogram of the 8-bit saturated codes, S*U*B)
+// and every CTA walks the projections in windows of kWin at the same pace, so the
+// map pixels being read belong to a few projections at a time and stay in L2.
+constexpr int kSlots = 64;
+constexpr int kWin = 8;
+constexpr int kSlotsPerWarp = kSlots / kWarps;
+constexpr int kHist8Words = 128;  // 256 u16 bins per slot, two per word
+
+__device__ __forceinline__ int64_t voxel_of(const Work &w, int64_t t) {
+    if (w.trial_voxel) return (int64_t)w.trial_voxel[t];
+    if (w.diag) return t;
+    return t / w.n_or;
+}
+
+struct SweepSmem {
+    RowF *rows;       // [rows_cap * kWin] rows of the current window, indexed vloc * kWin + wl
+    float4 *hk;       // [nhkl] h as float
+    uint32_t *hist;   // [kSlots * kHist8Words]
+    uint32_t *cnt;    // [kSlots] Nr_simu | Nr_intersect << 16
+    float *subf;      // [kSlots * 12]
+    double *subd;     // [kSlots * 9]
+    int *vloc;        // [kSlots]
+    int64_t *vglob;   // [kSlots]
+    int64_t *vlist;   // [kSlots]
+    uint32_t *queue;  // [kWarps * kQueueCap]
+    uint32_t *fqueue; // [kWarps * kFallbackCap]
+};
+
+__host__ __device__ inline size_t sweep_smem_layout(int nhkl, int rows_cap, size_t *offs) {
+    size_t o = 0, i = 0;
+    auto put = [&](size_t bytes) {
+        o = (o + 15) & ~size_t(15);
+        offs[i++] = o;
+        o += bytes;
+    };
+    put(sizeof(RowF) * rows_cap * kWin);
+    put(sizeof(float4) * nhkl);
+    put(sizeof(uint32_t) * kSlots * kHist8Words);
+    put(sizeof(uint32_t) * kSlots);
+    put(sizeof(float) * kSlots * 12);
+    put(sizeof(double) * kSlots * 9);
+    put(sizeof(int) * kSlots);
+    put(sizeof(int64_t) * kSlots);
+    put(sizeof(int64_t) * kSlots);
+    put(sizeof(uint32_t) * kWarps * kQueueCap);
+    put(sizeof(uint32_t) * kWarps * kFallbackCap);
+    return (o + 15) & ~size_t(15);
+}
+
+__device__ __forceinline__ SweepSmem sweep_carve(unsigned char *base, int nhkl, int rows_cap) {
+    size_t offs[11];
+    sweep_smem_layout(nhkl, rows_cap, offs);
+    SweepSmem m;
+    m.rows = (RowF *)(base + offs[0]);
+    m.hk = (float4 *)(base + offs[1]);
+    m.hist = (uint32_t *)(base + offs[2]);
+    m.cnt = (uint32_t *)(base + offs[3]);
+    m.subf = (float *)(base + offs[4]);
+    m.subd = (double *)(base + offs[5]);
+    m.vloc = (int *)(base + offs[6]);
+    m.vglob = (int64_t *)(base + offs[7]);
+    m.vlist = (int64_t *)(base + offs[8]);
+    m.queue = (uint32_t *)(base + offs[9]);
+    m.fqueue = (uint32_t *)(base + offs[10]);
+    return m;
+}
+
+// Gw (FP32) of one reflection from the slot's S*U*B and h; .w = 1/|Gw|.
+__device__ __forceinline__ float4 gw_of(const float *sf, const float4 h) {
+    const float x = sf[0] * h.x + sf[1] * h.y + sf[2] * h.z;
+    const float y = sf[3] * h.x + sf[4] * h.y + sf[5] * h.z;
+    const float z = sf[6] * h.x + sf[7] * h.y + sf[8] * h.z;
+    return make_float4(x, y, z, rsqrtf(x * x + y * y + z * z));
+}
+
+// Window on t = -(k_w . Gw) in FP32 (see window_of) from rG = 1/|G|; the 1e-5 |G|
+// margins dominate its FP32 rounding.
+__device__ __forceinline__ float4 window_f(const Geo &g, float rG) {
+    const float G = __frcp_rn(rG), G2 = G * G;
+    float lo = g.lo4pif * G2, hi = g.hi4pif * G2;
+    if (g.cbmaxf > -1.0f) hi = fminf(hi, -g.cbmaxf * G);
+    lo = fmaxf(lo, 0.0f);
+    const float m = 1e-5f * G;
+    return make_float4(lo - m, hi + m, lo + m, hi - m);
+}
+
+template <int HPL>
+__global__ void __launch_bounds__(kThreads, GRC_SWEEP_BLOCKS) sweep_kernel(Geo g, ScoreBufs b, Work w, int64_t round_base,
+                                                            int64_t n_trials, int rows_cap) {
+    const int64_t cta_base = round_base + (int64_t)blockIdx.x * kSlots;
+    if (cta_base >= n_trials) return;
+    const int nslot = (int)min((int64_t)kSlots, n_trials - cta_base);
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const SweepSmem sm = sweep_carve(smem_raw, g.nhkl, rows_cap);
+    __shared__ int s_nv;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const unsigned lt = (1u << lane) - 1u;
+    uint32_t *wq = sm.queue + warp * kQueueCap;
+    uint32_t *fq = sm.fqueue + warp * kFallbackCap;
+
+    // ---- set-up: per-slot S*U*B, voxels, zeroed counters and histograms
+    if (tid < nslot) {
+        const int64_t t = cta_base + tid;
+        const int64_t v = voxel_of(w, t);
+        const int64_t o = orient_of(w, t, v);
+        double SUB[9];
+        sub_matrix(g, b.U + 9 * o, SUB);
+#pragma unroll
+        for (int i = 0; i < 9; ++i) {
+            sm.subd[9 * tid + i] = SUB[i];
+            sm.subf[12 * tid + i] = (float)SUB[i];
+        }
+        sm.vglob[tid] = v;
+        sm.cnt[tid] = 0;
+    }
+    for (int i = tid; i < kSlots * kHist8Words; i += kThreads) sm.hist[i] = 0;
+    for (int i = tid; i < g.nhkl; i += kThreads)
+        sm.hk[i] = make_float4((float)b.hkl[3 * i], (float)b.hkl[3 * i + 1], (float)b.hkl[3 * i + 2], 0.f);
+    __syncthreads();
+    if (tid == 0) {
+        int nv = 0;
+        for (int s = 0; s < nslot; ++s) {
+            if (s == 0 || sm.vglob[s] != sm.vglob[s - 1]) sm.vlist[nv++] = sm.vglob[s];
+            sm.vloc[s] = nv - 1;
+        }
+        s_nv = nv;
+    }
+    float hx[HPL], hy[HPL], hz[HPL];
+#pragma unroll
+    for (int j = 0; j < HPL; ++j) {
+        const int ih = lane + 32 * j;
+        const float4 h = ih < g.nhkl ? sm.hk[ih] : make_float4(0.f, 0.f, 0.f, 0.f);
+        hx[j] = h.x;
+        hy[j] = h.y;
+        hz[j] = h.z;
+    }
+    __syncthreads();
+    const int nv = s_nv;
+
+    // Selected pixels reach the histogram one batch late: the code of batch k is loaded
+    // when batch k is evaluated and applied after batch k+1 has been computed, so the
+    // L2 latency of the gather overlaps the next landing computations.
+    int64_t pend_idx = -1;   // this lane's pending map index (or -1)
+    int pend_slot = 0;
+    uint32_t pend_code = 0;
+    auto apply_pending = [&]() {
+        const bool ok = pend_idx >= 0;
+        const uint32_t code = pend_code;
+        if (ok) atomicAdd(&sm.hist[pend_slot * kHist8Words + (code >> 1)], 1u << ((code & 1u) * 16));
+        // per-slot counters, one atomic per distinct slot of the warp
+        const unsigned peers = __match_any_sync(kFull, ok ? pend_slot : -1);
+        const unsigned mok = __ballot_sync(kFull, ok), mhit = __ballot_sync(kFull, ok && code < g.n_hit);
+        if (ok && (__ffs(peers) - 1) == lane)
+            atomicAdd(&sm.cnt[pend_slot], (uint32_t)__popc(peers & mok) + ((uint32_t)__popc(peers & mhit) << 16));
+        pend_idx = -1;
+    };
+    auto sink = [&](int64_t idx, int s) {  // warp-synchronous: every lane calls it once per batch
+        uint32_t code = 0;
+        if (idx >= 0) code = __ldg(b.codes8 + idx);
+        apply_pending();
+        pend_idx = idx;
+        pend_slot = s;
+        pend_code = code;
+    };
+
+    for (int w0 = 0; w0 < g.nrot; w0 += kWin) {
+        const int nw = min(kWin, g.nrot - w0);
+        // ---- omega rows of this window for every voxel of the round
+        for (int i = tid; i < nv * nw; i += kThreads) {
+            const int vl = i / nw, wl = i - vl * nw;
+            const OmegaRow r = omega_row(g, b.rot_cs[w0 + wl], b.vpos + 3 * sm.vlist[vl]);
+            RowF f;
+            f.kx = (float)r.kx; f.ky = (float)r.ky; f.kz = (float)r.kz; f.L2 = (float)r.L2;
+            f.ax = (float)r.ax; f.ay = (float)r.ay; f.az = (float)r.az; f.num = (float)r.num;
+            f.r2d = (float)r.r2d; f.r3d = (float)r.r3d; f.c = (float)r.c; f.s = (float)r.s;
+            f.wx = (float)(r.c * r.kx + r.s * r.ky);
+            f.wy = (float)(-r.s * r.kx + r.c * r.ky);
+            f.wz = (float)r.kz;
+            f.pad = 0.f;
+            sm.rows[vl * kWin + wl] = f;
+        }
+        __syncthreads();
+        int qn = 0, fn = 0;
+        auto fast = [&](uint32_t item, bool valid) {
+            int64_t r = -1;
+            const int s = (int)(item >> 16), wl = (int)((item >> 8) & 255u), ih = (int)(item & 255u);
+            if (valid) {
+                const float4 gv = gw_of(sm.subf + 12 * s, sm.hk[ih]);
+                const float4 win = window_f(g, gv.w);
+                r = landing_fp32(g, sm.rows[sm.vloc[s] * kWin + wl], gv, win.z, win.w, w0 + wl);
+#ifdef GRC_AUDIT
+                // audit build: every certain FP32 decision is re-decided by the FP64 path
+                if (r != -2) {
+                    const int64_t r64 = landing_exact(b.geo, b.rot_cs, b.vpos + 3 * sm.vglob[s], b.hkl,
+                                                      sm.subd + 9 * s, w0 + wl, ih);
+                    atomicAdd((unsigned long long *)(b.work_counter + 6), 1ull);
+                    if (r64 != r) atomicAdd(b.work_counter + 5, 1);
+                }
+#endif
+            }
+            const bool amb = r == -2;
+            const unsigned m = __ballot_sync(kFull, amb);
+            if (amb) fq[fn + __popc(m & lt)] = item;
+            fn += __popc(m);
+            sink(r >= 0 ? r : -1, s);
+        };
+        auto exact = [&](uint32_t item, bool valid) {
+            const int s = (int)(item >> 16), wl = (int)((item >> 8) & 255u), ih = (int)(item & 255u);
+            int64_t r = -1;
+            if (valid)
+                r = landing_exact(b.geo, b.rot_cs, b.vpos + 3 * sm.vglob[s], b.hkl, sm.subd + 9 * s, w0 + wl, ih);
+            sink(r, s);
+        };
+        auto drain = [&](bool all) {
+            while (qn >= 32 || (all && qn > 0)) {
+                const int take = qn >= 32 ? 32 : qn;
+                qn -= take;
+                const bool valid = lane < take;
+                const uint32_t item = valid ? wq[qn + lane] : 0u;
+                __syncwarp();
+                fast(item, valid);
+                __syncwarp();
+                while (fn >= 32) {
+                    fn -= 32;
+                    const uint32_t it2 = fq[fn + lane];
+                    __syncwarp();
+                    exact(it2, true);
+                    __syncwarp();
+                }
+            }
+            if (all) {
+                while (fn > 0) {
+                    const int tk = fn >= 32 ? 32 : fn;
+                    fn -= tk;
+                    const bool v2 = lane < tk;
+                    const uint32_t it2 = v2 ? fq[fn + lane] : 0u;
+                    __syncwarp();
+                    exact(it2, v2);
+                    __syncwarp();
+                }
+            }
+        };
+        for (int k = 0; k < kSlotsPerWarp; ++k) {
+            const int s = warp + kWarps * k;
+            if (s >= nslot) break;
+            const float *sf = sm.subf + 12 * s;
+            float gx[HPL], gy[HPL], gz[HPL], lo[HPL], hi[HPL];
+#pragma unroll
+            for (int j = 0; j < HPL; ++j) {
+                const float4 gv = gw_of(sf, make_float4(hx[j], hy[j], hz[j], 0.f));
+                const float4 win = window_f(g, gv.w);
+                const bool real = lane + 32 * j < g.nhkl;
+                gx[j] = gv.x;
+                gy[j] = gv.y;
+                gz[j] = gv.z;
+                lo[j] = real ? win.x : CUDART_INF_F;
+                hi[j] = real ? win.y : -CUDART_INF_F;
+            }
+            const RowF *vr = sm.rows + sm.vloc[s] * kWin;
+            for (int wl = 0; wl < nw; ++wl) {
+                const float kx = vr[wl].wx, ky = vr[wl].wy, kz = vr[wl].wz;
+#pragma unroll
+                for (int j = 0; j < HPL; ++j) {
+                    const float t = -fmaf(kx, gx[j], fmaf(ky, gy[j], kz * gz[j]));
+                    const bool pass = (t > lo[j]) && (t < hi[j]);
+                    const unsigned m = __ballot_sync(kFull, pass);
+                    if (pass)
+                        wq[qn + __popc(m & lt)] =
+                            ((uint32_t)s << 16) | ((uint32_t)wl << 8) | (uint32_t)(lane + 32 * j);
+                    qn += __popc(m);
+                }
+                __syncwarp();
+                drain(false);
+            }
+        }
+        drain(true);
+        apply_pending();
+        __syncthreads();  // rows are rebuilt for the next window
+    }
+
+    // ---- finalize: one warp per slot, exact median from the 8-bit histogram
+    for (int s = warp; s < nslot; s += kWarps) {
+        const uint32_t c = sm.cnt[s];
+        const int n = (int)(c & 0xffffu), inter = (int)(c >> 16);
+        const uint32_t *h = sm.hist + s * kHist8Words;
+        // lane owns bins [8*lane, 8*lane+8)
+        uint32_t bins[8];
+        uint32_t local = 0;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const uint32_t wv = h[4 * lane + i];
+            bins[2 * i] = wv & 0xffffu;
+            bins[2 * i + 1] = wv >> 16;
+        }
+        if (lane == 31) bins[7] = 0;  // bin 255 = saturated codes, not part of the exact range
+#pragma unroll
+        for (int i = 0; i < 8; ++i) local += bins[i];
+        uint32_t incl = local;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(kFull, incl, o);
+            if (lane >= o) incl += y;
+        }
+        const uint32_t inr = __shfl_sync(kFull, incl, 31);
+        const uint32_t excl = incl - local;
+        const uint32_t ra = (uint32_t)(n + 1) / 2, rb = (uint32_t)n / 2 + 1;
+        int ca = -1, cb = -1;
+        if (n > 0 && rb <= inr) {
+            uint32_t cum = excl;
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+                if (ca < 0 && cum < ra && ra <= cum + bins[i]) ca = 8 * lane + i;
+                if (cb < 0 && cum < rb && rb <= cum + bins[i]) cb = 8 * lane + i;
+                cum += bins[i];
+            }
+        }
+        const unsigned ma = __ballot_sync(kFull, ca >= 0), mb = __ballot_sync(kFull, cb >= 0);
+        ca = ma ? __shfl_sync(kFull, ca, __ffs(ma) - 1) : -1;
+        cb = mb ? __shfl_sync(kFull, cb, __ffs(mb) - 1) : -1;
+        if (lane == 0) {
+            const int64_t t = cta_base + s;
+            TrialRes r;
+            r.simu = n;
+            r.inter = inter;
+            if (n == 0) {
+                r.median = 2000.0;  // forward_comp.m:89
+            } else if (ca >= 0 && cb >= 0) {
+                r.median = ((double)b.vals[ca] + (double)b.vals[cb]) / 2.0;
+            } else {
+                r.median = CUDART_NAN;
+                const int k = atomicAdd(b.work_counter + 4, 1);
+                b.refine_list[k] = t;
+            }
+            b.res[t] = r;
+        }
+    }
+}
+
+// Exact median for the trials listed by the sweep: full omega table, full-width codes,
+// 10-bit radix passes (random gathers; these trials are rare).
+template <int HPL, typename CodeT>
+__global__ void __launch_bounds__(kThreads, 2) refine_list_kernel(Geo g, ScoreBufs b, Work w) {
+    const int n_list = b.work_counter[4];
+    if (n_list == 0) return;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const Smem sm = carve(smem_raw, g, 2);
+    __shared__ uint32_t s_pa, s_pb, s_ra, s_rb;
+    const int warp = threadIdx.x >> 5;
+    uint32_t *wq = sm.queue + warp * kQueueCap;
+    uint32_t *fq = sm.fqueue + warp * kFallbackCap;
+    const CodeT *codes = (const CodeT *)b.codes;
+    for (int k = blockIdx.x; k < n_list; k += gridDim.x) {
+        const int64_t t = b.refine_list[k];
+        const int64_t v = voxel_of(w, t);
+        const int64_t o = orient_of(w, t, v);
+        __syncthreads();
+        build_rows(g, b.rot_cs, b.vpos + 3 * v, sm.rows);
+        build_gw(g, b.hkl, b.U + 9 * o, sm.gw, sm.win, sm.sub);
+        const TrialCtx tc{sm.rows, sm.gw, sm.win, sm.sub, b.vpos + 3 * v, b.rot_cs, b.hkl, b.geo, wq, fq};
+        const int n = b.res[t].simu;
+        if (threadIdx.x == 0) {
+            s_pa = s_pb = 0;
+            s_ra = (uint32_t)((n + 1) / 2);
+            s_rb = (uint32_t)(n / 2 + 1);
+        }
+        int pos = g.code_bits;
+        while (pos > 0) {
+            const int width = pos < 10 ? pos : 10;
+            pos -= width;
+            for (int i = threadIdx.x; i < kHistBins; i += kThreads) sm.h0[i] = sm.h1[i] = 0;
+            __syncthreads();
+            RadixSink<CodeT> sink{codes, sm.h0, sm.h1, s_pa, s_pb, pos, pos + width, (1u << width) - 1u};
+            run_trial<HPL>(g, tc, sink);
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                uint32_t cum = 0;
+                for (uint32_t d = 0; d < (1u << width); ++d) {
+                    if (cum + sm.h0[d] >= s_ra) {
+                        s_ra -= cum;
+                        s_pa = (s_pa << width) | d;
+                        break;
+                    }
+                    cum += sm.h0[d];
+                }
+                cum = 0;
+                for (uint32_t d = 0; d < (1u << width); ++d) {
+                    if (cum + sm.h1[d] >= s_rb) {
+                        s_rb -= cum;
+                        s_pb = (s_pb << width) | d;
+                        break;
+                    }
+                    cum += sm.h1[d];
+                }
+            }
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) {
+            const uint32_t ca = min(s_pa, g.n_vals - 1u), cb = min(s_pb, g.n_vals - 1u);
+            b.res[t].median = ((double)b.vals[ca] + (double)b.vals[cb]) / 2.0;
+        }
+    }
+}
+
 template <typename K>
 cudaError_t prep_launch(K kern, size_t smem, int num_sms, int64_t n_items, int *grid_out) {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -684,6 +1099,43 @@ cudaError_t launch_score_t(const Geo &g, const ScoreBufs &b, const Work &w, int 
     if (ev1) cudaEventRecord(ev1, s);
     refine_kernel<HPL, CodeT><<<grid_r, kThreads, smem_r, s>>>(g, b, w);
     *launches += 2;
+    return cudaGetLastError();
+}
+
+
+template <int HPL, typename CodeT>
+cudaError_t launch_sweep_t(const Geo &g, const ScoreBufs &b, const Work &w, int64_t n_trials, int num_sms,
+                           cudaStream_t s, cudaEvent_t ev0, cudaEvent_t ev1, int *launches) {
+    // distinct voxels one CTA can meet among its kSlots consecutive trials
+    int rows_cap = kSlots;
+    if (!w.trial_voxel && !w.diag && w.n_or > 0) rows_cap = (int)(w.n_or >= kSlots ? 2 : kSlots / w.n_or + 2);
+    if (rows_cap > kSlots) rows_cap = kSlots;
+    size_t offs[11];
+    const size_t smem = sweep_smem_layout(g.nhkl, rows_cap, offs);
+    const size_t smem_r = refine_smem_bytes(g.nrot, g.nhkl);
+    int per_sm = 0;
+    cudaError_t e = cudaFuncSetAttribute(sweep_kernel<HPL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sweep_kernel<HPL>, kThreads, smem);
+    if (e != cudaSuccess) return e;
+    if (per_sm < 1) return cudaErrorInvalidConfiguration;
+    int grid_r = 0;
+    e = prep_launch(refine_list_kernel<HPL, CodeT>, smem_r, num_sms, (int64_t)num_sms * 4, &grid_r);
+    if (e != cudaSuccess) return e;
+    const int64_t grid = (int64_t)per_sm * num_sms;
+    const int64_t per_round = grid * kSlots;
+    e = cudaMemsetAsync(b.work_counter, 0, 8 * sizeof(int), s);
+    if (e != cudaSuccess) return e;
+    if (ev0) cudaEventRecord(ev0, s);
+    for (int64_t base = 0; base < n_trials; base += per_round) {
+        const int64_t left = (n_trials - base + kSlots - 1) / kSlots;
+        const int gr = (int)(left < grid ? left : grid);
+        sweep_kernel<HPL><<<gr, kThreads, smem, s>>>(g, b, w, base, n_trials, rows_cap);
+        ++*launches;
+    }
+    if (ev1) cudaEventRecord(ev1, s);
+    refine_list_kernel<HPL, CodeT><<<grid_r, kThreads, smem_r, s>>>(g, b, w);
+    ++*launches;
     return cudaGetLastError();
 }
 
@@ -741,6 +1193,28 @@ cudaError_t launch_simulate_work(const Geo &g, const ScoreBufs &b, const Work &w
         case 4: return launch_mark_t<4>(g, b, w, num_sms, mask, s);
         default: return cudaErrorInvalidValue;
     }
+}
+
+int64_t sweep_round_trials(const Geo &g, int num_sms) {
+    // 16-bit per-slot counters and histogram bins; hit codes must stay below the saturation code
+    if (g.n_hit >= 255u || g.nhkl > 128 || (int64_t)g.nrot * g.nhkl > 65535) return 0;
+    return (int64_t)num_sms * GRC_SWEEP_BLOCKS * kSlots;
+}
+
+cudaError_t launch_sweep(const Geo &g, const ScoreBufs &b, const Work &w, int64_t n_trials, int num_sms,
+                         cudaStream_t s, cudaEvent_t ev0, cudaEvent_t ev1, int *launches) {
+    const int hpl = (g.nhkl + 31) / 32;
+    const bool c16 = g.code_bits <= 16;
+#define GRC_DISPATCH(H)                                                                                     \
+    if (hpl == H)                                                                                           \
+        return c16 ? launch_sweep_t<H, uint16_t>(g, b, w, n_trials, num_sms, s, ev0, ev1, launches)        \
+                   : launch_sweep_t<H, uint32_t>(g, b, w, n_trials, num_sms, s, ev0, ev1, launches);
+    GRC_DISPATCH(1)
+    GRC_DISPATCH(2)
+    GRC_DISPATCH(3)
+    GRC_DISPATCH(4)
+#undef GRC_DISPATCH
+    return cudaErrorInvalidValue;
 }
 
 }  // namespace grc

@@ -155,11 +155,21 @@ typedef struct {
     int64_t trials;          /* (voxel, orientation) pairs scored */
     int64_t refined;         /* trials whose median needed the exact refine pass */
     int64_t kernel_launches; /* kernels enqueued by the call */
-    double score_ms;         /* device time of the scoring kernel (CUDA events), 0 if not timed */
+    double score_ms;         /* device time of the scoring kernel(s) (CUDA events), 0 if not timed */
+    int64_t path;            /* 1 = per-trial kernel, 2 = projection-window sweep */
+    int64_t audit_checked;   /* audit builds only: FP32 decisions re-decided in FP64 */
+    int64_t audit_mismatch;  /* audit builds only: of those, decisions that differed */
 } grc_stats;
 int grc_last_stats(grc_ctx *ctx, grc_stats *out);
 /* 1 = record CUDA events around the scoring kernel of each call (for benchmarks). */
 int grc_set_timing(grc_ctx *ctx, int enable);
+/*
+ * Scoring kernel selection: 0 = by size (default: the projection-window sweep, which
+ * keeps the map windows L2-resident, once a call holds at least half a sweep round of
+ * trials; the per-trial kernel below that), 1 = always the per-trial kernel,
+ * 2 = always the sweep.  Results are identical; only speed differs.
+ */
+int grc_set_path(grc_ctx *ctx, int path);
 
 /* Counts of selected reflections per trial are exact; this reports the codes of the
  * resident map: number of distinct values, code width in bits. */
