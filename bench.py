@@ -37,6 +37,23 @@ N_ORIENT = 32768
 N_SEEDS = 20000
 
 
+def seed_range(step: int, rank: int, world: int, per_rank: int):
+    """Seed rows [start, stop) that ``rank`` scores in ``step`` (weak scaling, disjoint shards)."""
+    base = (step * world + rank) * per_rank
+    return base, base + per_rank
+
+
+def max_over_ranks(seconds: float, device=None) -> float:
+    """Max of a per-rank time over all ranks (the job's time); identity without a process group."""
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return float(seconds)
+    t = torch.tensor([seconds], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def env_rank():
     return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
 
@@ -188,8 +205,8 @@ def run_ours(args):
     stream = torch.cuda.ExternalStream(ctx.stream)
 
     def seed_slice(step):
-        base = (step * world + rank) * S
-        return d_pos[3 * base: 3 * (base + S)]
+        a, z = seed_range(step, rank, world, S)
+        return d_pos[3 * a: 3 * z]
 
     ctx.set_timing(True)
     for i in range(W):
@@ -215,10 +232,7 @@ def run_ours(args):
     if args.profile:
         ctx.close()
         return 0
-    t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    max_ms = float(t.item())
+    max_ms = max_over_ranks(total_ms, device="cuda")
     trials = K * S * N_ORIENT * world
     value = trials / (max_ms / 1e3)
     lookups = d_out.view(K, -1, 4)[:, :, 0].double().sum(dim=1).cpu().numpy()  # selected reflections per launch
@@ -236,14 +250,11 @@ def run_ours(args):
         dist.barrier()
     t0 = time.perf_counter()
     for i in range(e2e_steps):
-        base = ((W + i) * world + rank) * S
-        for j in range(S):
-            ctx.forward_comp(pos_host[base + j], q_host, S9, B9, hkl, None, rot, R9, p, out=out_host)
-    e2e_s = time.perf_counter() - t0
-    te = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(te, op=dist.ReduceOp.MAX)
-    e2e_val = e2e_steps * S * N_ORIENT * world / float(te.item())
+        a, z = seed_range(W + i, rank, world, S)
+        for j in range(a, z):
+            ctx.forward_comp(pos_host[j], q_host, S9, B9, hkl, None, rot, R9, p, out=out_host)
+    e2e_s = max_over_ranks(time.perf_counter() - t0, device="cuda")
+    e2e_val = e2e_steps * S * N_ORIENT * world / e2e_s
 
     peaks = {}
     try:
