@@ -25,8 +25,9 @@ EXPORTS = [
     "grc_upload_masks", "grc_upload_masks_device", "grc_set_geometry", "grc_forward_comp",
     "grc_grow_indexed_region", "grc_forward_comp_compete", "grc_forward_comp_device", "grc_grow_device",
     "grc_compete_device", "grc_last_stats", "grc_set_timing", "grc_set_path", "grc_mask_info", "grc_simulate_spots",
-    "grc_edt",
+    "grc_edt", "grc_forward_comp_noalloc",
 ]
+NOALLOC_MAX_ORIENTATIONS = 65536
 
 
 class GrcError(RuntimeError):
@@ -83,6 +84,7 @@ def load(path: str | None = None):
         "grc_mask_info": [vp, C.POINTER(i64), C.POINTER(i), C.POINTER(i64), C.POINTER(i64), C.POINTER(i64)],
         "grc_simulate_spots": [vp, f, f, i64, f],
         "grc_edt": [vp, f, i64, i64, i64, f],
+        "grc_forward_comp_noalloc": [vp, f, f, i64, f],
     }
     for name, args in sig.items():
         fn = getattr(L, name)
@@ -221,6 +223,11 @@ class Context:
         p1 = f32(param1)
         self._check(self.L.grc_compete_device(self.h, _ptr(d_rows5), m, _ptr(d_id), n_neigb, _ptr(d_euler),
                                               n_grain, _ptr(p1), _ptr(d_out), _ptr(d_trial_out)))
+
+    def forward_comp_noalloc(self, pos, d_q, n_q: int, d_out):
+        """Allocation-free seeding scan: host pos (3 floats), device d_q / d_out; see the C header."""
+        p = f32(pos)
+        self._check(self.L.grc_forward_comp_noalloc(self.h, _ptr(p), _ptr(d_q), n_q, _ptr(d_out)))
 
     def simulate_spots(self, d_pos, d_U, n: int, d_mask):
         self._check(self.L.grc_simulate_spots(self.h, _ptr(d_pos), _ptr(d_U), n, _ptr(d_mask)))

@@ -742,3 +742,93 @@ int grc_edt(grc_ctx *ctx, const uint8_t *d_mask, int64_t dz, int64_t dy, int64_t
 }
 
 }  // extern "C"
+
+// ---- allocation-free seeding scan ---------------------------------------------------
+// Some callers cannot allocate GPU memory at the point where they score: a MEX shim
+// living inside MATLAB's gpuArray memory manager, a host framework whose caching
+// allocator owns the device, or a tight per-seed loop where cudaMalloc/cudaFree would
+// synchronise the whole device.  grc_forward_comp_noalloc serves them from a fixed,
+// file-scope device array instead of the context's growable workspace.
+
+namespace {
+
+constexpr int64_t kNoAllocMaxQ = GRC_NOALLOC_MAX_ORIENTATIONS;
+constexpr size_t kNaGeo = 0;                                                   // grc::Geo
+constexpr size_t kNaCounters = (sizeof(grc::Geo) + 255) & ~size_t(255);       // 8 ints
+constexpr size_t kNaPos = kNaCounters + 256;                                   // 3 doubles
+constexpr size_t kNaU = kNaPos + 256;                                          // 9 doubles / orientation
+constexpr size_t kNaRes = kNaU + sizeof(double) * 9 * kNoAllocMaxQ;            // TrialRes / orientation
+constexpr size_t kNaBytes = kNaRes + sizeof(grc::TrialRes) * kNoAllocMaxQ;
+
+// Every GPU that loads this library holds this array until the process exits.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNaBytes];
+
+std::mutex g_noalloc_mu;
+void *g_noalloc_addr[64];  // device address of g_noalloc_scratch, per device ordinal
+
+// Device address of the scratch array on the current device (looked up once per device).
+int noalloc_scratch(grc_ctx *ctx, unsigned char **out) {
+    if (ctx->device < 0 || ctx->device >= 64) return fail(ctx, GRC_EINVAL, "noalloc: device ordinal out of range");
+    std::lock_guard<std::mutex> g(g_noalloc_mu);
+    if (!g_noalloc_addr[ctx->device]) {
+        void *p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess || !p)
+            return fail(ctx, GRC_ECUDA, "noalloc: cudaGetSymbolAddress failed: %s", cudaGetErrorString(e));
+        g_noalloc_addr[ctx->device] = p;
+    }
+    *out = (unsigned char *)g_noalloc_addr[ctx->device];
+    return GRC_OK;
+}
+
+}  // namespace
+
+extern "C" int grc_forward_comp_noalloc(grc_ctx *ctx, const float *pos, const float *d_q, int64_t n_q,
+                                        float *d_out) {
+    if (!ctx) return GRC_EINVAL;
+    Lock l(ctx);
+    if (!pos || (n_q > 0 && (!d_q || !d_out))) return fail(ctx, GRC_EINVAL, "noalloc: NULL argument");
+    if (n_q < 0) return fail(ctx, GRC_EINVAL, "noalloc: negative orientation count");
+    if (n_q > kNoAllocMaxQ)
+        return fail(ctx, GRC_ECAPACITY,
+                    "noalloc: %lld orientations exceed the fixed scratch of %lld (GRC_NOALLOC_MAX_ORIENTATIONS); "
+                    "split the call or use grc_forward_comp_device",
+                    (long long)n_q, (long long)kNoAllocMaxQ);
+    TRY(check_ready(ctx));
+    if (n_q == 0) return GRC_OK;
+    unsigned char *base = nullptr;
+    TRY(noalloc_scratch(ctx, &base));
+    ctx->stats = grc_stats{};
+    // The pinned geometry staging copy is reused; wait until no earlier copy still reads it.
+    CU(cudaStreamSynchronize(ctx->stream));
+    *ctx->geo_pinned = ctx->geo;
+    CU(cudaMemcpyAsync(base + kNaGeo, ctx->geo_pinned, sizeof(grc::Geo), cudaMemcpyHostToDevice, ctx->stream));
+    const double p[3] = {pos[0], pos[1], pos[2]};
+    CU(cudaMemcpyAsync(base + kNaPos, p, sizeof p, cudaMemcpyHostToDevice, ctx->stream));
+    CU(grc::launch_quat_to_u(d_q, n_q, (double *)(base + kNaU), ctx->stream));
+    grc::ScoreBufs b{};
+    b.geo = (const grc::Geo *)(base + kNaGeo);
+    b.rot_cs = (const double2 *)ctx->rot_cs.p;
+    b.hkl = (const double *)ctx->hkl.p;
+    b.vpos = (const double *)(base + kNaPos);
+    b.U = (const double *)(base + kNaU);
+    b.codes = ctx->mc.codes;
+    b.codes8 = ctx->mc.codes8;
+    b.vals = ctx->mc.vals;
+    b.res = (grc::TrialRes *)(base + kNaRes);
+    b.work_counter = (int *)(base + kNaCounters);  // zeroed by launch_score before its kernels
+    grc::Work w{};
+    w.n_or = n_q;
+    w.chunk = kSeedChunk;
+    w.chunks_per_voxel = (n_q + kSeedChunk - 1) / kSeedChunk;
+    w.n_items = w.chunks_per_voxel;
+    int launches = 0;
+    cudaError_t e = grc::launch_score(ctx->geo, b, w, ctx->num_sms, ctx->stream, nullptr, nullptr, &launches);
+    if (e != cudaSuccess) return fail(ctx, GRC_ECUDA, "noalloc scorer launch: %s", cudaGetErrorString(e));
+    CU(grc::launch_epi_forward(b.res, n_q, d_out, ctx->stream));
+    CU(cudaStreamSynchronize(ctx->stream));
+    ctx->stats.trials = n_q;
+    ctx->stats.kernel_launches = launches + 2;
+    ctx->stats.path = 1;
+    return GRC_OK;
+}

@@ -150,6 +150,28 @@ int grc_compete_device(grc_ctx *ctx, const float *d_rows5, int64_t m, const floa
                        const float *d_euler, int64_t n_grain, const float *param1, float *d_out,
                        float *d_trial_out);
 
+/*
+ * Allocation-free seeding scan (no counterpart in the reference: the MEX functions
+ * always allocate their gpuArray output).  For callers that must not allocate GPU
+ * memory while they score -- a MEX shim inside MATLAB's gpuArray memory manager, a
+ * framework whose caching allocator owns the device, a per-seed loop where cudaMalloc
+ * or cudaFree would synchronise the device.  Same results as grc_forward_comp for one
+ * voxel: pos is 3 host floats [mm]; d_q (4*n_q floats) and d_out (4*n_q floats) are
+ * caller-owned device buffers.  Geometry and distance map must already be resident
+ * (set up earlier with grc_set_geometry / grc_upload_masks).
+ *
+ * Its scratch is one fixed device array of about 5.8 MB, compiled into the library and
+ * held by every GPU that loads it until the process exits; n_q above
+ * GRC_NOALLOC_MAX_ORIENTATIONS is rejected with GRC_ECAPACITY.  The first call on a
+ * device looks up that array's device address (cudaGetSymbolAddress), so make that
+ * first call before any stream capture.  All calls in the process share the array and
+ * each call leaves its contents behind: calls that overlap on the GPU (from different
+ * contexts or threads on the same device) race and must be serialised by the caller.
+ * The call returns after its work has finished on the context stream.
+ */
+#define GRC_NOALLOC_MAX_ORIENTATIONS 65536
+int grc_forward_comp_noalloc(grc_ctx *ctx, const float *pos, const float *d_q, int64_t n_q, float *d_out);
+
 /* Statistics of the last scorer launch on this context. */
 typedef struct {
     int64_t trials;          /* (voxel, orientation) pairs scored */
