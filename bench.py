@@ -218,14 +218,16 @@ def run_ours(args):
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     score_ms = []
     launches = 0
+    path = 0
     with ClockSampler(local) as clk:
         torch.cuda.synchronize()
         ev0.record(stream)
         for i in range(K):
             ctx.forward_comp_device(seed_slice(W + i), S, d_q, N_ORIENT, d_out[i])
-            st = ctx.last_stats()  # reads the scoring kernel's CUDA events of this step
+            st = ctx.last_stats()  # reads the scoring kernels' CUDA events of this step
             score_ms.append(st["score_ms"])
-            launches += 5
+            launches += st["kernel_launches"]
+            path = st["path"]
         ev1.record(stream)
         torch.cuda.synchronize()
     total_ms = ev0.elapsed_time(ev1)
@@ -264,9 +266,11 @@ def run_ours(args):
     peak = peaks.get("hbm_gbs")
     peak_note = "measured hbm_gbs (MEASURED_PEAKS.json)" if peak else "fallback 6650 GB/s"
     peak = peak or 6650.0
+    kernel = "sweep_kernel" if path == 2 else "score_kernel"
     traffic = None
     try:
-        prof = json.load(open(os.path.join(ROOT, "profiles", "score_kernel_dram.json")))
+        # DRAM bytes per selected reflection measured by ncu on the same kernel (profiles/)
+        prof = json.load(open(os.path.join(ROOT, "profiles", f"{kernel}_dram.json")))
         traffic = float(np.mean(lookups)) * prof["dram_bytes_per_lookup"]
     except (OSError, KeyError, ValueError):
         pass
@@ -285,7 +289,7 @@ def run_ours(args):
                 "gpu_launches": launches,
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                              "frac": achieved / peak, "traffic": traffic,
-                             "kernel": "score_kernel", "peak_source": peak_note,
+                             "kernel": kernel, "peak_source": peak_note,
                              "algorithmic_bytes": "32 B (one sector) per selected reflection's map lookup",
                              "lookups_per_launch": float(np.mean(lookups)),
                              "score_ms_per_launch": float(np.mean(score_ms))},

@@ -241,12 +241,14 @@ __device__ __forceinline__ int64_t landing_fp32(const Geo &g, const RowF &r, con
         // far off the detector (or NaN): certain rejection only for finite values
         return (isfinite(u) && isfinite(v)) ? -1 : -2;
     }
-    const float fu = u - floorf(u), fv = v - floorf(v);
-    if (fabsf(fu - 0.5f) < kAmbigPx || fabsf(fv - 0.5f) < kAmbigPx) return -2;
-    const float ru = floorf(u + 0.5f), rv = floorf(v + 0.5f);  // exact away from the half-pixel band
+    // nearest integer; within the ambiguity band of a half-pixel the item goes to the
+    // exact path, so the tie rule of rintf never decides anything
+    const float ru = rintf(u), rv = rintf(v);
+    if (fabsf(u - ru) > 0.5f - kAmbigPx || fabsf(v - rv) > 0.5f - kAmbigPx) return -2;
     if (!(ru >= 1.0f && ru <= (float)g.detysize && rv >= 1.0f && rv <= (float)g.detzsize)) return -1;
     if (ru >= g.bsy0f && ru <= g.bsy1f && rv >= g.bsz0f && rv <= g.bsz1f) return -1;
-    return (int64_t)iw * g.plane + (int64_t)(ru - 1.0f) * g.detzsize + (int64_t)(rv - 1.0f);
+    const uint32_t in_plane = (uint32_t)((int)ru - 1) * (uint32_t)g.detzsize + (uint32_t)((int)rv - 1);
+    return (int64_t)iw * g.plane + in_plane;
 }
 
 // Counts + histogram of codes below kHistBins (scoring pass).
@@ -740,8 +742,8 @@ __device__ __forceinline__ float4 gw_of(const float *sf, const float4 h) {
 
 // Window on t = -(k_w . Gw) in FP32 (see window_of) from rG = 1/|G|; the 1e-5 |G|
 // margins dominate its FP32 rounding.
-__device__ __forceinline__ float4 window_f(const Geo &g, float rG) {
-    const float G = __frcp_rn(rG), G2 = G * G;
+__device__ __forceinline__ float4 window_f(const Geo &g, const float4 gv) {
+    const float G2 = gv.x * gv.x + gv.y * gv.y + gv.z * gv.z, G = G2 * gv.w;
     float lo = g.lo4pif * G2, hi = g.hi4pif * G2;
     if (g.cbmaxf > -1.0f) hi = fminf(hi, -g.cbmaxf * G);
     lo = fmaxf(lo, 0.0f);
@@ -751,10 +753,10 @@ __device__ __forceinline__ float4 window_f(const Geo &g, float rG) {
 
 template <int HPL>
 __global__ void __launch_bounds__(kThreads, GRC_SWEEP_BLOCKS) sweep_kernel(Geo g, ScoreBufs b, Work w, int64_t round_base,
-                                                            int64_t n_trials, int rows_cap) {
-    const int64_t cta_base = round_base + (int64_t)blockIdx.x * kSlots;
+                                                            int64_t n_trials, int rows_cap, int slots) {
+    const int64_t cta_base = round_base + (int64_t)blockIdx.x * slots;
     if (cta_base >= n_trials) return;
-    const int nslot = (int)min((int64_t)kSlots, n_trials - cta_base);
+    const int nslot = (int)min((int64_t)slots, n_trials - cta_base);
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const SweepSmem sm = sweep_carve(smem_raw, g.nhkl, rows_cap);
     __shared__ int s_nv;
@@ -851,7 +853,7 @@ __global__ void __launch_bounds__(kThreads, GRC_SWEEP_BLOCKS) sweep_kernel(Geo g
             const int s = (int)(item >> 16), wl = (int)((item >> 8) & 255u), ih = (int)(item & 255u);
             if (valid) {
                 const float4 gv = gw_of(sm.subf + 12 * s, sm.hk[ih]);
-                const float4 win = window_f(g, gv.w);
+                const float4 win = window_f(g, gv);
                 r = landing_fp32(g, sm.rows[sm.vloc[s] * kWin + wl], gv, win.z, win.w, w0 + wl);
 #ifdef GRC_AUDIT
                 // audit build: every certain FP32 decision is re-decided by the FP64 path
@@ -913,7 +915,7 @@ __global__ void __launch_bounds__(kThreads, GRC_SWEEP_BLOCKS) sweep_kernel(Geo g
 #pragma unroll
             for (int j = 0; j < HPL; ++j) {
                 const float4 gv = gw_of(sf, make_float4(hx[j], hy[j], hz[j], 0.f));
-                const float4 win = window_f(g, gv.w);
+                const float4 win = window_f(g, gv);
                 const bool real = lane + 32 * j < g.nhkl;
                 gx[j] = gv.x;
                 gy[j] = gv.y;
@@ -923,7 +925,8 @@ __global__ void __launch_bounds__(kThreads, GRC_SWEEP_BLOCKS) sweep_kernel(Geo g
             }
             const RowF *vr = sm.rows + sm.vloc[s] * kWin;
             for (int wl = 0; wl < nw; ++wl) {
-                const float kx = vr[wl].wx, ky = vr[wl].wy, kz = vr[wl].wz;
+                const float4 kwv = reinterpret_cast<const float4 *>(vr + wl)[3];
+                const float kx = kwv.x, ky = kwv.y, kz = kwv.z;
 #pragma unroll
                 for (int j = 0; j < HPL; ++j) {
                     const float t = -fmaf(kx, gx[j], fmaf(ky, gy[j], kz * gz[j]));
@@ -1123,14 +1126,18 @@ cudaError_t launch_sweep_t(const Geo &g, const ScoreBufs &b, const Work &w, int6
     e = prep_launch(refine_list_kernel<HPL, CodeT>, smem_r, num_sms, (int64_t)num_sms * 4, &grid_r);
     if (e != cudaSuccess) return e;
     const int64_t grid = (int64_t)per_sm * num_sms;
-    const int64_t per_round = grid * kSlots;
+    // rounds of equal size: slots per CTA chosen so the last round is not a sliver
+    const int64_t rounds = (n_trials + grid * kSlots - 1) / (grid * kSlots);
+    int slots = (int)((n_trials + rounds * grid - 1) / (rounds * grid));
+    if (slots < 1) slots = 1;
+    const int64_t per_round = grid * slots;
     e = cudaMemsetAsync(b.work_counter, 0, 8 * sizeof(int), s);
     if (e != cudaSuccess) return e;
     if (ev0) cudaEventRecord(ev0, s);
     for (int64_t base = 0; base < n_trials; base += per_round) {
-        const int64_t left = (n_trials - base + kSlots - 1) / kSlots;
+        const int64_t left = (n_trials - base + slots - 1) / slots;
         const int gr = (int)(left < grid ? left : grid);
-        sweep_kernel<HPL><<<gr, kThreads, smem, s>>>(g, b, w, base, n_trials, rows_cap);
+        sweep_kernel<HPL><<<gr, kThreads, smem, s>>>(g, b, w, base, n_trials, rows_cap, slots);
         ++*launches;
     }
     if (ev1) cudaEventRecord(ev1, s);
