@@ -25,7 +25,8 @@ EXPORTS = [
     "grc_upload_masks", "grc_upload_masks_device", "grc_set_geometry", "grc_forward_comp",
     "grc_grow_indexed_region", "grc_forward_comp_compete", "grc_forward_comp_device", "grc_grow_device",
     "grc_compete_device", "grc_last_stats", "grc_set_timing", "grc_set_path", "grc_mask_info", "grc_simulate_spots",
-    "grc_edt", "grc_forward_comp_noalloc",
+    "grc_edt", "grc_forward_comp_noalloc", "grc_batch_create", "grc_batch_set_maps", "grc_batch_run",
+    "grc_batch_capture", "grc_batch_replay", "grc_batch_autotune", "grc_batch_info", "grc_batch_destroy",
 ]
 NOALLOC_MAX_ORIENTATIONS = 65536
 
@@ -85,6 +86,14 @@ def load(path: str | None = None):
         "grc_simulate_spots": [vp, f, f, i64, f],
         "grc_edt": [vp, f, i64, i64, i64, f],
         "grc_forward_comp_noalloc": [vp, f, f, i64, f],
+        "grc_batch_create": [vp, f, i64, f, i64, f, i64, f, C.POINTER(vp)],
+        "grc_batch_set_maps": [vp, C.POINTER(i64), f, f, f, f, f],
+        "grc_batch_run": [vp, f, f],
+        "grc_batch_capture": [vp, f],
+        "grc_batch_replay": [vp],
+        "grc_batch_autotune": [vp, f, i64, C.POINTER(i), C.POINTER(i), C.POINTER(d)],
+        "grc_batch_info": [vp, C.POINTER(i64), C.POINTER(i64), C.POINTER(i), C.POINTER(i)],
+        "grc_batch_destroy": [vp],
     }
     for name, args in sig.items():
         fn = getattr(L, name)
@@ -229,6 +238,10 @@ class Context:
         p = f32(pos)
         self._check(self.L.grc_forward_comp_noalloc(self.h, _ptr(p), _ptr(d_q), n_q, _ptr(d_out)))
 
+    def batch(self, d_rows5, m: int, d_id, n_neigb: int, d_euler, n_grain: int, param1):
+        """Plan a batched-grow work list on device buffers (see Batch)."""
+        return Batch(self, d_rows5, m, d_id, n_neigb, d_euler, n_grain, param1)
+
     def simulate_spots(self, d_pos, d_U, n: int, d_mask):
         self._check(self.L.grc_simulate_spots(self.h, _ptr(d_pos), _ptr(d_U), n, _ptr(d_mask)))
 
@@ -255,3 +268,54 @@ class Context:
         self._check(self.L.grc_mask_info(self.h, C.byref(nd), C.byref(bits), C.byref(nz), C.byref(ny), C.byref(nr)))
         return {"n_distinct": nd.value, "code_bits": bits.value, "detzsize": nz.value, "detysize": ny.value,
                 "nrot": nr.value}
+
+
+class Batch:
+    """A planned batched-grow iteration (grc_batch_*): run, capture into a CUDA graph, replay, autotune."""
+
+    def __init__(self, ctx: Context, d_rows5, m, d_id, n_neigb, d_euler, n_grain, param1):
+        self.ctx, self.L = ctx, ctx.L
+        self._keep = (d_rows5, d_id, d_euler)  # borrowed device arrays must outlive the batch
+        p1 = f32(param1)
+        h = C.c_void_p()
+        ctx._check(self.L.grc_batch_create(ctx.h, _ptr(d_rows5), m, _ptr(d_id), n_neigb, _ptr(d_euler), n_grain,
+                                           _ptr(p1), C.byref(h)))
+        self.h = h
+
+    def info(self) -> dict:
+        m, T = C.c_int64(), C.c_int64()
+        p, s = C.c_int(), C.c_int()
+        self.ctx._check(self.L.grc_batch_info(self.h, C.byref(m), C.byref(T), C.byref(p), C.byref(s)))
+        return {"voxels": m.value, "trials": T.value, "path": p.value, "slots": s.value}
+
+    def set_maps(self, dims, completeness=None, grain_id=None, dismedian=None, ninter=None, visitflag=None):
+        d = (C.c_int64 * 3)(*[int(x) for x in dims])
+        self._maps = (completeness, grain_id, dismedian, ninter, visitflag)
+        self.ctx._check(self.L.grc_batch_set_maps(self.h, d, *[_ptr(x) for x in self._maps]))
+
+    def run(self, d_out8, d_trial_out=None):
+        self.ctx._check(self.L.grc_batch_run(self.h, _ptr(d_out8), _ptr(d_trial_out)))
+
+    def capture(self, d_out8):
+        self._graph_out = d_out8
+        self.ctx._check(self.L.grc_batch_capture(self.h, _ptr(d_out8)))
+
+    def replay(self):
+        self.ctx._check(self.L.grc_batch_replay(self.h))
+
+    def autotune(self, d_out8, max_voxels: int = 0) -> dict:
+        p, s, ms = C.c_int(), C.c_int(), C.c_double()
+        self.ctx._check(self.L.grc_batch_autotune(self.h, _ptr(d_out8), max_voxels, C.byref(p), C.byref(s),
+                                                  C.byref(ms)))
+        return {"path": p.value, "slots": s.value, "ms": ms.value}
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.grc_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -167,6 +167,23 @@ __global__ void epi_compete_k(const TrialRes *res, const longlong4 *items, const
     }
 }
 
+// grow_unindexed_compete_comp_cuda.m:51-64 on device: write each voxel's winner into the
+// sample maps (MATLAB column-major volumes, 1-based voxel indices in rows5).
+__global__ void apply_compete_k(const float *out8, const float *rows5, int64_t m, int64_t d1, int64_t d2,
+                                int64_t d3, float *comp, float *gid, float *dmed, float *ninter, float *visit) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < m; i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t x = (int64_t)rows5[5 * i] - 1, y = (int64_t)rows5[5 * i + 1] - 1, z = (int64_t)rows5[5 * i + 2] - 1;
+        if (x < 0 || y < 0 || z < 0 || x >= d1 || y >= d2 || z >= d3) continue;
+        const int64_t k = x + d1 * (y + d2 * z);
+        const float *o = out8 + 8 * i;
+        if (comp) comp[k] = o[5];
+        if (gid) gid[k] = o[4];
+        if (dmed) dmed[k] = o[7];
+        if (ninter) ninter[k] = o[6];
+        if (visit) visit[k] = 0.5f;
+    }
+}
+
 // ---- distance-map rank coding --------------------------------------------------
 // Each float maps to an order-preserving 32-bit key; a 2^32-bit presence bitmap
 // plus a prefix popcount gives every value its rank among the distinct values.
@@ -318,6 +335,13 @@ cudaError_t launch_csr_fill(const float *rows5, int64_t m, const int64_t *offset
 cudaError_t launch_epi_compete(const TrialRes *res, const longlong4 *items, const int32_t *trial_orient, int64_t m,
                                const float *euler, float *out8, float *trial_out4, cudaStream_t s) {
     epi_compete_k<<<blocks_for(m), kB, 0, s>>>(res, items, trial_orient, m, euler, out8, trial_out4);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_apply_compete(const float *out8, const float *rows5, int64_t m, const int64_t *dims, float *comp,
+                                 float *gid, float *dmed, float *ninter, float *visit, cudaStream_t s) {
+    apply_compete_k<<<blocks_for(m), kB, 0, s>>>(out8, rows5, m, dims[0], dims[1], dims[2], comp, gid, dmed, ninter,
+                                                 visit);
     return cudaGetLastError();
 }
 

@@ -832,3 +832,320 @@ extern "C" int grc_forward_comp_noalloc(grc_ctx *ctx, const float *pos, const fl
     ctx->stats.path = 1;
     return GRC_OK;
 }
+
+// ---- batched grower: planned CSR work list, graph capture, autotuned tile -------------
+// A grow iteration of grow_unindexed_compete_comp_cuda.m / revise_all_unindexed_voxel_cuda.m
+// scores every waiting voxel against its own uneven candidate list.  The plan below builds
+// the device work list once, so each iteration is a fixed sequence of kernels with no host
+// synchronisation: it can be replayed from a CUDA graph.
+
+struct grc_batch {
+    grc_ctx *ctx = nullptr;
+    int64_t m = 0, T = 0, n_grain = 0;
+    const float *rows5 = nullptr, *euler = nullptr;  // borrowed device arrays
+    DevBuf items, torient, tvoxel, res, pos, U, rlist, counter, offsets_h_dummy;
+    std::vector<int64_t> offsets;  // host copy of the CSR offsets (m + 1)
+    int path = 0, slots = 0;       // chosen tile (0 = by size)
+    float *maps[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+    int64_t dims[3] = {0, 0, 0};
+    DevBuf dims_dev;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    int graph_launches = 0;
+};
+
+namespace {
+
+uint64_t geo_hash(const grc_ctx *ctx) {
+    uint64_t h = 1469598103934665603ull;
+    for (float v : ctx->geo_key) {
+        uint32_t b;
+        std::memcpy(&b, &v, 4);
+        h = (h ^ b) * 1099511628211ull;
+    }
+    return h;
+}
+
+std::mutex g_tune_mu;
+std::vector<std::pair<uint64_t, std::pair<int, int>>> g_tune_cache;  // geometry hash -> (path, slots)
+
+int batch_enqueue(grc_batch *bt, float *d_out8, float *d_trial_out, int path, int slots, int64_t m_lim,
+                  cudaEvent_t e0, cudaEvent_t e1, int *launches) {
+    grc_ctx *ctx = bt->ctx;
+    const int64_t T = bt->offsets[m_lim];
+    grc::ScoreBufs b{};
+    b.geo = (const grc::Geo *)ctx->geo_dev.p;
+    b.rot_cs = (const double2 *)ctx->rot_cs.p;
+    b.hkl = (const double *)ctx->hkl.p;
+    b.vpos = (const double *)bt->pos.p;
+    b.U = (const double *)bt->U.p;
+    b.codes = ctx->mc.codes;
+    b.codes8 = ctx->mc.codes8;
+    b.vals = ctx->mc.vals;
+    b.res = (grc::TrialRes *)bt->res.p;
+    b.work_counter = (int *)bt->counter.p;
+    b.refine_list = (int64_t *)bt->rlist.p;
+    grc::Work w{};
+    w.items = (const longlong4 *)bt->items.p;
+    w.trial_orient = (const int32_t *)bt->torient.p;
+    w.trial_voxel = (const int32_t *)bt->tvoxel.p;
+    w.n_items = m_lim;
+    cudaError_t e = cudaSuccess;
+    if (T > 0) {
+        const bool sweep = path == 2 || (path == 0 && grc::sweep_round_trials(ctx->geo, ctx->num_sms) > 0 &&
+                                         T * 2 >= grc::sweep_round_trials(ctx->geo, ctx->num_sms));
+        if (sweep && grc::sweep_round_trials(ctx->geo, ctx->num_sms) > 0)
+            e = grc::launch_sweep(ctx->geo, b, w, T, ctx->num_sms, ctx->stream, e0, e1, launches, slots);
+        else
+            e = grc::launch_score(ctx->geo, b, w, ctx->num_sms, ctx->stream, e0, e1, launches);
+        if (e != cudaSuccess) return fail(ctx, GRC_ECUDA, "batch scorer launch: %s", cudaGetErrorString(e));
+    }
+    CU(grc::launch_epi_compete((const grc::TrialRes *)bt->res.p, (const longlong4 *)bt->items.p,
+                               (const int32_t *)bt->torient.p, m_lim, bt->euler, d_out8, d_trial_out, ctx->stream));
+    ++*launches;
+    if (bt->maps[0] || bt->maps[1] || bt->maps[2] || bt->maps[3] || bt->maps[4]) {
+        CU(grc::launch_apply_compete(d_out8, bt->rows5, m_lim, bt->dims, bt->maps[0], bt->maps[1], bt->maps[2],
+                                     bt->maps[3], bt->maps[4], ctx->stream));
+        ++*launches;
+    }
+    return GRC_OK;
+}
+
+}  // namespace
+
+extern "C" int grc_batch_create(grc_ctx *ctx, const float *d_rows5, int64_t m, const float *d_id, int64_t n_neigb,
+                                const float *d_euler, int64_t n_grain, const float *param1, grc_batch **out) {
+    if (!ctx || !out) return GRC_EINVAL;
+    *out = nullptr;
+    Lock l(ctx);
+    TRY(check_ready(ctx));
+    if (!param1 || m < 1 || !d_rows5 || !d_euler || n_grain < 1 || n_grain > (int64_t)INT32_MAX || n_neigb < 0)
+        return fail(ctx, GRC_EINVAL, "batch: bad arguments");
+    double p1[14] = {0};
+    for (int i = 0; i < 11; ++i) {
+        if (!std::isfinite(param1[i])) return fail(ctx, GRC_EINVAL, "param1(%d) is not finite", i + 1);
+        p1[i] = param1[i];
+    }
+    grc_batch *bt = new grc_batch();
+    bt->ctx = ctx;
+    bt->m = m;
+    bt->n_grain = n_grain;
+    bt->rows5 = d_rows5;
+    bt->euler = d_euler;
+    auto bail = [&](int rc) {
+        DevBuf *all[] = {&bt->items, &bt->torient, &bt->tvoxel, &bt->res, &bt->pos, &bt->U, &bt->rlist,
+                         &bt->counter, &bt->dims_dev};
+        for (DevBuf *d : all) cudaFree(d->p);
+        delete bt;
+        return rc;
+    };
+    int rc;
+    if ((rc = ensure(ctx, ctx->p1, sizeof(p1))) || (rc = ensure(ctx, bt->U, sizeof(double) * 9 * n_grain)) ||
+        (rc = ensure(ctx, bt->pos, sizeof(double) * 3 * m)) || (rc = ensure(ctx, ctx->counts, sizeof(int64_t) * m)) ||
+        (rc = ensure(ctx, ctx->offsets, sizeof(int64_t) * m)) || (rc = ensure(ctx, bt->items, sizeof(longlong4) * m)) ||
+        (rc = ensure(ctx, ctx->bad, sizeof(int))) || (rc = ensure(ctx, bt->counter, 8 * sizeof(int))))
+        return bail(rc);
+    cudaStream_t s = ctx->stream;
+    size_t tmp_bytes = 0;
+    int64_t last_off = 0, last_cnt = 0;
+    int hbad = 0;
+    cudaError_t e;
+#define BCK(x)                                                                                  \
+    do {                                                                                        \
+        e = (x);                                                                                \
+        if (e != cudaSuccess) return bail(fail(ctx, GRC_ECUDA, "batch: %s", cudaGetErrorString(e))); \
+    } while (0)
+    BCK(cudaMemcpyAsync(ctx->p1.p, p1, sizeof(p1), cudaMemcpyHostToDevice, s));
+    BCK(cudaMemsetAsync(ctx->bad.p, 0, sizeof(int), s));
+    BCK(grc::launch_euler_to_u(d_euler, n_grain, (double *)bt->U.p, s));
+    BCK(grc::launch_pos_rows(d_rows5, 5, m, (const double *)ctx->p1.p, (double *)bt->pos.p, s));
+    BCK(grc::launch_csr_counts(d_rows5, m, (int64_t *)ctx->counts.p, s));
+    BCK(cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, (int64_t *)ctx->counts.p, (int64_t *)ctx->offsets.p, m, s));
+    if ((rc = ensure(ctx, ctx->tmp, tmp_bytes))) return bail(rc);
+    BCK(cub::DeviceScan::ExclusiveSum(ctx->tmp.p, tmp_bytes, (int64_t *)ctx->counts.p, (int64_t *)ctx->offsets.p, m, s));
+    bt->offsets.resize(m + 1);
+    BCK(cudaMemcpyAsync(bt->offsets.data(), ctx->offsets.p, sizeof(int64_t) * m, cudaMemcpyDeviceToHost, s));
+    BCK(cudaMemcpyAsync(&last_cnt, (int64_t *)ctx->counts.p + (m - 1), 8, cudaMemcpyDeviceToHost, s));
+    BCK(cudaStreamSynchronize(s));
+    last_off = bt->offsets[m - 1];
+    bt->T = last_off + last_cnt;
+    bt->offsets[m] = bt->T;
+    const int64_t T = bt->T > 0 ? bt->T : 1;
+    if ((rc = ensure(ctx, bt->torient, sizeof(int32_t) * T)) || (rc = ensure(ctx, bt->tvoxel, sizeof(int32_t) * T)) ||
+        (rc = ensure(ctx, bt->res, sizeof(grc::TrialRes) * T)) || (rc = ensure(ctx, bt->rlist, sizeof(int64_t) * T)))
+        return bail(rc);
+    BCK(grc::launch_csr_fill(d_rows5, m, (const int64_t *)ctx->offsets.p, d_id, n_neigb, n_grain,
+                             (longlong4 *)bt->items.p, (int32_t *)bt->torient.p, (int32_t *)bt->tvoxel.p,
+                             (int *)ctx->bad.p, s));
+    BCK(cudaMemcpyAsync(&hbad, ctx->bad.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+    BCK(cudaStreamSynchronize(s));
+#undef BCK
+    if (hbad & 1) return bail(fail(ctx, GRC_EINVAL, "batch: a [first,last] range lies outside id_neigb_all"));
+    if (hbad & 2) return bail(fail(ctx, GRC_EINVAL, "batch: a grain id lies outside the Euler table"));
+    if ((rc = stage_geo(ctx))) return bail(rc);
+    if (cudaStreamSynchronize(s) != cudaSuccess) return bail(fail(ctx, GRC_ECUDA, "batch: sync failed"));
+    {
+        std::lock_guard<std::mutex> g(g_tune_mu);
+        const uint64_t h = geo_hash(ctx);
+        for (auto &kv : g_tune_cache)
+            if (kv.first == h) {
+                bt->path = kv.second.first;
+                bt->slots = kv.second.second;
+            }
+    }
+    *out = bt;
+    return GRC_OK;
+}
+
+extern "C" int grc_batch_set_maps(grc_batch *bt, const int64_t *dims, float *d_completeness, float *d_grain_id,
+                                  float *d_dismedian, float *d_ninter, float *d_visitflag) {
+    if (!bt || !dims) return GRC_EINVAL;
+    Lock l(bt->ctx);
+    for (int i = 0; i < 3; ++i) {
+        if (dims[i] < 1) return fail(bt->ctx, GRC_EINVAL, "batch maps: dimensions must be positive");
+        bt->dims[i] = dims[i];
+    }
+    bt->maps[0] = d_completeness;
+    bt->maps[1] = d_grain_id;
+    bt->maps[2] = d_dismedian;
+    bt->maps[3] = d_ninter;
+    bt->maps[4] = d_visitflag;
+    return GRC_OK;
+}
+
+extern "C" int grc_batch_run(grc_batch *bt, float *d_out8, float *d_trial_out) {
+    if (!bt || !d_out8) return GRC_EINVAL;
+    grc_ctx *ctx = bt->ctx;
+    Lock l(ctx);
+    ctx->stats = grc_stats{};
+    int launches = 0;
+    cudaEvent_t e0 = ctx->timing ? ctx->ev0 : nullptr, e1 = ctx->timing ? ctx->ev1 : nullptr;
+    TRY(batch_enqueue(bt, d_out8, d_trial_out, bt->path, bt->slots, bt->m, e0, e1, &launches));
+    ctx->timed_last = ctx->timing;
+    ctx->stats.trials = bt->T;
+    ctx->stats.kernel_launches = launches;
+    return GRC_OK;
+}
+
+extern "C" int grc_batch_capture(grc_batch *bt, float *d_out8) {
+    if (!bt || !d_out8) return GRC_EINVAL;
+    grc_ctx *ctx = bt->ctx;
+    Lock l(ctx);
+    CU(cudaStreamSynchronize(ctx->stream));
+    if (bt->exec) {
+        cudaGraphExecDestroy(bt->exec);
+        bt->exec = nullptr;
+    }
+    if (bt->graph) {
+        cudaGraphDestroy(bt->graph);
+        bt->graph = nullptr;
+    }
+    CU(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+    int launches = 0;
+    const int rc = batch_enqueue(bt, d_out8, nullptr, bt->path, bt->slots, bt->m, nullptr, nullptr, &launches);
+    cudaGraph_t g = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(ctx->stream, &g);
+    if (rc != GRC_OK) {
+        if (g) cudaGraphDestroy(g);
+        return rc;
+    }
+    if (e != cudaSuccess) return fail(ctx, GRC_ECUDA, "batch capture: %s", cudaGetErrorString(e));
+    bt->graph = g;
+    CU(cudaGraphInstantiate(&bt->exec, g, 0));
+    bt->graph_launches = launches;
+    return GRC_OK;
+}
+
+extern "C" int grc_batch_replay(grc_batch *bt) {
+    if (!bt) return GRC_EINVAL;
+    grc_ctx *ctx = bt->ctx;
+    Lock l(ctx);
+    if (!bt->exec) return fail(ctx, GRC_EINVAL, "batch: no captured graph");
+    ctx->stats = grc_stats{};
+    CU(cudaGraphLaunch(bt->exec, ctx->stream));
+    ctx->stats.trials = bt->T;
+    ctx->stats.kernel_launches = bt->graph_launches;
+    return GRC_OK;
+}
+
+extern "C" int grc_batch_autotune(grc_batch *bt, float *d_out8, int64_t max_voxels, int *path_out, int *slots_out,
+                                  double *ms_out) {
+    if (!bt || !d_out8) return GRC_EINVAL;
+    grc_ctx *ctx = bt->ctx;
+    Lock l(ctx);
+    int64_t m_lim = bt->m;
+    if (max_voxels > 0 && max_voxels < m_lim) m_lim = max_voxels;
+    struct Cand {
+        int path, slots;
+    };
+    const Cand cands[] = {{1, 0}, {2, 16}, {2, 32}, {2, 48}, {2, 64}};
+    cudaEvent_t a, z;
+    CU(cudaEventCreate(&a));
+    CU(cudaEventCreate(&z));
+    double best = 1e300;
+    Cand pick{0, 0};
+    int rc = GRC_OK;
+    for (const Cand &c : cands) {
+        if (c.path == 2 && grc::sweep_round_trials(ctx->geo, ctx->num_sms) == 0) continue;
+        double t_best = 1e300;
+        for (int rep = 0; rep < 2 && rc == GRC_OK; ++rep) {
+            int launches = 0;
+            cudaEventRecord(a, ctx->stream);
+            rc = batch_enqueue(bt, d_out8, nullptr, c.path, c.slots, m_lim, nullptr, nullptr, &launches);
+            cudaEventRecord(z, ctx->stream);
+            if (cudaEventSynchronize(z) != cudaSuccess) rc = fail(ctx, GRC_ECUDA, "autotune: sync failed");
+            float ms = 0;
+            cudaEventElapsedTime(&ms, a, z);
+            if (rep > 0 || true) t_best = std::min(t_best, (double)ms);
+        }
+        if (rc != GRC_OK) break;
+        if (t_best < best) {
+            best = t_best;
+            pick = c;
+        }
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(z);
+    if (rc != GRC_OK) return rc;
+    bt->path = pick.path;
+    bt->slots = pick.slots;
+    {
+        std::lock_guard<std::mutex> g(g_tune_mu);
+        const uint64_t h = geo_hash(ctx);
+        bool found = false;
+        for (auto &kv : g_tune_cache)
+            if (kv.first == h) {
+                kv.second = {pick.path, pick.slots};
+                found = true;
+            }
+        if (!found) g_tune_cache.push_back({h, {pick.path, pick.slots}});
+    }
+    if (path_out) *path_out = pick.path;
+    if (slots_out) *slots_out = pick.slots;
+    if (ms_out) *ms_out = best;
+    return GRC_OK;
+}
+
+extern "C" int grc_batch_info(grc_batch *bt, int64_t *n_voxels, int64_t *n_trials, int *path, int *slots) {
+    if (!bt) return GRC_EINVAL;
+    if (n_voxels) *n_voxels = bt->m;
+    if (n_trials) *n_trials = bt->T;
+    if (path) *path = bt->path;
+    if (slots) *slots = bt->slots;
+    return GRC_OK;
+}
+
+extern "C" int grc_batch_destroy(grc_batch *bt) {
+    if (!bt) return GRC_EINVAL;
+    {
+        Lock l(bt->ctx);
+        cudaStreamSynchronize(bt->ctx->stream);
+        if (bt->exec) cudaGraphExecDestroy(bt->exec);
+        if (bt->graph) cudaGraphDestroy(bt->graph);
+        DevBuf *all[] = {&bt->items, &bt->torient, &bt->tvoxel, &bt->res, &bt->pos, &bt->U, &bt->rlist,
+                         &bt->counter, &bt->dims_dev};
+        for (DevBuf *d : all) cudaFree(d->p);
+    }
+    delete bt;
+    return GRC_OK;
+}

@@ -82,8 +82,9 @@ cudaError_t launch_score(const Geo &g, const ScoreBufs &b, const Work &w, int nu
 // cannot serve this geometry.
 int64_t sweep_round_trials(const Geo &g, int num_sms);
 // Enqueue the projection-window sweep over n_trials trials (+ the list refine pass).
+// max_slots (1..64) caps the trials each CTA holds per round (tile height); 0 = 64.
 cudaError_t launch_sweep(const Geo &g, const ScoreBufs &b, const Work &w, int64_t n_trials, int num_sms,
-                         cudaStream_t s, cudaEvent_t ev0, cudaEvent_t ev1, int *launches);
+                         cudaStream_t s, cudaEvent_t ev0, cudaEvent_t ev1, int *launches, int max_slots = 0);
 
 // Orientation / position preparation kernels.
 cudaError_t launch_quat_to_u(const float *q, int64_t n, double *U, cudaStream_t s);
@@ -104,6 +105,10 @@ cudaError_t launch_csr_fill(const float *rows5, int64_t m, const int64_t *offset
                             int32_t *trial_voxel, int *bad, cudaStream_t s);
 cudaError_t launch_epi_compete(const TrialRes *res, const longlong4 *items, const int32_t *trial_orient,
                                int64_t m, const float *euler, float *out8, float *trial_out4, cudaStream_t s);
+
+// Device update of the sample maps with compete winners (rows5 1-based indices).
+cudaError_t launch_apply_compete(const float *out8, const float *rows5, int64_t m, const int64_t *dims, float *comp,
+                                 float *gid, float *dmed, float *ninter, float *visit, cudaStream_t s);
 
 // Distance-map rank coding.
 struct MapCodes {

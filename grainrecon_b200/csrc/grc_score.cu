@@ -1108,7 +1108,7 @@ cudaError_t launch_score_t(const Geo &g, const ScoreBufs &b, const Work &w, int 
 
 template <int HPL, typename CodeT>
 cudaError_t launch_sweep_t(const Geo &g, const ScoreBufs &b, const Work &w, int64_t n_trials, int num_sms,
-                           cudaStream_t s, cudaEvent_t ev0, cudaEvent_t ev1, int *launches) {
+                           cudaStream_t s, cudaEvent_t ev0, cudaEvent_t ev1, int *launches, int max_slots) {
     // distinct voxels one CTA can meet among its kSlots consecutive trials
     int rows_cap = kSlots;
     if (!w.trial_voxel && !w.diag && w.n_or > 0) rows_cap = (int)(w.n_or >= kSlots ? 2 : kSlots / w.n_or + 2);
@@ -1127,7 +1127,8 @@ cudaError_t launch_sweep_t(const Geo &g, const ScoreBufs &b, const Work &w, int6
     if (e != cudaSuccess) return e;
     const int64_t grid = (int64_t)per_sm * num_sms;
     // rounds of equal size: slots per CTA chosen so the last round is not a sliver
-    const int64_t rounds = (n_trials + grid * kSlots - 1) / (grid * kSlots);
+    if (max_slots < 1 || max_slots > kSlots) max_slots = kSlots;
+    const int64_t rounds = (n_trials + grid * max_slots - 1) / (grid * max_slots);
     int slots = (int)((n_trials + rounds * grid - 1) / (rounds * grid));
     if (slots < 1) slots = 1;
     const int64_t per_round = grid * slots;
@@ -1209,13 +1210,13 @@ int64_t sweep_round_trials(const Geo &g, int num_sms) {
 }
 
 cudaError_t launch_sweep(const Geo &g, const ScoreBufs &b, const Work &w, int64_t n_trials, int num_sms,
-                         cudaStream_t s, cudaEvent_t ev0, cudaEvent_t ev1, int *launches) {
+                         cudaStream_t s, cudaEvent_t ev0, cudaEvent_t ev1, int *launches, int max_slots) {
     const int hpl = (g.nhkl + 31) / 32;
     const bool c16 = g.code_bits <= 16;
 #define GRC_DISPATCH(H)                                                                                     \
     if (hpl == H)                                                                                           \
-        return c16 ? launch_sweep_t<H, uint16_t>(g, b, w, n_trials, num_sms, s, ev0, ev1, launches)        \
-                   : launch_sweep_t<H, uint32_t>(g, b, w, n_trials, num_sms, s, ev0, ev1, launches);
+        return c16 ? launch_sweep_t<H, uint16_t>(g, b, w, n_trials, num_sms, s, ev0, ev1, launches, max_slots) \
+                   : launch_sweep_t<H, uint32_t>(g, b, w, n_trials, num_sms, s, ev0, ev1, launches, max_slots);
     GRC_DISPATCH(1)
     GRC_DISPATCH(2)
     GRC_DISPATCH(3)

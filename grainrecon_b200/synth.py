@@ -313,3 +313,57 @@ def device_maps(sample: Sample, ctx, keep_host_map: bool = False):
     del d_map
     torch.cuda.empty_cache()
     return host
+
+
+def _rot_small(rng, n, sigma_deg):
+    """n random rotations with Gaussian angle (sigma_deg) about uniformly random axes."""
+    ax = rng.normal(size=(n, 3))
+    ax /= np.linalg.norm(ax, axis=1, keepdims=True)
+    ang = np.radians(rng.normal(0.0, sigma_deg, n))
+    K = np.zeros((n, 3, 3))
+    K[:, 0, 1], K[:, 0, 2], K[:, 1, 2] = -ax[:, 2], ax[:, 1], -ax[:, 0]
+    K[:, 1, 0], K[:, 2, 0], K[:, 2, 1] = ax[:, 2], -ax[:, 1], ax[:, 0]
+    s, c = np.sin(ang)[:, None, None], np.cos(ang)[:, None, None]
+    return np.eye(3)[None] + s * K + (1 - c) * (K @ K)
+
+
+def compete_worklist(sample: Sample, seed: int = 0, p: float = 0.15, kmax: int = 64, n_variants: int = 32,
+                     sigma_deg: float = 0.5, voxels: np.ndarray | None = None):
+    """Uneven candidate lists for the batched grower (cuda_forward_comp_compete layout).
+
+    Every voxel gets k ~ Geometric(p) candidates truncated to [1, kmax]; each candidate is
+    the orientation of the voxel's own grain or of a face-neighbour's grain, either exact
+    or one of ``n_variants`` copies perturbed by a Gaussian ``sigma_deg`` rotation.
+    Returns (rows5 [m x 5: x y z first last], id_neigb [1-based rows of euler], euler
+    [n_entries x 3, degrees]) as float32 arrays.
+    """
+    rng = np.random.default_rng(seed)
+    gid = sample.grain_id
+    idx = sample.voxel_indices() if voxels is None else np.asarray(voxels, np.int64)
+    m = len(idx)
+    ng = len(sample.grain_q)
+    # Euler table: grain g (1-based), variant v (0 = exact) -> row (g-1)*(n_variants+1)+v
+    Ug = np.stack([G.quat_to_u(q) for q in sample.grain_q])
+    rows = []
+    for g in range(ng):
+        R = _rot_small(rng, n_variants, sigma_deg)
+        rows.append(np.concatenate([Ug[g][None], R @ Ug[g]], 0))
+    Uall = np.concatenate(rows, 0)
+    euler = (np.degrees(np.stack([G.u_to_euler(u) for u in Uall])) % 360).astype(np.float32)
+    k = np.minimum(rng.geometric(p, m), kmax)
+    off = np.concatenate([[0], np.cumsum(k)])
+    n = int(off[-1])
+    vox_of = np.repeat(np.arange(m), k)
+    shifts = np.array([[0, 0, 0], [1, 0, 0], [-1, 0, 0], [0, 1, 0], [0, -1, 0], [0, 0, 1], [0, 0, -1]])
+    sh = shifts[rng.integers(0, len(shifts), n)]
+    nb = np.clip(idx[vox_of] - 1 + sh, 0, np.array(gid.shape) - 1)
+    g_nb = gid[nb[:, 0], nb[:, 1], nb[:, 2]]
+    g_own = gid[idx[vox_of, 0] - 1, idx[vox_of, 1] - 1, idx[vox_of, 2] - 1]
+    g = np.where(g_nb > 0, g_nb, g_own).astype(np.int64)
+    var = rng.integers(0, n_variants + 1, n)
+    id_neigb = ((g - 1) * (n_variants + 1) + var + 1).astype(np.float32)
+    rows5 = np.zeros((m, 5), np.float32)
+    rows5[:, :3] = idx
+    rows5[:, 3] = off[:-1] + 1
+    rows5[:, 4] = off[1:]
+    return rows5, id_neigb, euler

@@ -172,6 +172,34 @@ int grc_compete_device(grc_ctx *ctx, const float *d_rows5, int64_t m, const floa
 #define GRC_NOALLOC_MAX_ORIENTATIONS 65536
 int grc_forward_comp_noalloc(grc_ctx *ctx, const float *pos, const float *d_q, int64_t n_q, float *d_out);
 
+/*
+ * Batched grower (uneven candidate sets; the grow iteration of
+ * grow_unindexed_compete_comp_cuda.m:3-65 / revise_all_unindexed_voxel_cuda.m).
+ * grc_batch_create builds the CSR work list of a fixed voxel set once (device rows5,
+ * id_neigb, euler, as grc_compete_device; they must stay valid while the batch lives) and
+ * binds it to the context's current geometry and map, which must not change while the
+ * batch lives.  grc_batch_run enqueues one iteration (scoring of every candidate, the
+ * per-voxel argmax into d_out8, and the optional map update) with no host
+ * synchronisation; grc_batch_capture records that sequence into a CUDA graph that
+ * grc_batch_replay launches.  grc_batch_autotune times the scoring tile shapes
+ * (per-trial kernel, or the projection-window sweep holding 16/32/48/64 trials per CTA)
+ * on the first max_voxels voxels, keeps the fastest for this batch and caches it per
+ * geometry for later batches.  grc_batch_set_maps makes every run also write each
+ * voxel's completeness, grain id, dis_median, Nr_intersect and VisitFlag = 0.5 into
+ * device volumes (float, dims[0] x dims[1] x dims[2], column-major, any may be NULL).
+ */
+typedef struct grc_batch grc_batch;
+int grc_batch_create(grc_ctx *ctx, const float *d_rows5, int64_t m, const float *d_id_neigb, int64_t n_neigb,
+                     const float *d_euler, int64_t n_grain, const float *param1, grc_batch **out);
+int grc_batch_set_maps(grc_batch *batch, const int64_t *dims, float *d_completeness, float *d_grain_id,
+                       float *d_dismedian, float *d_ninter, float *d_visitflag);
+int grc_batch_run(grc_batch *batch, float *d_out8, float *d_trial_out);
+int grc_batch_capture(grc_batch *batch, float *d_out8);
+int grc_batch_replay(grc_batch *batch);
+int grc_batch_autotune(grc_batch *batch, float *d_out8, int64_t max_voxels, int *path, int *slots, double *best_ms);
+int grc_batch_info(grc_batch *batch, int64_t *n_voxels, int64_t *n_trials, int *path, int *slots);
+int grc_batch_destroy(grc_batch *batch);
+
 /* Statistics of the last scorer launch on this context. */
 typedef struct {
     int64_t trials;          /* (voxel, orientation) pairs scored */
