@@ -27,6 +27,9 @@ EXPORTS = [
     "grc_compete_device", "grc_last_stats", "grc_set_timing", "grc_set_path", "grc_mask_info", "grc_simulate_spots",
     "grc_edt", "grc_forward_comp_noalloc", "grc_batch_create", "grc_batch_set_maps", "grc_batch_run",
     "grc_batch_capture", "grc_batch_replay", "grc_batch_autotune", "grc_batch_info", "grc_batch_destroy",
+    "grc_fit_spot_count", "grc_fit_spot_fill", "grc_centroid_residual_adjoint", "grc_fit_grains_lm",
+    "grc_fit_grains_nm", "grc_fit_grains_rms", "grc_fit_geometry_lm", "grc_fit_geometry_cost",
+    "grc_fit_geometry_rms",
 ]
 NOALLOC_MAX_ORIENTATIONS = 65536
 
@@ -94,6 +97,15 @@ def load(path: str | None = None):
         "grc_batch_autotune": [vp, f, i64, C.POINTER(i), C.POINTER(i), C.POINTER(d)],
         "grc_batch_info": [vp, C.POINTER(i64), C.POINTER(i64), C.POINTER(i), C.POINTER(i)],
         "grc_batch_destroy": [vp],
+        "grc_fit_spot_count": [vp, f, f, i64, f],
+        "grc_fit_spot_fill": [vp, f, f, i64, f, f, f, f, f],
+        "grc_centroid_residual_adjoint": [vp, i, f, f, f, f, f, f, i64, f, f],
+        "grc_fit_grains_lm": [vp, f, f, i64, f, f, f, f, i64, f, f, i, C.POINTER(i)],
+        "grc_fit_grains_nm": [vp, f, f, i64, f, f, f, f, i64, f, f, i, i, f, i],
+        "grc_fit_grains_rms": [vp, f, f, f, i64, f, f, f, f, i64, f, f],
+        "grc_fit_geometry_lm": [vp, f, i, f, f, f, f, f, i64, f, i, C.POINTER(i)],
+        "grc_fit_geometry_cost": [vp, f, i, f, f, f, f, f, i64, f],
+        "grc_fit_geometry_rms": [vp, f, i, f, f, f, f, f, f, i64, f],
     }
     for name, args in sig.items():
         fn = getattr(L, name)

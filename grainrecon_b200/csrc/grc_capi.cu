@@ -13,6 +13,7 @@
 #include <vector>
 
 #include "grainrecon_b200.h"
+#include "grc_fit.h"
 #include "grc_internal.h"
 
 namespace {
@@ -41,7 +42,7 @@ struct grc_ctx {
     grc::MapCodes mc{};
     int64_t mz = 0, my = 0, mrot = 0;
     std::vector<float> h_vals;
-    DevBuf geo_dev, rot_cs, hkl, pos, U, res, tvoxel, rlist, in1, in2, in3, out, items, torient, counts, offsets, tmp, counter, p1, bad;
+    DevBuf fgeo, fne, ftrial, fcost0, fcost1, fimp, fhw, geo_dev, rot_cs, hkl, pos, U, res, tvoxel, rlist, in1, in2, in3, out, items, torient, counts, offsets, tmp, counter, p1, bad;
     grc::Geo *geo_pinned = nullptr;  // staging of the per-launch geometry copy
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     bool timing = false;
@@ -489,7 +490,8 @@ int grc_ctx_destroy(grc_ctx *ctx) {
         Lock l(ctx);
         cudaStreamSynchronize(ctx->stream);
         cudaFreeHost(ctx->geo_pinned);
-        DevBuf *all[] = {&ctx->tvoxel, &ctx->rlist, &ctx->geo_dev, &ctx->rot_cs, &ctx->hkl, &ctx->pos, &ctx->U, &ctx->res, &ctx->in1, &ctx->in2,
+        DevBuf *all[] = {&ctx->fgeo, &ctx->fne, &ctx->ftrial, &ctx->fcost0, &ctx->fcost1, &ctx->fimp, &ctx->fhw,
+                         &ctx->tvoxel, &ctx->rlist, &ctx->geo_dev, &ctx->rot_cs, &ctx->hkl, &ctx->pos, &ctx->U, &ctx->res, &ctx->in1, &ctx->in2,
                          &ctx->in3, &ctx->out, &ctx->items, &ctx->torient, &ctx->counts, &ctx->offsets,
                          &ctx->tmp, &ctx->counter, &ctx->p1, &ctx->bad};
         for (DevBuf *b : all) cudaFree(b->p);
@@ -1147,5 +1149,232 @@ extern "C" int grc_batch_destroy(grc_batch *bt) {
         for (DevBuf *d : all) cudaFree(d->p);
     }
     delete bt;
+    return GRC_OK;
+}
+
+
+// ---- spot-centroid residual, its derivatives and the fits ---------------------------
+namespace {
+
+int fit_prepare(grc_ctx *ctx, const double *geo10, grc::FitFixed *fx) {
+    if (!ctx->has_geo) return fail(ctx, GRC_EINVAL, "fit: no geometry set");
+    const grc::Geo &g = ctx->geo;
+    for (int i = 0; i < 9; ++i) {
+        fx->S[i] = g.S[i];
+        fx->B[i] = g.B[i];
+    }
+    fx->pxy = g.pxy;
+    fx->pxz = g.pxz;
+    fx->dety0 = g.dety0;
+    fx->detz0 = g.detz0;
+    fx->lmin = g.lmin;
+    fx->lmax = g.lmax;
+    fx->cbmax = g.cbmax;
+    fx->detysize = g.detysize;
+    fx->detzsize = g.detzsize;
+    fx->nrot = g.nrot;
+    fx->nhkl = g.nhkl;
+    fx->rot_cs = (const double2 *)ctx->rot_cs.p;
+    fx->hkl = (const double *)ctx->hkl.p;
+    if (geo10) {
+        for (int i = 0; i < 10; ++i)
+            if (!std::isfinite(geo10[i])) return fail(ctx, GRC_EINVAL, "fit: geometry parameter %d is not finite", i);
+        TRY(ensure(ctx, ctx->fgeo, sizeof(double) * 10));
+        CU(cudaMemcpyAsync(ctx->fgeo.p, geo10, sizeof(double) * 10, cudaMemcpyHostToDevice, ctx->stream));
+    }
+    return GRC_OK;
+}
+
+grc::SpotList spots_of(const int32_t *g, const int32_t *w, const int32_t *h, const double *uv, int64_t n) {
+    grc::SpotList sp;
+    sp.grain = const_cast<int32_t *>(g);
+    sp.iw = const_cast<int32_t *>(w);
+    sp.ih = const_cast<int32_t *>(h);
+    sp.uv = const_cast<double *>(uv);
+    sp.n = n;
+    return sp;
+}
+
+}  // namespace
+
+extern "C" int grc_fit_spot_count(grc_ctx *ctx, const double *geo10, const double *d_grains, int64_t n_grains,
+                                  int64_t *d_counts) {
+    if (!ctx) return GRC_EINVAL;
+    Lock l(ctx);
+    if (!geo10 || !d_grains || !d_counts || n_grains < 0) return fail(ctx, GRC_EINVAL, "fit: bad arguments");
+    grc::FitFixed fx;
+    TRY(fit_prepare(ctx, geo10, &fx));
+    if (n_grains == 0) return GRC_OK;
+    CU(grc::fit_spots_count(fx, d_grains, (const double *)ctx->fgeo.p, n_grains, d_counts, ctx->stream));
+    CU(cudaStreamSynchronize(ctx->stream));
+    return GRC_OK;
+}
+
+extern "C" int grc_fit_spot_fill(grc_ctx *ctx, const double *geo10, const double *d_grains, int64_t n_grains,
+                                 const int64_t *d_offsets, int32_t *d_grain, int32_t *d_iw, int32_t *d_ih,
+                                 double *d_uv) {
+    if (!ctx) return GRC_EINVAL;
+    Lock l(ctx);
+    if (!geo10 || !d_grains || !d_offsets || !d_grain || !d_iw || !d_ih || !d_uv || n_grains < 0)
+        return fail(ctx, GRC_EINVAL, "fit: bad arguments");
+    grc::FitFixed fx;
+    TRY(fit_prepare(ctx, geo10, &fx));
+    if (n_grains == 0) return GRC_OK;
+    CU(grc::fit_spots_fill(fx, d_grains, (const double *)ctx->fgeo.p, n_grains, d_offsets,
+                           spots_of(d_grain, d_iw, d_ih, d_uv, 0), ctx->stream));
+    CU(cudaStreamSynchronize(ctx->stream));
+    return GRC_OK;
+}
+
+extern "C" int grc_centroid_residual_adjoint(grc_ctx *ctx, int mode, const double *geo10, const double *d_grains,
+                                             const int32_t *d_grain, const int32_t *d_iw, const int32_t *d_ih,
+                                             const double *d_uv, int64_t n_spots, double *d_res, double *d_jac) {
+    if (!ctx) return GRC_EINVAL;
+    Lock l(ctx);
+    if (mode != 0 && mode != 1) return fail(ctx, GRC_EINVAL, "fit: mode must be 0 (grain) or 1 (geometry)");
+    if (!geo10 || !d_grains || n_spots < 0 || (n_spots > 0 && (!d_grain || !d_iw || !d_ih || !d_uv || !d_res || !d_jac)))
+        return fail(ctx, GRC_EINVAL, "fit: bad arguments");
+    grc::FitFixed fx;
+    TRY(fit_prepare(ctx, geo10, &fx));
+    if (n_spots == 0) return GRC_OK;
+    CU(grc::fit_residual_jacobian(fx, mode, d_grains, (const double *)ctx->fgeo.p,
+                                  spots_of(d_grain, d_iw, d_ih, d_uv, n_spots), d_res, d_jac, ctx->stream));
+    CU(cudaStreamSynchronize(ctx->stream));
+    return GRC_OK;
+}
+
+extern "C" int grc_fit_grains_lm(grc_ctx *ctx, const double *geo10, double *d_grains, int64_t n_grains,
+                                 const int32_t *d_grain, const int32_t *d_iw, const int32_t *d_ih, const double *d_uv,
+                                 int64_t n_spots, const int64_t *d_offsets, double *d_lambda, int iters,
+                                 int *n_improved) {
+    if (!ctx) return GRC_EINVAL;
+    Lock l(ctx);
+    if (!geo10 || !d_grains || !d_offsets || !d_lambda || n_grains < 1 || iters < 0)
+        return fail(ctx, GRC_EINVAL, "fit: bad arguments");
+    grc::FitFixed fx;
+    TRY(fit_prepare(ctx, geo10, &fx));
+    TRY(ensure(ctx, ctx->fne, sizeof(double) * 29 * n_grains));
+    TRY(ensure(ctx, ctx->ftrial, sizeof(double) * 6 * n_grains));
+    TRY(ensure(ctx, ctx->fcost0, sizeof(double) * 2 * n_grains));
+    TRY(ensure(ctx, ctx->fcost1, sizeof(double) * 2 * n_grains));
+    TRY(ensure(ctx, ctx->fimp, sizeof(int)));
+    const grc::SpotList sp = spots_of(d_grain, d_iw, d_ih, d_uv, n_spots);
+    const double *g10 = (const double *)ctx->fgeo.p;
+    int improved = 0;
+    for (int it = 0; it < iters; ++it) {
+        CU(cudaMemsetAsync(ctx->fimp.p, 0, sizeof(int), ctx->stream));
+        CU(grc::fit_grain_normal(fx, d_grains, g10, sp, d_offsets, n_grains, (double *)ctx->fne.p, ctx->stream));
+        CU(grc::fit_grain_cost(fx, d_grains, g10, sp, d_offsets, n_grains, (double *)ctx->fcost0.p, ctx->stream));
+        CU(grc::fit_grain_lm_propose(d_grains, (const double *)ctx->fne.p, d_lambda, n_grains,
+                                     (double *)ctx->ftrial.p, ctx->stream));
+        CU(grc::fit_grain_cost(fx, (const double *)ctx->ftrial.p, g10, sp, d_offsets, n_grains,
+                               (double *)ctx->fcost1.p, ctx->stream));
+        CU(grc::fit_grain_lm_accept(d_grains, (const double *)ctx->ftrial.p, (const double *)ctx->fcost0.p,
+                                    (const double *)ctx->fcost1.p, d_lambda, n_grains, (int *)ctx->fimp.p,
+                                    ctx->stream));
+        CU(cudaMemcpyAsync(&improved, ctx->fimp.p, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+        CU(cudaStreamSynchronize(ctx->stream));
+        if (improved == 0) break;
+    }
+    if (n_improved) *n_improved = improved;
+    return GRC_OK;
+}
+
+extern "C" int grc_fit_grains_nm(grc_ctx *ctx, const double *geo10, double *d_grains, int64_t n_grains,
+                                 const int32_t *d_grain, const int32_t *d_iw, const int32_t *d_ih, const double *d_uv,
+                                 int64_t n_spots, const int64_t *d_offsets, const double *half_width, int max_evals,
+                                 int checkpoint, double *d_trace, int n_ck) {
+    if (!ctx) return GRC_EINVAL;
+    Lock l(ctx);
+    if (!geo10 || !d_grains || !d_offsets || !half_width || n_grains < 1 || max_evals < 7 ||
+        (d_trace && (checkpoint < 1 || n_ck < 1)))
+        return fail(ctx, GRC_EINVAL, "fit: bad arguments");
+    grc::FitFixed fx;
+    TRY(fit_prepare(ctx, geo10, &fx));
+    TRY(ensure(ctx, ctx->fhw, sizeof(double) * 6));
+    CU(cudaMemcpyAsync(ctx->fhw.p, half_width, sizeof(double) * 6, cudaMemcpyHostToDevice, ctx->stream));
+    CU(grc::fit_grain_nm(fx, d_grains, (const double *)ctx->fgeo.p, spots_of(d_grain, d_iw, d_ih, d_uv, n_spots),
+                         d_offsets, n_grains, (const double *)ctx->fhw.p, max_evals, checkpoint, d_trace,
+                         d_trace ? n_ck : 0, ctx->stream));
+    CU(cudaStreamSynchronize(ctx->stream));
+    return GRC_OK;
+}
+
+extern "C" int grc_fit_grains_rms(grc_ctx *ctx, const double *geo10, const double *d_grains, const double *d_truth,
+                                  int64_t n_grains, const int32_t *d_grain, const int32_t *d_iw, const int32_t *d_ih,
+                                  const double *d_uv, int64_t n_spots, const int64_t *d_offsets, double *d_rms) {
+    if (!ctx) return GRC_EINVAL;
+    Lock l(ctx);
+    if (!geo10 || !d_grains || !d_truth || !d_offsets || !d_rms || n_grains < 1)
+        return fail(ctx, GRC_EINVAL, "fit: bad arguments");
+    grc::FitFixed fx;
+    TRY(fit_prepare(ctx, geo10, &fx));
+    CU(grc::fit_grain_rms(fx, d_grains, d_truth, (const double *)ctx->fgeo.p,
+                          spots_of(d_grain, d_iw, d_ih, d_uv, n_spots), d_offsets, n_grains, d_rms, ctx->stream));
+    CU(cudaStreamSynchronize(ctx->stream));
+    return GRC_OK;
+}
+
+extern "C" int grc_fit_geometry_lm(grc_ctx *ctx, double *d_starts, int n_starts, const double *d_grains,
+                                   const int32_t *d_grain, const int32_t *d_iw, const int32_t *d_ih, const double *d_uv,
+                                   int64_t n_spots, double *d_lambda, int iters, int *n_improved) {
+    if (!ctx) return GRC_EINVAL;
+    Lock l(ctx);
+    if (!d_starts || !d_grains || !d_lambda || n_starts < 1 || n_starts > 65535 || iters < 0 || n_spots < 1)
+        return fail(ctx, GRC_EINVAL, "fit: bad arguments");
+    grc::FitFixed fx;
+    TRY(fit_prepare(ctx, nullptr, &fx));
+    TRY(ensure(ctx, ctx->fne, sizeof(double) * 67 * n_starts));
+    TRY(ensure(ctx, ctx->ftrial, sizeof(double) * 10 * n_starts));
+    TRY(ensure(ctx, ctx->fcost0, sizeof(double) * 2 * n_starts));
+    TRY(ensure(ctx, ctx->fcost1, sizeof(double) * 2 * n_starts));
+    TRY(ensure(ctx, ctx->fimp, sizeof(int)));
+    const grc::SpotList sp = spots_of(d_grain, d_iw, d_ih, d_uv, n_spots);
+    int improved = 0;
+    for (int it = 0; it < iters; ++it) {
+        CU(cudaMemsetAsync(ctx->fimp.p, 0, sizeof(int), ctx->stream));
+        CU(grc::fit_geo_normal(fx, d_grains, d_starts, n_starts, sp, (double *)ctx->fne.p, ctx->num_sms, ctx->stream));
+        CU(grc::fit_geo_cost(fx, d_grains, d_starts, n_starts, sp, (double *)ctx->fcost0.p, ctx->num_sms, ctx->stream));
+        CU(grc::fit_geo_lm_propose(d_starts, (const double *)ctx->fne.p, d_lambda, n_starts, (double *)ctx->ftrial.p,
+                                   ctx->stream));
+        CU(grc::fit_geo_cost(fx, d_grains, (const double *)ctx->ftrial.p, n_starts, sp, (double *)ctx->fcost1.p,
+                             ctx->num_sms, ctx->stream));
+        CU(grc::fit_geo_lm_accept(d_starts, (const double *)ctx->ftrial.p, (const double *)ctx->fcost0.p,
+                                  (const double *)ctx->fcost1.p, d_lambda, n_starts, (int *)ctx->fimp.p, ctx->stream));
+        CU(cudaMemcpyAsync(&improved, ctx->fimp.p, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+        CU(cudaStreamSynchronize(ctx->stream));
+        if (improved == 0) break;
+    }
+    if (n_improved) *n_improved = improved;
+    return GRC_OK;
+}
+
+extern "C" int grc_fit_geometry_cost(grc_ctx *ctx, const double *d_points, int n_points, const double *d_grains,
+                                     const int32_t *d_grain, const int32_t *d_iw, const int32_t *d_ih,
+                                     const double *d_uv, int64_t n_spots, double *d_cost) {
+    if (!ctx) return GRC_EINVAL;
+    Lock l(ctx);
+    if (!d_points || !d_grains || !d_cost || n_points < 1 || n_points > 65535 || n_spots < 1)
+        return fail(ctx, GRC_EINVAL, "fit: bad arguments");
+    grc::FitFixed fx;
+    TRY(fit_prepare(ctx, nullptr, &fx));
+    CU(grc::fit_geo_cost(fx, d_grains, d_points, n_points, spots_of(d_grain, d_iw, d_ih, d_uv, n_spots), d_cost,
+                         ctx->num_sms, ctx->stream));
+    CU(cudaStreamSynchronize(ctx->stream));
+    return GRC_OK;
+}
+
+extern "C" int grc_fit_geometry_rms(grc_ctx *ctx, const double *d_starts, int n_starts, const double *geo_truth10,
+                                    const double *d_grains, const int32_t *d_grain, const int32_t *d_iw,
+                                    const int32_t *d_ih, const double *d_uv, int64_t n_spots, double *d_acc) {
+    if (!ctx) return GRC_EINVAL;
+    Lock l(ctx);
+    if (!d_starts || !geo_truth10 || !d_grains || !d_acc || n_starts < 1 || n_starts > 65535 || n_spots < 1)
+        return fail(ctx, GRC_EINVAL, "fit: bad arguments");
+    grc::FitFixed fx;
+    TRY(fit_prepare(ctx, geo_truth10, &fx));
+    CU(grc::fit_geo_rms(fx, d_grains, d_starts, n_starts, (const double *)ctx->fgeo.p,
+                        spots_of(d_grain, d_iw, d_ih, d_uv, n_spots), d_acc, ctx->num_sms, ctx->stream));
+    CU(cudaStreamSynchronize(ctx->stream));
     return GRC_OK;
 }

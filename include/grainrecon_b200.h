@@ -200,6 +200,65 @@ int grc_batch_autotune(grc_batch *batch, float *d_out8, int64_t max_voxels, int 
 int grc_batch_info(grc_batch *batch, int64_t *n_voxels, int64_t *n_trials, int *path, int *slots);
 int grc_batch_destroy(grc_batch *batch);
 
+/*
+ * Spot-centroid fits (replace fminsearchbnd in fit_OR_constrain_* / fit_grain_COM.m and
+ * GrainMapping_fit_geo.m / L_shift_tilt_fitting.m).  The residual of a matched spot is the
+ * continuous landing point (u, v) [pixel] of forward_comp.m:28-59 (no rounding) minus the
+ * measured centroid.  Fixed geometry (S, B, hkl, rot_angles, pixel sizes, detector size,
+ * beam centre, wavelength window) comes from grc_set_geometry / grc_set_options; the fitted
+ * quantities are doubles:
+ *   grain  (6 per grain): Rodrigues vector r (U from q0 = 1/sqrt(1+|r|^2), q = r q0), centre [mm]
+ *   geo10: Lsam2sou, Lsam2det, dety00, detz00, tilt_x, tilt_y, tilt_z [deg] (RotDet = Rz*Ry*Rx,
+ *          get_det_R.m:1-7), P0y, P0z, RotAxisOffset.
+ * Spots: d_grain (0-based grain index), d_iw (omega index), d_ih (hkl index) int32, d_uv
+ * (2 doubles, measured centroid); for per-grain fits the spots of a grain are contiguous and
+ * d_offsets (n_grains+1) delimits them.  All pointers named d_* are device memory.
+ */
+/* Synthetic matched spots: count / fill the selected landings of each grain (no noise). */
+int grc_fit_spot_count(grc_ctx *ctx, const double *geo10, const double *d_grains, int64_t n_grains,
+                       int64_t *d_counts);
+int grc_fit_spot_fill(grc_ctx *ctx, const double *geo10, const double *d_grains, int64_t n_grains,
+                      const int64_t *d_offsets, int32_t *d_grain, int32_t *d_iw, int32_t *d_ih, double *d_uv);
+/*
+ * Residuals (model - measured, 2 per spot) and Jacobian rows d(u,v)/d(params) (2*K per
+ * spot, u row then v row) by hand-propagated FP64 tangents; mode 0: K = 6 grain parameters,
+ * mode 1: K = 10 geometry parameters.  The loss gradient is J^T r.  A spot that leaves the
+ * wavelength window or the detector gets NaN residuals.
+ */
+int grc_centroid_residual_adjoint(grc_ctx *ctx, int mode, const double *geo10, const double *d_grains,
+                                  const int32_t *d_grain, const int32_t *d_iw, const int32_t *d_ih,
+                                  const double *d_uv, int64_t n_spots, double *d_res, double *d_jac);
+/* Levenberg-Marquardt on every grain (6x6 FP64 normal equations per grain), `iters` iterations
+ * or until no grain improves; d_lambda (one damping value per grain) carries over calls. */
+int grc_fit_grains_lm(grc_ctx *ctx, const double *geo10, double *d_grains, int64_t n_grains, const int32_t *d_grain,
+                      const int32_t *d_iw, const int32_t *d_ih, const double *d_uv, int64_t n_spots,
+                      const int64_t *d_offsets, double *d_lambda, int iters, int *n_improved);
+/* Forward-only baseline: batched Nelder-Mead with fminsearchbnd's sine bound transform
+ * (fminsearchbnd.m:263-265) inside [start - half_width, start + half_width]; d_trace (optional)
+ * receives the best point every `checkpoint` evaluations (n_ck x n_grains x 6). */
+int grc_fit_grains_nm(grc_ctx *ctx, const double *geo10, double *d_grains, int64_t n_grains, const int32_t *d_grain,
+                      const int32_t *d_iw, const int32_t *d_ih, const double *d_uv, int64_t n_spots,
+                      const int64_t *d_offsets, const double *half_width, int max_evals, int checkpoint,
+                      double *d_trace, int n_ck);
+/* Per-grain RMS distance [pixel] of the predicted spots of d_grains from those of d_truth. */
+int grc_fit_grains_rms(grc_ctx *ctx, const double *geo10, const double *d_grains, const double *d_truth,
+                       int64_t n_grains, const int32_t *d_grain, const int32_t *d_iw, const int32_t *d_ih,
+                       const double *d_uv, int64_t n_spots, const int64_t *d_offsets, double *d_rms);
+/* Levenberg-Marquardt on the 10 geometry parameters of n_starts starting points at once (10x10
+ * FP64 normal equations reduced over all spots per start); grains held fixed. */
+int grc_fit_geometry_lm(grc_ctx *ctx, double *d_starts, int n_starts, const double *d_grains, const int32_t *d_grain,
+                        const int32_t *d_iw, const int32_t *d_ih, const double *d_uv, int64_t n_spots,
+                        double *d_lambda, int iters, int *n_improved);
+/* Sum of squared residuals and spot count (2 doubles) of each geometry point (forward only). */
+int grc_fit_geometry_cost(grc_ctx *ctx, const double *d_points, int n_points, const double *d_grains,
+                          const int32_t *d_grain, const int32_t *d_iw, const int32_t *d_ih, const double *d_uv,
+                          int64_t n_spots, double *d_cost);
+/* Sum of squared distances and count (2 doubles per start) of predicted spots from those of the
+ * geometry geo_truth10 (host). */
+int grc_fit_geometry_rms(grc_ctx *ctx, const double *d_starts, int n_starts, const double *geo_truth10,
+                         const double *d_grains, const int32_t *d_grain, const int32_t *d_iw, const int32_t *d_ih,
+                         const double *d_uv, int64_t n_spots, double *d_acc);
+
 /* Statistics of the last scorer launch on this context. */
 typedef struct {
     int64_t trials;          /* (voxel, orientation) pairs scored */

@@ -39,8 +39,8 @@ def build() -> str:
 def lib():
     global _lib
     if _lib is None:
-        if not os.path.exists(_LIB_PATH) or (
-                os.path.getmtime(_LIB_PATH) < os.path.getmtime(os.path.join(_HERE, "grc_oracle.c"))):
+        srcs = [os.path.join(_HERE, f) for f in ("grc_oracle.c", "grc_fit_oracle.c")]
+        if not os.path.exists(_LIB_PATH) or any(os.path.getmtime(_LIB_PATH) < os.path.getmtime(f) for f in srcs):
             build()
         L = C.CDLL(_LIB_PATH)
         d, i64, i = C.c_double, C.c_int64, C.c_int
@@ -55,6 +55,7 @@ def lib():
         L.oracle_compete.argtypes = [_f32p, i64, _f32p, _f32p, _f32p, _f32p, _f32p, _f32p, _f32p, _f32p,
                                      _f32p, _f32p, d, d, d, i, _f32p, _i32p]
         L.oracle_max_threads.restype = i
+        L.oracle_fit_uv_jac.argtypes = [i, _f64p, _f64p, _f64p, _f64p, _f64p, d, d, d, d, d, _f64p, _f64p, _f64p]
         _lib = L
     return _lib
 
@@ -144,3 +145,16 @@ def compete(rows5, id_neigb, euler, S, B, hkl, proj_bin_bw, rot_angles, RotDet, 
 
 def max_threads() -> int:
     return int(lib().oracle_max_threads())
+
+
+def fit_uv_jac(mode, grain6, geo10, S, B, h, omega_deg, pxy, pxz, dety0, detz0):
+    """Landing (u, v) and Jacobian rows (ju, jv) of one spot by complex step (FP64).
+
+    mode 0: 6 grain parameters (Rodrigues, centre); mode 1: 10 geometry parameters.
+    S, B: 3x3 (row-major), h: (h, k, l)."""
+    K = 6 if mode == 0 else 10
+    uv, ju, jv = np.zeros(2), np.zeros(K), np.zeros(K)
+    f64 = lambda a: np.ascontiguousarray(a, dtype=np.float64).reshape(-1)
+    lib().oracle_fit_uv_jac(mode, f64(grain6), f64(geo10), f64(S), f64(B), f64(h), float(omega_deg), float(pxy),
+                            float(pxz), float(dety0), float(detz0), uv, ju, jv)
+    return uv, ju, jv
