@@ -381,13 +381,89 @@ def run_grow(args):
     return 0
 
 
+def verify_fitted_completeness(ctx, fitted_geo10, seed, n_vox=64, n_or=1024):
+    """Score the al400 sample's masks with the true and with the fitted geometry.
+
+    Trials: ``n_vox`` sample voxels x (their grain's true orientation + ``n_or - 1`` random
+    ones).  Returns the mean and max |C_fitted - C_true| and the share of trials whose
+    (Nr_simu, Nr_intersect) did not change."""
+    from grainrecon_b200 import fit as F
+    from grainrecon_b200 import geometry as G
+    from grainrecon_b200 import synth
+    s = synth.make_sample("al400", seed=seed)
+    synth.device_maps(s, ctx)
+    idx = s.voxel_indices()
+    rng = np.random.default_rng(seed + 17)
+    pick = idx[rng.choice(len(idx), n_vox, replace=False)]
+    gid = s.grain_id[pick[:, 0] - 1, pick[:, 1] - 1, pick[:, 2] - 1]
+    pos = s.vol.pos_of_index(pick).astype(np.float32)
+    rand_q = G.cubic_fz_orientations(n_or - 1, seed + 23).astype(np.float32)
+    S9, B9, hkl, rot, R9, p = s.mex_arrays()
+    gf = F.geometry_with(s.geom, fitted_geo10)
+    R9f, pf = G.flat_rowmajor(gf.rot_det), gf.param20(s.nhkl)
+    dc, same, hit_true = [], 0, 0
+    for v in range(n_vox):
+        q = np.concatenate([s.grain_q[gid[v] - 1][None].astype(np.float32), rand_q]).reshape(-1)
+        a = ctx.forward_comp(pos[v], q, S9, B9, hkl, None, rot, R9, p).reshape(-1, 4)
+        b = ctx.forward_comp(pos[v], q, S9, B9, hkl, None, rot, R9f, pf).reshape(-1, 4)
+        ca, cb = np.nan_to_num(a[:, 2]), np.nan_to_num(b[:, 2])
+        dc.append(np.abs(ca - cb))
+        same += int(np.all(a[:, 0:2] == b[:, 0:2], axis=1).sum())
+        hit_true += int(ca[0] > 0.9)
+    dc = np.concatenate(dc)
+    return {"trials": n_vox * n_or, "mean_abs_dC": float(dc.mean()), "max_abs_dC": float(dc.max()),
+            "unchanged_trials": same / (n_vox * n_or), "true_orientation_C>0.9_voxels": hit_true}
+
+
+def run_fit(args):
+    """Fit benchmarks: 5,000-grain orientation+centre fit (BCC Fe, 1024^2, 181 projections) or the
+    10-parameter geometry fit (FCC Al, 2048^2, 361 projections, 2,000 grains, 64 starts)."""
+    import torch
+    from grainrecon_b200 import fit as F
+    from grainrecon_b200 import synth
+    from grainrecon_b200._lib import Context
+
+    rank, world, local = env_rank()
+    torch.cuda.set_device(local)
+    kind = "fe6" if args.config == "fe-fit" else "al400"
+    # the named set-up's geometry and lattice; a fit needs no volume or masks
+    geom, cell, _, hkl, *_ = synth.named_setup(kind, seed=args.seed)
+    from grainrecon_b200 import geometry as G
+    ctx = Context(local)
+    ctx.set_geometry(G.flat_rowmajor(np.eye(3)), G.flat_rowmajor(G.form_b(cell)), G.flat_hkl(hkl),
+                     np.asarray(geom.rot_angles, np.float32), G.flat_rowmajor(geom.rot_det), geom.param20(len(hkl)))
+    if args.config == "fe-fit":
+        res = F.bench_grain_fit(ctx, geom, n_grains=args.fit_grains or 5000, seed=args.seed)
+        lm = res["lm"]["reached"]
+        metric = f"fit time to 0.1 px RMS (orientation + centre, {res['grains']} grains)"
+    else:
+        res = F.bench_geometry_fit(ctx, geom, n_grains=args.fit_grains or 2000, seed=args.seed,
+                                   nm_iters=args.nm_iters)
+        lm = res["lm"]["first_start_below"]
+        res.pop("grains_array")
+        fitted = res.pop("fitted_geo")
+        res["fitted_geo"] = fitted.tolist()
+        if not args.no_verify:
+            res["completeness_with_fitted_geometry"] = verify_fitted_completeness(ctx, fitted, args.seed)
+        metric = f"fit time to 0.1 px RMS (10-parameter geometry, {res['starts']} starts)"
+    line = {"metric": metric, "value": lm["seconds"] if lm else None, "unit": "s", "n_gpus": 1,
+            "higher_is_better": False, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": args.config, "geometry": kind}, "result": res}
+    print(json.dumps(line, default=float), flush=True)
+    ctx.close()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="al400", choices=["al400", "fe6", "al400-grow"])
+    ap.add_argument("--config", default="al400", choices=["al400", "fe6", "al400-grow", "fe-fit", "al-geofit"])
+    ap.add_argument("--fit-grains", type=int, default=0, help="0: 5,000 (fe-fit) or 2,000 (al-geofit)")
+    ap.add_argument("--no-verify", action="store_true", help="al-geofit: skip the completeness re-check")
+    ap.add_argument("--nm-iters", type=int, default=400)
     ap.add_argument("--grow-voxels", type=int, default=262144, help="voxels per batched-grow iteration")
     ap.add_argument("--plain-voxels", type=int, default=2000, help="voxels timed one call each")
     ap.add_argument("--seeds", type=int, default=64, help="seed voxels per step per GPU")
@@ -402,6 +478,8 @@ def main():
         return run_reference(args)
     if args.config == "al400-grow":
         return run_grow(args)
+    if args.config in ("fe-fit", "al-geofit"):
+        return run_fit(args)
     return run_ours(args)
 
 

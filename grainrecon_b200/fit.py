@@ -24,6 +24,14 @@ def geo10_of(geom: G.Geometry) -> np.ndarray:
                      geom.rot_axis_offset], dtype=np.float64)
 
 
+def geometry_with(geom: G.Geometry, geo10) -> G.Geometry:
+    """A copy of ``geom`` carrying the 10 fitted parameters ``geo10``."""
+    import dataclasses
+    g = [float(v) for v in geo10]
+    return dataclasses.replace(geom, lss=g[0], lsd=g[1], dety00=g[2], detz00=g[3], tilt=(g[4], g[5], g[6]),
+                               p0y=g[7], p0z=g[8], rot_axis_offset=g[9])
+
+
 def quat_to_rod(q) -> np.ndarray:
     q = np.asarray(q, dtype=np.float64)
     return q[..., 1:] / q[..., :1]
@@ -246,3 +254,154 @@ class BatchedNelderMead:
                 fv = self._f(self.S[:, v])
                 self.evals += 1
                 self.F[shrink, v] = fv[shrink]
+
+
+# ---- benchmarks: time to 0.1 px RMS, Levenberg-Marquardt vs forward-only Nelder-Mead --------
+
+def _pooled_rms(rms, counts):
+    rms, counts = np.asarray(rms, float), np.asarray(counts, float)
+    ok = np.isfinite(rms)
+    return float(np.sqrt((counts[ok] * rms[ok] ** 2).sum() / counts[ok].sum()))
+
+
+def bench_grain_fit(ctx, geom: G.Geometry, n_grains=5000, noise_px=0.5, deg=1.0, shift_mm=0.005, seed=1,
+                    radius_mm=0.05, height_mm=0.1, nm_evals=4000, nm_checkpoint=100, target_px=0.1):
+    """Orientation + centre fit of many grains: time to reach ``target_px`` pooled RMS.
+
+    Measured centroids = ground-truth landing + N(0, noise_px); starts rotated by ``deg`` and
+    moved by ``shift_mm``.  RMS is the distance of the fitted model's spots from the
+    ground-truth spots (the noise floor does not count)."""
+    import time
+
+    import torch
+    geo = geo10_of(geom)
+    truth = random_grains(n_grains, radius_mm, height_mm, seed)
+    d_truth = torch.from_numpy(truth.reshape(-1).copy()).cuda()
+    spots = simulate_spots(ctx, geo, d_truth, noise_px, seed + 1)
+    counts = (spots.offsets[1:] - spots.offsets[:-1]).cpu().numpy()
+    start = perturb_grains(truth, deg, shift_mm, seed + 2)
+    out = {"grains": n_grains, "spots": spots.n, "noise_px": noise_px, "start": f"{deg} deg, {shift_mm * 1e3} um"}
+
+    d = torch.from_numpy(start.reshape(-1).copy()).cuda()
+    lam = torch.full((n_grains,), 1e-3, dtype=torch.float64, device="cuda")
+    out["rms_start"] = _pooled_rms(grains_rms(ctx, geo, d, d_truth, spots).cpu().numpy(), counts)
+    t_fit, it, hist = 0.0, 0, []
+    reached = None
+    while it < 30:
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        improved = grains_lm(ctx, geo, d, spots, lam, 1)
+        torch.cuda.synchronize()
+        t_fit += time.perf_counter() - t0
+        it += 1
+        r = grains_rms(ctx, geo, d, d_truth, spots).cpu().numpy()
+        pr = _pooled_rms(r, counts)
+        hist.append(pr)
+        if reached is None and pr <= target_px:
+            reached = {"seconds": t_fit, "iterations": it, "rms": pr, "frac_grains_below": float((r <= target_px).mean())}
+        if improved == 0:
+            break
+    out["lm"] = {"reached": reached, "final_rms": hist[-1], "iterations_run": it, "seconds_run": t_fit,
+                 "rms_history": hist[:12]}
+
+    d = torch.from_numpy(start.reshape(-1).copy()).cuda()
+    n_ck = nm_evals // nm_checkpoint
+    trace = torch.zeros(n_ck * n_grains * 6, dtype=torch.float64, device="cuda")
+    hw = np.array([0.03, 0.03, 0.03, 0.02, 0.02, 0.02])  # fminsearchbnd bounds: ~3.4 deg, 20 um
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    grains_nm(ctx, geo, d, spots, hw, nm_evals, nm_checkpoint, trace)
+    torch.cuda.synchronize()
+    t_nm = time.perf_counter() - t0
+    tr = trace.view(n_ck, n_grains * 6)
+    nm_hist, nm_reached = [], None
+    for k in range(n_ck):
+        r = grains_rms(ctx, geo, tr[k].contiguous(), d_truth, spots).cpu().numpy()
+        pr = _pooled_rms(r, counts)
+        nm_hist.append(pr)
+        if nm_reached is None and pr <= target_px:
+            ev = (k + 1) * nm_checkpoint
+            nm_reached = {"seconds": t_nm * ev / nm_evals, "evaluations": ev, "rms": pr,
+                          "frac_grains_below": float((r <= target_px).mean())}
+    out["nm"] = {"reached": nm_reached, "evaluations_run": nm_evals, "seconds_run": t_nm, "final_rms": nm_hist[-1],
+                 "rms_every_checkpoint": nm_hist[:: max(1, n_ck // 10)]}
+    if reached and nm_reached:
+        out["speedup_lm_vs_nm"] = nm_reached["seconds"] / reached["seconds"]
+    elif reached:
+        out["speedup_lm_vs_nm_lower_bound"] = t_nm / reached["seconds"]
+    return out
+
+
+def bench_geometry_fit(ctx, geom: G.Geometry, n_grains=2000, n_starts=64, noise_px=0.5, seed=1, radius_mm=0.2,
+                       height_mm=0.4, nm_iters=400, target_px=0.1):
+    """10-parameter geometry fit from ``n_starts`` perturbed starts (+-0.5 mm distances, +-1 deg
+    tilts, +-20 px detector offsets, +-0.02 mm source/axis offsets), all in one batch."""
+    import time
+
+    import torch
+    geo = geo10_of(geom)
+    grains = random_grains(n_grains, radius_mm, height_mm, seed)
+    d_grains = torch.from_numpy(grains.reshape(-1).copy()).cuda()
+    spots = simulate_spots(ctx, geo, d_grains, noise_px, seed + 1)
+    rng = np.random.default_rng(seed + 3)
+    half = np.array([0.5, 0.5, 20 * geom.pxy, 20 * geom.pxz, 1, 1, 1, 0.02, 0.02, 0.02])
+    starts = geo[None] + rng.uniform(-1, 1, (n_starts, 10)) * half
+    out = {"grains": n_grains, "spots": spots.n, "starts": n_starts, "noise_px": noise_px,
+           "start_spread": dict(zip(GEO_NAMES, half.tolist()))}
+
+    d_s = torch.from_numpy(starts.reshape(-1).copy()).cuda()
+    lam = torch.full((n_starts,), 1e-3, dtype=torch.float64, device="cuda")
+    rms0 = geometry_rms(ctx, d_s, geo, d_grains, spots).cpu().numpy()
+    out["rms_start_median"] = float(np.median(rms0))
+    t_fit, it, first, allr, hist = 0.0, 0, None, None, []
+    while it < 60:
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        improved = geometry_lm(ctx, d_s, d_grains, spots, lam, 1)
+        torch.cuda.synchronize()
+        t_fit += time.perf_counter() - t0
+        it += 1
+        r = geometry_rms(ctx, d_s, geo, d_grains, spots).cpu().numpy()
+        hist.append(float(np.median(r)))
+        n_ok = int((r <= target_px).sum())
+        if first is None and n_ok > 0:
+            first = {"seconds": t_fit, "iterations": it}
+        if allr is None and n_ok == n_starts:
+            allr = {"seconds": t_fit, "iterations": it}
+        if improved == 0:
+            break
+    r = geometry_rms(ctx, d_s, geo, d_grains, spots).cpu().numpy()
+    best = d_s.view(n_starts, 10)[int(np.argmin(r))].cpu().numpy()
+    out["lm"] = {"first_start_below": first, "all_starts_below": allr, "accepted": int((r <= target_px).sum()),
+                 "iterations_run": it, "seconds_run": t_fit, "median_rms_history": hist[:15],
+                 "best_rms": float(r.min()), "best": dict(zip(GEO_NAMES, best.tolist()))}
+
+    lb, ub = geo - 1.5 * half, geo + 1.5 * half
+
+    def f(x):
+        return geometry_cost(ctx, torch.from_numpy(np.ascontiguousarray(x).reshape(-1)).cuda(), d_grains,
+                             spots).cpu().numpy()
+
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    nm = BatchedNelderMead(f, starts, lb, ub)
+    t_nm, nm_first, nm_hist = time.perf_counter() - t0, None, []
+    for k in range(nm_iters):
+        t0 = time.perf_counter()
+        nm.step()
+        t_nm += time.perf_counter() - t0
+        if (k + 1) % 20 == 0:
+            rr = geometry_rms(ctx, torch.from_numpy(nm.best().reshape(-1).copy()).cuda(), geo, d_grains,
+                              spots).cpu().numpy()
+            nm_hist.append(float(np.median(rr)))
+            if nm_first is None and (rr <= target_px).any():
+                nm_first = {"seconds": t_nm, "iterations": k + 1, "evaluations": nm.evals}
+    out["nm"] = {"first_start_below": nm_first, "iterations_run": nm_iters, "evaluations_run": nm.evals,
+                 "seconds_run": t_nm, "median_rms_every_20_iterations": nm_hist}
+    if first and nm_first:
+        out["speedup_lm_vs_nm"] = nm_first["seconds"] / first["seconds"]
+    elif first:
+        out["speedup_lm_vs_nm_lower_bound"] = t_nm / first["seconds"]
+    out["fitted_geo"] = best
+    out["grains_array"] = grains
+    return out

@@ -89,18 +89,9 @@ def voronoi_cylinder(dim: int, n_grains: int, seed: int, lognormal_sigma: float 
     return gid
 
 
-def make_sample(kind: str = "fe_small", seed: int = 1, **over) -> Sample:
-    """Named synthetic samples.
-
-    ``fe6``   : BCC Fe a=2.8665, 6 grains, 100 um cylinder at 5 um (20^3 grid, ~6.3k voxels),
-                6 families (86 reflections), 1024^2 detector at 0.0672 mm, Lss=Lsd=11 mm,
-                tilts U(-0.5,0.5) deg, 181 projections 0:2:360, E 10-70 keV.
-    ``al400`` : FCC Al a=4.0495, 400 grains log-normal (sigma 0.4), 400 um cylinder at 2.5 um
-                (160^3 grid, ~3.2M voxels), 6 families (64 reflections), 2048^2 detector at
-                0.0336 mm, 361 projections 0:1:360.
-    ``fe_small``: the fe6 set-up shrunk for fast CPU tests (12^3 grid, 256^2 detector at
-                0.2688 mm, 37 projections 0:10:360).
-    """
+def named_setup(kind: str, seed: int = 1, **over):
+    """Geometry, lattice and grid of a named sample: (geom, cell, space_group, hkl, dim, n_grains,
+    voxel_mm, lognormal_sigma).  The volume itself is not built."""
     rng = np.random.default_rng(seed + 1000)
     tilt = tuple(rng.uniform(-0.5, 0.5, 3))
     if kind in ("fe6", "fe_small", "fe_tiny"):
@@ -128,6 +119,22 @@ def make_sample(kind: str = "fe_small", seed: int = 1, **over) -> Sample:
     geom = G.Geometry(pxy=px, pxz=px, detysize=det, detzsize=det, tilt=tilt, rot_angles=rot)
     for k, v in over.items():
         setattr(geom, k, v)
+    return geom, cell, sg, G.gen_hkl(sg, 6), dim, ng, vox, sigma
+
+
+def make_sample(kind: str = "fe_small", seed: int = 1, **over) -> Sample:
+    """Named synthetic samples.
+
+    ``fe6``   : BCC Fe a=2.8665, 6 grains, 100 um cylinder at 5 um (20^3 grid, ~6.3k voxels),
+                6 families (86 reflections), 1024^2 detector at 0.0672 mm, Lss=Lsd=11 mm,
+                tilts U(-0.5,0.5) deg, 181 projections 0:2:360, E 10-70 keV.
+    ``al400`` : FCC Al a=4.0495, 400 grains log-normal (sigma 0.4), 400 um cylinder at 2.5 um
+                (160^3 grid, ~3.2M voxels), 6 families (64 reflections), 2048^2 detector at
+                0.0336 mm, 361 projections 0:1:360.
+    ``fe_small``: the fe6 set-up shrunk for fast CPU tests (12^3 grid, 256^2 detector at
+                0.2688 mm, 37 projections 0:10:360).
+    """
+    geom, cell, sg, hkl, dim, ng, vox, sigma = named_setup(kind, seed, **over)
     vol = G.Volume(rec_volume_pixel=(1, 1, 1), simap=1, vox_size=vox, center=(0.0, 0.0, 0.0),
                    dimension=(dim, dim, dim))
     if dim >= 64:
@@ -143,7 +150,6 @@ def make_sample(kind: str = "fe_small", seed: int = 1, **over) -> Sample:
     else:
         gid = voronoi_cylinder(dim, ng, seed, sigma)
     q = G.cubic_fz_orientations(ng, seed + 7)
-    hkl = G.gen_hkl(sg, 6)
     return Sample(geom=geom, vol=vol, cell=cell, space_group=sg, B=G.form_b(cell), hkl=hkl, S=np.eye(3),
                   grain_id=gid, grain_q=q, seed=seed)
 

@@ -146,3 +146,41 @@ def test_batched_nelder_mead_geometry_decreases(env):
     for _ in range(30):
         nm.step()
     assert np.all(nm.F.min(1) <= f0) and np.any(nm.F.min(1) < f0)
+
+
+def test_completeness_with_fitted_geometry_matches_oracle(env):
+    """Fit the 10 geometry parameters, then score completeness with the fitted geometry: the
+    CUDA scorer and the oracle agree bit-exactly on every edge-free trial, and the ground-truth
+    orientation of each voxel's grain stays (almost) complete."""
+    import torch
+    s, ctx, geo, truth, d_truth, spots = env
+    start = geo.copy()
+    start[0:2] += (0.2, -0.15)
+    start[2:4] += (0.3, -0.2)
+    start[4:7] += (0.3, -0.2, 0.25)
+    d_s = torch.from_numpy(start.copy()).cuda()
+    lam = torch.full((1,), 1e-3, dtype=torch.float64, device="cuda")
+    for _ in range(40):
+        if F.geometry_lm(ctx, d_s, d_truth, spots, lam, 1) == 0:
+            break
+    fitted = d_s.cpu().numpy()
+    assert F.geometry_rms(ctx, d_s, geo, d_truth, spots).cpu().numpy()[0] < 0.1
+    dmap = synth.distance_map(synth.simulate_mask(s))
+    gf = F.geometry_with(s.geom, fitted)
+    S9, B9, hkl, rot, _, _ = s.mex_arrays()
+    R9, p = G.flat_rowmajor(gf.rot_det), gf.param20(s.nhkl)
+    q = np.concatenate([s.grain_q, G.cubic_fz_orientations(500, 31)]).astype(np.float32)
+    idx = s.voxel_indices()
+    rng = np.random.default_rng(11)
+    for v in idx[rng.choice(len(idx), 3, replace=False)]:
+        pos = s.vol.pos_of_index(v).astype(np.float32)
+        gpu = ctx.forward_comp(pos, q, S9, B9, hkl, dmap, rot, R9, p).reshape(-1, 4)
+        ref, edges = O.orientation_scan(pos, q, S9, B9, hkl, dmap, rot, R9, p)
+        ref = ref.reshape(-1, 4)
+        clean = edges == 0
+        assert clean.sum() > len(q) // 2
+        np.testing.assert_array_equal(gpu[clean, :3], ref[clean, :3])
+        np.testing.assert_allclose(gpu[clean, 3], ref[clean, 3], rtol=1e-6)
+        d = np.abs(gpu[~clean, :2] - ref[~clean, :2]).max(axis=1)
+        assert np.all(d <= edges[~clean])
+        assert gpu[s.grain_id[tuple(v - 1)] - 1, 2] >= 0.9
