@@ -9,6 +9,7 @@ from __future__ import annotations
 
 import ctypes as C
 import os
+import sys
 
 import numpy as np
 
@@ -29,7 +30,7 @@ EXPORTS = [
     "grc_batch_capture", "grc_batch_replay", "grc_batch_autotune", "grc_batch_info", "grc_batch_destroy",
     "grc_fit_spot_count", "grc_fit_spot_fill", "grc_centroid_residual_adjoint", "grc_fit_grains_lm",
     "grc_fit_grains_nm", "grc_fit_grains_rms", "grc_fit_geometry_lm", "grc_fit_geometry_cost",
-    "grc_fit_geometry_rms",
+    "grc_fit_geometry_rms", "grc_score_trials_device", "grc_fit_orientation_nm",
 ]
 NOALLOC_MAX_ORIENTATIONS = 65536
 
@@ -106,6 +107,8 @@ def load(path: str | None = None):
         "grc_fit_geometry_lm": [vp, f, i, f, f, f, f, f, i64, f, i, C.POINTER(i)],
         "grc_fit_geometry_cost": [vp, f, i, f, f, f, f, f, i64, f],
         "grc_fit_geometry_rms": [vp, f, i, f, f, f, f, f, f, i64, f],
+        "grc_score_trials_device": [vp, f, i64, f, i64, f, f, i64, f],
+        "grc_fit_orientation_nm": [vp, f, f, i64, d, i, i, d, d, f, f, f, f, f],
     }
     for name, args in sig.items():
         fn = getattr(L, name)
@@ -145,6 +148,8 @@ class Context:
 
     def __init__(self, device: int = 0):
         self.L = load()
+        self.device = device
+        self._ext = None
         h = C.c_void_p()
         rc = self.L.grc_ctx_create(C.byref(h), device)
         if rc != GRC_OK:
@@ -176,6 +181,25 @@ class Context:
     def stream(self) -> int:
         return int(self.L.grc_ctx_stream(self.h) or 0)
 
+    def _dev(self, fn, *args):
+        """Call a C entry that reads or writes device buffers, ordered with torch's current stream.
+
+        The library works on its own non-blocking stream; when torch is in use, that stream first
+        waits for the work already queued on torch's current stream (which produced the inputs),
+        and torch's stream then waits for the library's work (which produces the outputs).  No host
+        synchronisation is added."""
+        torch = sys.modules.get("torch")
+        cur = ext = None
+        if torch is not None and torch.cuda.is_initialized():
+            if self._ext is None:
+                self._ext = torch.cuda.ExternalStream(self.stream, device=torch.device("cuda", self.device))
+            ext = self._ext
+            cur = torch.cuda.current_stream(self.device)
+            ext.wait_stream(cur)
+        self._check(fn(self.h, *args))
+        if ext is not None:
+            cur.wait_stream(ext)
+
     def sync(self):
         self._check(self.L.grc_sync(self.h))
 
@@ -185,7 +209,9 @@ class Context:
     def upload_masks(self, proj_bin_bw, detzsize: int, detysize: int, nrot: int):
         if isinstance(proj_bin_bw, np.ndarray):
             proj_bin_bw = np.ascontiguousarray(proj_bin_bw, dtype=np.float32)
-        self._check(self.L.grc_upload_masks(self.h, _ptr(proj_bin_bw), detzsize, detysize, nrot))
+            self._check(self.L.grc_upload_masks(self.h, _ptr(proj_bin_bw), detzsize, detysize, nrot))
+        else:  # a device array (torch tensor): ordered with the stream that produced it
+            self._dev(self.L.grc_upload_masks, _ptr(proj_bin_bw), detzsize, detysize, nrot)
 
     def set_geometry(self, S, B, hkl, rot_angles, RotDet, param):
         keep = [f32(x) for x in (S, B, hkl, rot_angles, RotDet, param)]
@@ -233,32 +259,48 @@ class Context:
 
     # device-resident entries (torch CUDA tensors / device pointers)
     def forward_comp_device(self, d_pos, n_vox: int, d_q, n_q: int, d_out):
-        self._check(self.L.grc_forward_comp_device(self.h, _ptr(d_pos), n_vox, _ptr(d_q), n_q, _ptr(d_out)))
+        self._dev(self.L.grc_forward_comp_device, _ptr(d_pos), n_vox, _ptr(d_q), n_q, _ptr(d_out))
 
     def grow_device(self, d_rows6, m: int, U, param1, d_out):
         u, p1 = f32(U), f32(param1)
-        self._check(self.L.grc_grow_device(self.h, _ptr(d_rows6), m, _ptr(u), _ptr(p1), _ptr(d_out)))
+        self._dev(self.L.grc_grow_device, _ptr(d_rows6), m, _ptr(u), _ptr(p1), _ptr(d_out))
 
     def compete_device(self, d_rows5, m: int, d_id, n_neigb: int, d_euler, n_grain: int, param1, d_out,
                        d_trial_out=None):
         p1 = f32(param1)
-        self._check(self.L.grc_compete_device(self.h, _ptr(d_rows5), m, _ptr(d_id), n_neigb, _ptr(d_euler),
-                                              n_grain, _ptr(p1), _ptr(d_out), _ptr(d_trial_out)))
+        self._dev(self.L.grc_compete_device, _ptr(d_rows5), m, _ptr(d_id), n_neigb, _ptr(d_euler),
+                                              n_grain, _ptr(p1), _ptr(d_out), _ptr(d_trial_out))
+
+    def score_trials_device(self, d_pos, n_vox: int, d_q, n_q: int, d_trial_voxel, d_trial_orient, n_trials: int,
+                            d_out):
+        """FP64 trial list: trial t = (voxel d_trial_voxel[t], orientation d_trial_orient[t]); both None
+        means trial t = (voxel t, orientation t).  d_pos: 3 doubles per voxel, d_q: 4 doubles per
+        orientation, d_out: 4 floats per trial (device buffers)."""
+        self._dev(self.L.grc_score_trials_device, _ptr(d_pos), n_vox, _ptr(d_q), n_q, _ptr(d_trial_voxel),
+                                                   _ptr(d_trial_orient), n_trials, _ptr(d_out))
+
+    def fit_orientation_nm(self, d_pos, d_x0, n: int, d_x, d_fval, d_evals=None, d_iters=None, d_flag=None,
+                           half_width: float = 0.02, max_evals: int = 2000, max_iter: int = 2000,
+                           tol_f: float = 1e-10, tol_x: float = 1e-4):
+        """Batched fminsearchbnd on 1 - completeness over (q1, q2, q3), one simplex per seed."""
+        self._dev(self.L.grc_fit_orientation_nm, _ptr(d_pos), _ptr(d_x0), n, half_width, max_evals, max_iter,
+                                                  tol_f, tol_x, _ptr(d_x), _ptr(d_fval), _ptr(d_evals), _ptr(d_iters),
+                                                  _ptr(d_flag))
 
     def forward_comp_noalloc(self, pos, d_q, n_q: int, d_out):
         """Allocation-free seeding scan: host pos (3 floats), device d_q / d_out; see the C header."""
         p = f32(pos)
-        self._check(self.L.grc_forward_comp_noalloc(self.h, _ptr(p), _ptr(d_q), n_q, _ptr(d_out)))
+        self._dev(self.L.grc_forward_comp_noalloc, _ptr(p), _ptr(d_q), n_q, _ptr(d_out))
 
     def batch(self, d_rows5, m: int, d_id, n_neigb: int, d_euler, n_grain: int, param1):
         """Plan a batched-grow work list on device buffers (see Batch)."""
         return Batch(self, d_rows5, m, d_id, n_neigb, d_euler, n_grain, param1)
 
     def simulate_spots(self, d_pos, d_U, n: int, d_mask):
-        self._check(self.L.grc_simulate_spots(self.h, _ptr(d_pos), _ptr(d_U), n, _ptr(d_mask)))
+        self._dev(self.L.grc_simulate_spots, _ptr(d_pos), _ptr(d_U), n, _ptr(d_mask))
 
     def edt(self, d_mask, detzsize: int, detysize: int, nrot: int, d_map):
-        self._check(self.L.grc_edt(self.h, _ptr(d_mask), detzsize, detysize, nrot, _ptr(d_map)))
+        self._dev(self.L.grc_edt, _ptr(d_mask), detzsize, detysize, nrot, _ptr(d_map))
 
     def set_timing(self, enable: bool):
         self._check(self.L.grc_set_timing(self.h, int(bool(enable))))
@@ -290,8 +332,8 @@ class Batch:
         self._keep = (d_rows5, d_id, d_euler)  # borrowed device arrays must outlive the batch
         p1 = f32(param1)
         h = C.c_void_p()
-        ctx._check(self.L.grc_batch_create(ctx.h, _ptr(d_rows5), m, _ptr(d_id), n_neigb, _ptr(d_euler), n_grain,
-                                           _ptr(p1), C.byref(h)))
+        ctx._dev(lambda _h, *a: self.L.grc_batch_create(ctx.h, *a), _ptr(d_rows5), m, _ptr(d_id), n_neigb,
+                 _ptr(d_euler), n_grain, _ptr(p1), C.byref(h))
         self.h = h
 
     def info(self) -> dict:
@@ -303,22 +345,22 @@ class Batch:
     def set_maps(self, dims, completeness=None, grain_id=None, dismedian=None, ninter=None, visitflag=None):
         d = (C.c_int64 * 3)(*[int(x) for x in dims])
         self._maps = (completeness, grain_id, dismedian, ninter, visitflag)
-        self.ctx._check(self.L.grc_batch_set_maps(self.h, d, *[_ptr(x) for x in self._maps]))
+        self.ctx._dev(lambda _h, *a: self.L.grc_batch_set_maps(self.h, *a), d, *[_ptr(x) for x in self._maps])
 
     def run(self, d_out8, d_trial_out=None):
-        self.ctx._check(self.L.grc_batch_run(self.h, _ptr(d_out8), _ptr(d_trial_out)))
+        self.ctx._dev(lambda _h, *a: self.L.grc_batch_run(self.h, *a), _ptr(d_out8), _ptr(d_trial_out))
 
     def capture(self, d_out8):
         self._graph_out = d_out8
-        self.ctx._check(self.L.grc_batch_capture(self.h, _ptr(d_out8)))
+        self.ctx._dev(lambda _h, *a: self.L.grc_batch_capture(self.h, *a), _ptr(d_out8))
 
     def replay(self):
-        self.ctx._check(self.L.grc_batch_replay(self.h))
+        self.ctx._dev(lambda _h: self.L.grc_batch_replay(self.h))
 
     def autotune(self, d_out8, max_voxels: int = 0) -> dict:
         p, s, ms = C.c_int(), C.c_int(), C.c_double()
-        self.ctx._check(self.L.grc_batch_autotune(self.h, _ptr(d_out8), max_voxels, C.byref(p), C.byref(s),
-                                                  C.byref(ms)))
+        self.ctx._dev(lambda _h, *a: self.L.grc_batch_autotune(self.h, *a), _ptr(d_out8), max_voxels, C.byref(p), C.byref(s),
+                                                  C.byref(ms))
         return {"path": p.value, "slots": s.value, "ms": ms.value}
 
     def close(self):

@@ -42,8 +42,9 @@ struct grc_ctx {
     grc::MapCodes mc{};
     int64_t mz = 0, my = 0, mrot = 0;
     std::vector<float> h_vals;
-    DevBuf fgeo, fne, ftrial, fcost0, fcost1, fimp, fhw, geo_dev, rot_cs, hkl, pos, U, res, tvoxel, rlist, in1, in2, in3, out, items, torient, counts, offsets, tmp, counter, p1, bad;
+    DevBuf fgeo, fne, ftrial, fcost0, fcost1, fimp, fhw, geo_dev, rot_cs, hkl, pos, U, res, tvoxel, rlist, in1, in2, in3, out, items, torient, counts, offsets, tmp, counter, p1, bad, nm;
     grc::Geo *geo_pinned = nullptr;  // staging of the per-launch geometry copy
+    int *nm_active = nullptr;        // pinned: seeds still running in the orientation fit
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     bool timing = false;
     bool timed_last = false;
@@ -490,7 +491,8 @@ int grc_ctx_destroy(grc_ctx *ctx) {
         Lock l(ctx);
         cudaStreamSynchronize(ctx->stream);
         cudaFreeHost(ctx->geo_pinned);
-        DevBuf *all[] = {&ctx->fgeo, &ctx->fne, &ctx->ftrial, &ctx->fcost0, &ctx->fcost1, &ctx->fimp, &ctx->fhw,
+        if (ctx->nm_active) cudaFreeHost(ctx->nm_active);
+        DevBuf *all[] = {&ctx->nm, &ctx->fgeo, &ctx->fne, &ctx->ftrial, &ctx->fcost0, &ctx->fcost1, &ctx->fimp, &ctx->fhw,
                          &ctx->tvoxel, &ctx->rlist, &ctx->geo_dev, &ctx->rot_cs, &ctx->hkl, &ctx->pos, &ctx->U, &ctx->res, &ctx->in1, &ctx->in2,
                          &ctx->in3, &ctx->out, &ctx->items, &ctx->torient, &ctx->counts, &ctx->offsets,
                          &ctx->tmp, &ctx->counter, &ctx->p1, &ctx->bad};
@@ -659,6 +661,136 @@ int grc_compete_device(grc_ctx *ctx, const float *d_rows5, int64_t m, const floa
     if (m < 0 || n_neigb < 0 || n_grain < 0) return fail(ctx, GRC_EINVAL, "negative size");
     if (m > 0 && (!d_rows5 || !d_out || !d_euler)) return fail(ctx, GRC_EINVAL, "NULL device buffer");
     return compete_device(ctx, d_rows5, m, d_id, n_neigb, d_euler, n_grain, param1, d_out, d_trial_out);
+}
+
+int grc_score_trials_device(grc_ctx *ctx, const double *d_pos, int64_t n_vox, const double *d_q, int64_t n_q,
+                            const int32_t *d_tv, const int32_t *d_to, int64_t n_trials, float *d_out) {
+    if (!ctx) return GRC_EINVAL;
+    Lock l(ctx);
+    TRY(check_ready(ctx));
+    ctx->stats = grc_stats{};
+    if (n_trials < 0 || n_vox < 0 || n_q < 0) return fail(ctx, GRC_EINVAL, "negative size");
+    if (n_trials == 0) return GRC_OK;
+    if (!d_pos || !d_q || !d_out || n_vox < 1 || n_q < 1) return fail(ctx, GRC_EINVAL, "trials: NULL buffer or no rows");
+    if ((d_tv == nullptr) != (d_to == nullptr))
+        return fail(ctx, GRC_EINVAL, "trials: give both index arrays or neither");
+    if (!d_tv && (n_vox != n_trials || n_q != n_trials))
+        return fail(ctx, GRC_EINVAL, "trials: without index arrays n_vox and n_q must equal n_trials");
+    if (n_vox > (int64_t)INT32_MAX || n_q > (int64_t)INT32_MAX)
+        return fail(ctx, GRC_ECAPACITY, "trials: more than 2^31-1 voxels or orientations");
+    TRY(ensure(ctx, ctx->U, sizeof(double) * 9 * n_q));
+    TRY(ensure(ctx, ctx->pos, sizeof(double) * 3 * n_vox));
+    TRY(ensure(ctx, ctx->res, sizeof(grc::TrialRes) * n_trials));
+    CU(grc::launch_quat_to_u_d(d_q, n_q, (double *)ctx->U.p, ctx->stream));
+    CU(cudaMemcpyAsync(ctx->pos.p, d_pos, sizeof(double) * 3 * n_vox, cudaMemcpyDeviceToDevice, ctx->stream));
+    grc::Work w{};
+    if (d_tv) {
+        TRY(ensure(ctx, ctx->items, sizeof(longlong4) * n_trials));
+        TRY(ensure(ctx, ctx->bad, sizeof(int)));
+        CU(cudaMemsetAsync(ctx->bad.p, 0, sizeof(int), ctx->stream));
+        CU(grc::launch_trial_items(d_tv, d_to, n_trials, n_vox, n_q, (longlong4 *)ctx->items.p, (int *)ctx->bad.p,
+                                   ctx->stream));
+        int hbad = 0;
+        CU(cudaMemcpyAsync(&hbad, ctx->bad.p, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+        CU(cudaStreamSynchronize(ctx->stream));
+        if (hbad) return fail(ctx, GRC_EINVAL, "trials: a voxel or orientation index lies out of range");
+        w.items = (const longlong4 *)ctx->items.p;
+        w.trial_orient = d_to;
+        w.trial_voxel = d_tv;
+        w.n_items = n_trials;
+    } else {
+        w.diag = 1;
+        w.n_or = 1;
+        w.chunk = 1;
+        w.chunks_per_voxel = 1;
+        w.n_items = n_trials;
+    }
+    TRY(run_score(ctx, w, n_trials));
+    CU(grc::launch_epi_forward((const grc::TrialRes *)ctx->res.p, n_trials, d_out, ctx->stream));
+    ctx->stats.kernel_launches += 3 + (d_tv ? 1 : 0);
+    return GRC_OK;
+}
+
+int grc_fit_orientation_nm(grc_ctx *ctx, const double *d_pos, const double *d_x0, int64_t n, double half_width,
+                           int max_evals, int max_iter, double tol_f, double tol_x, double *d_x, double *d_fval,
+                           int32_t *d_evals, int32_t *d_iters, int32_t *d_flag) {
+    if (!ctx) return GRC_EINVAL;
+    Lock l(ctx);
+    TRY(check_ready(ctx));
+    ctx->stats = grc_stats{};
+    if (n < 0) return fail(ctx, GRC_EINVAL, "negative size");
+    if (n == 0) return GRC_OK;
+    if (!d_pos || !d_x0 || !d_x || !d_fval) return fail(ctx, GRC_EINVAL, "orientation fit: NULL buffer");
+    if (!(half_width > 0) || max_evals < 1 || max_iter < 1 || !(tol_f >= 0) || !(tol_x >= 0))
+        return fail(ctx, GRC_EINVAL, "orientation fit: bad options");
+    if (n > (int64_t)INT32_MAX / 4) return fail(ctx, GRC_ECAPACITY, "orientation fit: too many seeds");
+    const int64_t T = 4 * n;
+    TRY(ensure(ctx, ctx->nm, sizeof(grc::NmSeed) * n));
+    TRY(ensure(ctx, ctx->U, sizeof(double) * 9 * T));
+    TRY(ensure(ctx, ctx->pos, sizeof(double) * 3 * n));
+    TRY(ensure(ctx, ctx->res, sizeof(grc::TrialRes) * T));
+    TRY(ensure(ctx, ctx->items, sizeof(longlong4) * T));
+    TRY(ensure(ctx, ctx->counter, 8 * sizeof(int)));
+    TRY(ensure(ctx, ctx->bad, sizeof(int)));
+    if (!ctx->nm_active) CU(cudaMallocHost(&ctx->nm_active, sizeof(int)));
+    CU(cudaMemcpyAsync(ctx->pos.p, d_pos, sizeof(double) * 3 * n, cudaMemcpyDeviceToDevice, ctx->stream));
+    CU(grc::launch_nm_init((grc::NmSeed *)ctx->nm.p, n, d_x0, half_width, ctx->stream));
+    TRY(stage_geo(ctx));
+    grc::ScoreBufs b = bufs(ctx);
+    grc::Work w{};
+    w.items = (const longlong4 *)ctx->items.p;
+    w.n_items = T;
+    w.n_or = 1;
+    w.diag = 1;  // trial t uses orientation t; the voxel comes from items[t]
+    int *active = (int *)ctx->bad.p;
+    // One graph = kSteps (propose, score, accept) steps plus the running-seed count of the last.
+    constexpr int kSteps = 8;
+    const int64_t max_steps = 2 * (int64_t)std::min(max_evals, 2 * max_iter) + 8;
+    int launches = 0;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    auto enqueue = [&]() -> int {
+        for (int k = 0; k < kSteps; ++k) {
+            CU(cudaMemsetAsync(active, 0, sizeof(int), ctx->stream));
+            CU(grc::launch_nm_propose((grc::NmSeed *)ctx->nm.p, n, max_evals, max_iter, tol_f, tol_x,
+                                      (double *)ctx->U.p, (longlong4 *)ctx->items.p, active, ctx->stream));
+            cudaError_t e = grc::launch_score(ctx->geo, b, w, ctx->num_sms, ctx->stream, nullptr, nullptr, &launches);
+            if (e != cudaSuccess) return fail(ctx, GRC_ECUDA, "orientation fit scorer: %s", cudaGetErrorString(e));
+            CU(grc::launch_nm_accept((grc::NmSeed *)ctx->nm.p, n, (const grc::TrialRes *)ctx->res.p, ctx->stream));
+        }
+        CU(cudaMemcpyAsync(ctx->nm_active, active, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+        return GRC_OK;
+    };
+    int rc = GRC_OK;
+    cudaError_t e = cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+        rc = enqueue();
+        e = cudaStreamEndCapture(ctx->stream, &graph);
+        if (rc == GRC_OK && e == cudaSuccess) e = cudaGraphInstantiate(&exec, graph, 0);
+    }
+    if (rc != GRC_OK || e != cudaSuccess) {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        cudaGetLastError();
+        return rc != GRC_OK ? rc : fail(ctx, GRC_ECUDA, "orientation fit graph: %s", cudaGetErrorString(e));
+    }
+    int64_t steps = 0;
+    int graphs = 0;
+    for (; steps < max_steps; steps += kSteps) {
+        e = cudaGraphLaunch(exec, ctx->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+        ++graphs;
+        if (e != cudaSuccess || *ctx->nm_active == 0) break;
+    }
+    cudaGraphExecDestroy(exec);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) return fail(ctx, GRC_ECUDA, "orientation fit: %s", cudaGetErrorString(e));
+    CU(grc::launch_nm_final((const grc::NmSeed *)ctx->nm.p, n, d_x, d_fval, d_evals, d_iters, d_flag, ctx->stream));
+    CU(cudaStreamSynchronize(ctx->stream));
+    ctx->stats.trials = steps * T;
+    ctx->stats.kernel_launches = (int64_t)graphs * kSteps * (2 + launches / kSteps) + 2;
+    ctx->stats.path = 1;
+    return GRC_OK;
 }
 
 int grc_last_stats(grc_ctx *ctx, grc_stats *out) {

@@ -126,4 +126,28 @@ cudaError_t launch_simulate_work(const Geo &g, const ScoreBufs &b, const Work &w
                                  cudaStream_t s);
 cudaError_t launch_edt(const uint8_t *mask, int64_t nz, int64_t ny, int64_t nrot, float *map, cudaStream_t s);
 
+// FP64 trial lists (grc_seed.cu): U from double quaternions, work items from (voxel, orientation)
+// index pairs (bad |= 1 for an index out of range; that item is left empty).
+cudaError_t launch_quat_to_u_d(const double *q, int64_t n, double *U, cudaStream_t s);
+cudaError_t launch_trial_items(const int32_t *tv, const int32_t *to, int64_t n, int64_t n_vox, int64_t n_q,
+                               longlong4 *items, int *bad, cudaStream_t s);
+
+// Batched bounded Nelder-Mead on 1 - completeness over (q1, q2, q3): one simplex per seed in the
+// transformed variables of fminsearchbnd (z), vertices sorted by objective.
+struct NmSeed {
+    double z[4][3];
+    double fv[4];
+    double cand[4][3];   // points proposed by the current step
+    double lb[3], ub[3];
+    int evals, iters, phase, flag;
+    int nanmask;         // slots of the current step whose point has no real q0
+};
+cudaError_t launch_nm_init(NmSeed *st, int64_t n, const double *x0, double half_width, cudaStream_t s);
+// Writes U for trials 4i..4i+3 (empty work items for unused slots) and counts running seeds.
+cudaError_t launch_nm_propose(NmSeed *st, int64_t n, int max_evals, int max_iter, double tol_f, double tol_x,
+                              double *U, longlong4 *items, int *active, cudaStream_t s);
+cudaError_t launch_nm_accept(NmSeed *st, int64_t n, const TrialRes *res, cudaStream_t s);
+cudaError_t launch_nm_final(const NmSeed *st, int64_t n, double *x, double *fval, int32_t *evals, int32_t *iters,
+                            int32_t *flag, cudaStream_t s);
+
 }  // namespace grc

@@ -93,7 +93,7 @@ def simulate_spots(ctx, geo10, d_grains, noise_px: float, seed: int) -> Spots:
     n = d_grains.numel() // 6
     geo = np.ascontiguousarray(geo10, dtype=np.float64)
     counts = torch.zeros(n, dtype=torch.int64, device="cuda")
-    ctx._check(ctx.L.grc_fit_spot_count(ctx.h, _ptr(geo), _ptr(d_grains), n, _ptr(counts)))
+    ctx._dev(ctx.L.grc_fit_spot_count, _ptr(geo), _ptr(d_grains), n, _ptr(counts))
     offsets = torch.zeros(n + 1, dtype=torch.int64, device="cuda")
     offsets[1:] = torch.cumsum(counts, 0)
     ns = int(offsets[-1].item())
@@ -101,8 +101,8 @@ def simulate_spots(ctx, geo10, d_grains, noise_px: float, seed: int) -> Spots:
     iw = torch.empty(ns, dtype=torch.int32, device="cuda")
     ih = torch.empty(ns, dtype=torch.int32, device="cuda")
     uv = torch.empty(2 * ns, dtype=torch.float64, device="cuda")
-    ctx._check(ctx.L.grc_fit_spot_fill(ctx.h, _ptr(geo), _ptr(d_grains), n, _ptr(offsets), _ptr(grain), _ptr(iw),
-                                       _ptr(ih), _ptr(uv)))
+    ctx._dev(ctx.L.grc_fit_spot_fill, _ptr(geo), _ptr(d_grains), n, _ptr(offsets), _ptr(grain), _ptr(iw),
+                                       _ptr(ih), _ptr(uv))
     exact = uv.clone()
     if noise_px > 0:
         gen = torch.Generator(device="cuda").manual_seed(seed)
@@ -118,8 +118,8 @@ def residual_jacobian(ctx, mode: int, geo10, d_grains, spots: Spots):
     res = torch.empty(2 * spots.n, dtype=torch.float64, device="cuda")
     jac = torch.empty(2 * K * spots.n, dtype=torch.float64, device="cuda")
     geo = np.ascontiguousarray(geo10, dtype=np.float64)
-    ctx._check(ctx.L.grc_centroid_residual_adjoint(ctx.h, mode, _ptr(geo), _ptr(d_grains),
-                                                   *[_ptr(a) for a in spots.args()], spots.n, _ptr(res), _ptr(jac)))
+    ctx._dev(ctx.L.grc_centroid_residual_adjoint, mode, _ptr(geo), _ptr(d_grains),
+                                                   *[_ptr(a) for a in spots.args()], spots.n, _ptr(res), _ptr(jac))
     return res.view(-1, 2), jac.view(-1, 2, K)
 
 
@@ -129,9 +129,9 @@ def grains_lm(ctx, geo10, d_grains, spots: Spots, d_lambda, iters: int) -> int:
     from ._lib import _ptr
     geo = np.ascontiguousarray(geo10, dtype=np.float64)
     imp = C.c_int()
-    ctx._check(ctx.L.grc_fit_grains_lm(ctx.h, _ptr(geo), _ptr(d_grains), d_grains.numel() // 6,
+    ctx._dev(ctx.L.grc_fit_grains_lm, _ptr(geo), _ptr(d_grains), d_grains.numel() // 6,
                                        *[_ptr(a) for a in spots.args()], spots.n, _ptr(spots.offsets),
-                                       _ptr(d_lambda), iters, C.byref(imp)))
+                                       _ptr(d_lambda), iters, C.byref(imp))
     return imp.value
 
 
@@ -141,9 +141,9 @@ def grains_nm(ctx, geo10, d_grains, spots: Spots, half_width, max_evals: int, ch
     geo = np.ascontiguousarray(geo10, dtype=np.float64)
     hw = np.ascontiguousarray(half_width, dtype=np.float64)
     n_ck = 0 if d_trace is None else d_trace.numel() // (6 * (d_grains.numel() // 6))
-    ctx._check(ctx.L.grc_fit_grains_nm(ctx.h, _ptr(geo), _ptr(d_grains), d_grains.numel() // 6,
+    ctx._dev(ctx.L.grc_fit_grains_nm, _ptr(geo), _ptr(d_grains), d_grains.numel() // 6,
                                        *[_ptr(a) for a in spots.args()], spots.n, _ptr(spots.offsets), _ptr(hw),
-                                       max_evals, checkpoint, _ptr(d_trace), n_ck))
+                                       max_evals, checkpoint, _ptr(d_trace), n_ck)
 
 
 def grains_rms(ctx, geo10, d_grains, d_truth, spots: Spots):
@@ -153,8 +153,8 @@ def grains_rms(ctx, geo10, d_grains, d_truth, spots: Spots):
     n = d_grains.numel() // 6
     rms = torch.empty(n, dtype=torch.float64, device="cuda")
     geo = np.ascontiguousarray(geo10, dtype=np.float64)
-    ctx._check(ctx.L.grc_fit_grains_rms(ctx.h, _ptr(geo), _ptr(d_grains), _ptr(d_truth), n,
-                                        *[_ptr(a) for a in spots.args()], spots.n, _ptr(spots.offsets), _ptr(rms)))
+    ctx._dev(ctx.L.grc_fit_grains_rms, _ptr(geo), _ptr(d_grains), _ptr(d_truth), n,
+                                        *[_ptr(a) for a in spots.args()], spots.n, _ptr(spots.offsets), _ptr(rms))
     return rms
 
 
@@ -162,9 +162,9 @@ def geometry_lm(ctx, d_starts, d_grains, spots: Spots, d_lambda, iters: int) -> 
     import ctypes as C
     from ._lib import _ptr
     imp = C.c_int()
-    ctx._check(ctx.L.grc_fit_geometry_lm(ctx.h, _ptr(d_starts), d_starts.numel() // 10, _ptr(d_grains),
+    ctx._dev(ctx.L.grc_fit_geometry_lm, _ptr(d_starts), d_starts.numel() // 10, _ptr(d_grains),
                                          *[_ptr(a) for a in spots.args()], spots.n, _ptr(d_lambda), iters,
-                                         C.byref(imp)))
+                                         C.byref(imp))
     return imp.value
 
 
@@ -174,8 +174,8 @@ def geometry_cost(ctx, d_points, d_grains, spots: Spots):
     from ._lib import _ptr
     n = d_points.numel() // 10
     cost = torch.empty(2 * n, dtype=torch.float64, device="cuda")
-    ctx._check(ctx.L.grc_fit_geometry_cost(ctx.h, _ptr(d_points), n, _ptr(d_grains),
-                                           *[_ptr(a) for a in spots.args()], spots.n, _ptr(cost)))
+    ctx._dev(ctx.L.grc_fit_geometry_cost, _ptr(d_points), n, _ptr(d_grains),
+                                           *[_ptr(a) for a in spots.args()], spots.n, _ptr(cost))
     return cost.view(-1, 2)[:, 0]
 
 
@@ -185,8 +185,8 @@ def geometry_rms(ctx, d_starts, geo_truth10, d_grains, spots: Spots):
     n = d_starts.numel() // 10
     acc = torch.empty(2 * n, dtype=torch.float64, device="cuda")
     geo = np.ascontiguousarray(geo_truth10, dtype=np.float64)
-    ctx._check(ctx.L.grc_fit_geometry_rms(ctx.h, _ptr(d_starts), n, _ptr(geo), _ptr(d_grains),
-                                          *[_ptr(a) for a in spots.args()], spots.n, _ptr(acc)))
+    ctx._dev(ctx.L.grc_fit_geometry_rms, _ptr(d_starts), n, _ptr(geo), _ptr(d_grains),
+                                          *[_ptr(a) for a in spots.args()], spots.n, _ptr(acc))
     acc = acc.view(-1, 2)
     return torch.sqrt(acc[:, 0] / acc[:, 1])
 

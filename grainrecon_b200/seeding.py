@@ -1,0 +1,488 @@
+"""Seeding stage of the grain-mapping engine, batched on the GPU.
+
+Mirrors GrainMapping_engine_gpu_comp.m:54-331 and its orientation fit
+fit_OR_constrain_with_local_comp_cuda.m:1-185.  Per seed the reference runs, one seed
+after the other:
+
+1. the orientation scan ``cuda_forward_comp`` over the whole grid (:74-78);
+2. ``sortrows(Output, 3, 'descend')`` and the top ``Nr_seed`` rows (:102-112);
+3. a local refine: every candidate's ``ori_local_sampling(q, 8, 0.004)`` grid (730
+   orientations) scored in one ``cuda_forward_comp`` call; the best of each grid, sorted
+   by completeness (fit_OR_constrain_with_local_comp_cuda.m:12-49,100-112);
+4. ``fminsearchbnd`` on 1 - completeness from the best one, ±0.02 on q1..q3, up to 2000
+   evaluations of the CPU scorer (:115-126);
+5. the Euler-angle round trip and a final scoring of the fitted orientation (:128-153);
+6. the accept rule ``C >= minComp and C >= Completeness(seed) and median <= maxDmedian``
+   (GrainMapping_engine_gpu_comp.m:180-181), then region growth.
+
+Steps 1-5 depend only on the seed position and the static distance map, so here they run
+for a whole batch of seeds at once: one scan launch, one local-refine launch over
+``n_seeds x Nr_seed x 730`` trials, one batched Nelder-Mead (every simplex on the device,
+one scorer launch per step for all seeds), one final launch.  Step 6 changes the sample
+maps and stays sequential: ``GrainMapping_engine_gpu_comp`` commits the batch's results
+in seed order, discarding a result whose seed an earlier growth made redundant, and
+re-indexes a moved centre (the replace_center loop, :256-300) on the spot.
+
+Every scorer evaluation goes through libgrainrecon_b200.so; torch only holds device
+buffers and does the small sorts between launches.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+from . import geometry as G
+
+NR_LOCAL = 8          # fit_OR_constrain_with_local_comp_cuda.m:20
+GRID_LOCAL = 0.004
+NR_RECENTRE = 4       # GrainMapping_engine_gpu_comp.m:87 (126 orientations)
+FIT_HALF_WIDTH = 0.02  # fit_OR_constrain_with_local_comp_cuda.m:124-125
+FIT_MAX_EVALS = 2000   # :120-121 (MaxFunEvals = MaxIter = 2000, TolFun 1e-10; TolX default 1e-4)
+FIT_TOL_F = 1e-10
+FIT_TOL_X = 1e-4
+TRIALS_PER_LAUNCH = 1 << 24
+
+
+# ---- orientation conversions of the Euler round trip (:128-145) -------------------------------
+# Restated from the Aerospace-toolbox semantics of quat2rod / rod2angle / angle2rod / rod2quat.
+
+def quat2rod(q) -> np.ndarray:
+    """Rodrigues vector of a quaternion [q0 q1 q2 q3] (normalised first; zero when q0 = 1)."""
+    q = np.asarray(q, dtype=np.float64)
+    qn = q / math.sqrt(float((q * q).sum()))
+    thalf = math.acos(qn[0])
+    if thalf == 0:
+        return np.zeros(3)
+    return qn[1:] / math.cos(thalf)
+
+
+def rod2angle_zxz(R):
+    """ZXZ rotation angles (radians) of a Rodrigues vector."""
+    R = np.asarray(R, dtype=np.float64)
+    n = math.sqrt(float((R * R).sum()))
+    if n == 0:
+        return 0.0, 0.0, 0.0
+    th = 2 * math.atan(n)
+    sx, sy, sz = R / n
+    cth, sth = math.cos(th), math.sin(th)
+    r11 = sx * sz * (1 - cth) + sy * sth
+    r12 = sx * sth - sy * sz * (1 - cth)
+    r21 = sz ** 2 + (1 - sz ** 2) * cth
+    r31 = sx * sz * (1 - cth) - sy * sth
+    r32 = sy * sz * (1 - cth) + sx * sth
+    r21 = min(1.0, max(-1.0, r21))
+    return math.atan2(r11, r12), math.acos(r21), math.atan2(r31, r32)
+
+
+def angle2rod_zxz(r1, r2, r3) -> np.ndarray:
+    """Rodrigues vector of ZXZ rotation angles (radians)."""
+    cps, sps = math.cos(r1), math.sin(r1)
+    cth, sth = math.cos(r2), math.sin(r2)
+    cph, sph = math.cos(r3), math.sin(r3)
+    tr = cph * cps - sph * cth * sps - sph * sps + cph * cth * cps + cth
+    r31 = sth * sps - sph * sth
+    r23 = cph * sth + sth * cps
+    r12 = cph * sps + sph * cth * cps + sph * cps + cph * cth * sps
+    th = math.acos(min(1.0, max(-1.0, (tr - 1) / 2)))
+    if th == 0:
+        return np.zeros(3)
+    s2 = 2 * math.sin(th)
+    return math.tan(th / 2) * np.array([r23 / s2, r31 / s2, r12 / s2])
+
+
+def rod2quat(R) -> np.ndarray:
+    """Quaternion of a Rodrigues vector (all zeros for a zero vector, as the reference returns)."""
+    R = np.asarray(R, dtype=np.float64)
+    n = math.sqrt(float((R * R).sum()))
+    if n == 0:
+        return np.zeros(4)
+    thalf = math.atan(n)
+    return np.concatenate([[math.cos(thalf)], R * math.sin(thalf) / n])
+
+
+def fitted_orientation(x):
+    """(euler_deg[3], rod[3], quat[4]) of fitted (q1, q2, q3), via the reference's Euler round trip."""
+    x = [float(v) for v in x]
+    q = np.array([math.sqrt(1 - x[0] ** 2 - x[1] ** 2 - x[2] ** 2), x[0], x[1], x[2]])
+    ang = [a * 180 / math.pi for a in rod2angle_zxz(quat2rod(q))]
+    ang = [a + 360 if a < 0 else a for a in ang]
+    rod = angle2rod_zxz(*(a * math.pi / 180 for a in ang))
+    return np.array(ang), rod, rod2quat(rod)
+
+
+# ---- device helpers -------------------------------------------------------------------------------
+
+def sort_desc_nan_first(C, dim: int = -1):
+    """Indices of ``sortrows(.., 'descend')`` on one column: stable, NaN rows first."""
+    import torch
+    return torch.sort(C, dim=dim, descending=True, stable=True).indices
+
+
+def local_grids(qc, nr: int = NR_LOCAL, gridsize: float = GRID_LOCAL):
+    """``ori_local_sampling(q, nr, gridsize)`` for every row of qc (n x 4, float64, device).
+
+    Returns (n, (nr+1)^3 + 1, 4): the centre row and the (b, c, d) grid with
+    q0 = sqrt(1 - (b^2 + c^2 + d^2)), in ``unique(q, 'rows')`` order (ascending by q0, then
+    b, c, d).  A grid point equal to the centre stays in as an adjacent twin; it scores the
+    same, so a first-maximum search picks the same orientation as on the de-duplicated list."""
+    import torch
+    n = qc.shape[0]
+    steps = torch.arange(nr + 1, dtype=torch.float64, device=qc.device) * gridsize - gridsize * nr / 2
+    b = qc[:, 1, None] + steps[None, :]
+    c = qc[:, 2, None] + steps[None, :]
+    d = qc[:, 3, None] + steps[None, :]
+    m = nr + 1
+    B = b[:, :, None, None].expand(n, m, m, m).reshape(n, -1)
+    Cc = c[:, None, :, None].expand(n, m, m, m).reshape(n, -1)
+    D = d[:, None, None, :].expand(n, m, m, m).reshape(n, -1)
+    q0 = torch.sqrt(1 - (B * B + Cc * Cc + D * D))
+    grid = torch.stack([q0, B, Cc, D], dim=-1)
+    rows = torch.cat([qc[:, None, :], grid], dim=1)
+    # lexicographic order by stable sorts from the last key to the first
+    for k in (3, 2, 1, 0):
+        o = torch.sort(rows[:, :, k], dim=1, stable=True).indices
+        rows = torch.gather(rows, 1, o[:, :, None].expand_as(rows))
+    return rows
+
+
+def _f32(t):
+    return t.float().double()
+
+
+class SeedIndexer:
+    """Steps 1-5 of the seeding stage for batches of seeds on one context.
+
+    ``q_grid``: the orientation set (N x 4, [q0 q1 q2 q3]) scored at every seed."""
+
+    def __init__(self, ctx, q_grid, nr_seed: int, fit: bool = True):
+        import torch
+        self.ctx = ctx
+        self.dev = torch.device("cuda", torch.cuda.current_device())
+        self.q = torch.as_tensor(np.ascontiguousarray(q_grid, np.float64), device=self.dev)
+        self.q32 = self.q.float().contiguous()
+        self.nr_seed = int(nr_seed)
+        self.fit = fit
+        self.stats = {"scan_trials": 0, "local_trials": 0, "fit_seeds": 0, "fit_evals": 0, "final_trials": 0}
+
+    # 1. scan of the whole grid (ForwardCalc_OR_space_comp_cuda: float32 pos and q)
+    def scan(self, pos):
+        import torch
+        p = torch.as_tensor(np.ascontiguousarray(pos, np.float32), device=self.dev).reshape(-1, 3).contiguous()
+        n, N = p.shape[0], self.q.shape[0]
+        out = torch.empty(n * N * 4, dtype=torch.float32, device=self.dev)
+        self.ctx.forward_comp_device(p, n, self.q32, N, out)
+        self.stats["scan_trials"] += n * N
+        return out.view(n, N, 4)
+
+    # 2. top Nr_seed rows by completeness
+    def top(self, out, q_rows):
+        """q_rows: (n, N, 4) or (N, 4) orientations of the scored rows; returns (n, k, 4) float64."""
+        import torch
+        k = min(self.nr_seed, out.shape[1])
+        idx = sort_desc_nan_first(out[:, :, 2].double(), dim=1)[:, :k]
+        if q_rows.dim() == 2:
+            return q_rows[idx]
+        return torch.gather(q_rows, 1, idx[:, :, None].expand(-1, -1, 4))
+
+    def score_pairs(self, pos64, q64, tv, to):
+        import torch
+        out = torch.empty(tv.numel() * 4, dtype=torch.float32, device=self.dev)
+        self.ctx.score_trials_device(pos64, pos64.shape[0], q64, q64.shape[0], tv, to, tv.numel(), out)
+        return out.view(-1, 4)
+
+    # 3. local refine of every candidate; best row of each grid
+    def local_best(self, pos, cand, nr: int = NR_LOCAL, gridsize: float = GRID_LOCAL):
+        """cand: (n, k, 4) float64.  Returns (best_q (n, k, 4), best_C (n, k) float64 with NaN)."""
+        import torch
+        n, k = cand.shape[0], cand.shape[1]
+        pos32 = _f32(torch.as_tensor(np.ascontiguousarray(pos, np.float64), device=self.dev).reshape(-1, 3))
+        L = (nr + 1) ** 3 + 1
+        best_q = torch.empty(n, k, 4, dtype=torch.float64, device=self.dev)
+        best_c = torch.empty(n, k, dtype=torch.float64, device=self.dev)
+        per = max(1, TRIALS_PER_LAUNCH // max(1, k * L))
+        for s0 in range(0, n, per):
+            s1 = min(n, s0 + per)
+            m = s1 - s0
+            grids = local_grids(cand[s0:s1].reshape(-1, 4), nr, gridsize)          # (m*k, L, 4)
+            q32 = _f32(grids.reshape(-1, 4)).contiguous()                           # MEX q is single
+            tv = torch.arange(m, dtype=torch.int32, device=self.dev).repeat_interleave(k * L)
+            to = torch.arange(m * k * L, dtype=torch.int32, device=self.dev)
+            res = self.score_pairs(pos32[s0:s1].contiguous(), q32, tv, to).view(m, k, L, 4)
+            C = res[..., 2].double()
+            Cm = torch.where(torch.isnan(C), torch.full_like(C, -math.inf), C)
+            j = torch.argmax(Cm, dim=2)                                             # first maximum
+            best_q[s0:s1] = torch.gather(grids.view(m, k, L, 4), 2, j[:, :, None, None].expand(-1, -1, 1, 4))[:, :, 0]
+            best_c[s0:s1] = torch.gather(C, 2, j[:, :, None])[:, :, 0]
+            self.stats["local_trials"] += m * k * L
+        return best_q, best_c
+
+    # 4. batched fminsearchbnd on 1 - C
+    def fit_nm(self, pos, x0):
+        import torch
+        p = torch.as_tensor(np.ascontiguousarray(pos, np.float64), device=self.dev).reshape(-1, 3).contiguous()
+        x0 = x0.reshape(-1, 3).contiguous()
+        n = x0.shape[0]
+        x = torch.empty(n, 3, dtype=torch.float64, device=self.dev)
+        fval = torch.empty(n, dtype=torch.float64, device=self.dev)
+        ev = torch.empty(n, dtype=torch.int32, device=self.dev)
+        it = torch.empty(n, dtype=torch.int32, device=self.dev)
+        fl = torch.empty(n, dtype=torch.int32, device=self.dev)
+        self.ctx.fit_orientation_nm(p, x0, n, x, fval, ev, it, fl, FIT_HALF_WIDTH, FIT_MAX_EVALS, FIT_MAX_EVALS,
+                                    FIT_TOL_F, FIT_TOL_X)
+        self.stats["fit_seeds"] += n
+        self.stats["fit_evals"] += int(ev.sum().item())
+        return x, fval, ev, it, fl
+
+    # 5. Euler round trip and final scoring (FP64 U, FP64 pos)
+    def final(self, pos, x):
+        import torch
+        xs = x.reshape(-1, 3).cpu().numpy()
+        eul, rod, quat = zip(*(fitted_orientation(v) for v in xs))
+        quat = np.array(quat)
+        p = torch.as_tensor(np.ascontiguousarray(pos, np.float64), device=self.dev).reshape(-1, 3).contiguous()
+        qd = torch.as_tensor(quat, device=self.dev).contiguous()
+        out = torch.empty(len(xs) * 4, dtype=torch.float32, device=self.dev)
+        self.ctx.score_trials_device(p, p.shape[0], qd, qd.shape[0], None, None, len(xs), out)
+        self.stats["final_trials"] += len(xs)
+        return out.view(-1, 4).cpu().numpy().astype(np.float64), np.array(eul), np.array(rod), quat
+
+    def fit_candidates(self, seed_ids, pos, cand, fit_all: bool = False):
+        """fit_OR_constrain_with_local_comp_cuda for a batch: cand (n, k, 4) -> rows (n, 18) and the
+        1-based candidate index that gave each row (confident_index_list)."""
+        import torch
+        pos = np.asarray(pos, np.float64).reshape(-1, 3)
+        n, k = cand.shape[0], cand.shape[1]
+        best_q, best_c = self.local_best(pos, cand)
+        order = sort_desc_nan_first(best_c, dim=1)                                  # sortrows(Output_max, 3, 'descend')
+        nfit = k if fit_all else 1
+        sel = order[:, :nfit]
+        x0 = torch.gather(best_q, 1, sel[:, :, None].expand(-1, -1, 4))[:, :, 1:].contiguous()
+        pos_rep = np.repeat(pos, nfit, axis=0)
+        if self.fit:
+            x, _, _, _, _ = self.fit_nm(pos_rep, x0)
+        else:
+            x = x0.reshape(-1, 3)
+        out, eul, rod, quat = self.final(pos_rep, x)
+        C = out[:, 1] / out[:, 0]                                                   # Nr_intersect / Nr_simu
+        rows = np.zeros((n * nfit, 18))
+        rows[:, 0] = np.repeat(np.asarray(seed_ids, np.float64), nfit)
+        rows[:, 1:4] = pos_rep
+        rows[:, 4], rows[:, 5], rows[:, 6], rows[:, 7] = out[:, 0], out[:, 1], C, out[:, 3]
+        rows[:, 8:11], rows[:, 11:14], rows[:, 14:18] = eul, rod, quat
+        rows = rows.reshape(n, nfit, 18)
+        Cs = np.where(np.isnan(rows[:, :, 6]), -np.inf, rows[:, :, 6])
+        pick = np.argmax(Cs, axis=1)                                                 # max(indexing_result(:,7))
+        cand_id = sel.cpu().numpy()[np.arange(n), pick] + 1
+        return rows[np.arange(n), pick], cand_id
+
+    def index(self, seed_ids, pos, fit_all: bool = False):
+        """Steps 1-5 for seeds at ``pos`` (n x 3 mm) against the full grid."""
+        out = self.scan(pos)
+        cand = self.top(out, self.q)
+        return self.fit_candidates(seed_ids, pos, cand, fit_all)
+
+    def index_local(self, seed_id, pos, q_center, nr: int = NR_RECENTRE, gridsize: float = GRID_LOCAL):
+        """Re-indexing at a moved centre: ori_local_sampling(q, 4) scanned, then steps 2-5."""
+        import torch
+        qc = torch.as_tensor(np.asarray(q_center, np.float64).reshape(1, 4), device=self.dev)
+        grid = local_grids(qc, nr, gridsize)[0]                                     # (126, 4)
+        p = np.asarray(pos, np.float64).reshape(1, 3)
+        p32 = _f32(torch.as_tensor(p, device=self.dev))
+        tv = torch.zeros(grid.shape[0], dtype=torch.int32, device=self.dev)
+        to = torch.arange(grid.shape[0], dtype=torch.int32, device=self.dev)
+        out = self.score_pairs(p32.contiguous(), _f32(grid).contiguous(), tv, to).view(1, -1, 4)
+        self.stats["scan_trials"] += grid.shape[0]
+        cand = self.top(out, grid[None])
+        return self.fit_candidates([seed_id], p, cand)
+
+
+# ---- the engine -----------------------------------------------------------------------------------
+
+def pos2ind(pos_indexing, tomo_scale, VoxSize, RecVolumePixel, sz, simap_data_flag):
+    """pos2ind.m: 1-based voxel indices of a position [mm], clipped to the volume."""
+    p = np.asarray(pos_indexing, np.float64)
+    c = np.asarray(tomo_scale["Center"], np.float64)
+    d = np.asarray(tomo_scale["Dimension"], np.float64)
+    if simap_data_flag == 1:
+        pi = np.array([(-p[0] - c[0]) / VoxSize + d[0] / 2, (-p[1] - c[1]) / VoxSize + d[1] / 2,
+                       (p[2] - c[2]) / VoxSize + d[2] / 2])
+    else:
+        pi = (p - c) / VoxSize + d / 2
+    pi = np.ceil(pi - np.asarray(RecVolumePixel, np.float64)[:, 0] + 1)
+    return np.clip(pi, 1, np.asarray(sz)).astype(np.int64)
+
+
+def GrainMapping_engine_gpu_comp(pos_list, OR, RotDet, Spots, proj_bin_bw, rot_angles, S, B, Ahkl, nrhkl, thetamax,
+                                 lambda_min, lambda_max, Lsam2sou, Lsam2det, TrustComp, minComp, minEucDis, dety00,
+                                 detz00, P0y, P0z, RotAxisOffset, pixelysize, pixelzsize, dety0, detz0, detysize,
+                                 detzsize, BeamStopY, BeamStopZ, drop_off, maxD, DS, tomo_scale, VoxSize,
+                                 RecVolumePixel, FirstGrainID, simap_data_flag, maxDmedian, Nr_seed,
+                                 OutputFolder=None, iter=1, check_fit_all=0, batch: int = 64):
+    """GrainMapping_engine_gpu_comp.m:11-331 with batched, speculative seed indexing.
+
+    ``OR``: dict with 'q' (N x 4); ``DS``: dict of the sample maps (Mask, Completeness,
+    GrainId, Rodrigues 3 x dims, EulerZXZ 3 x dims, IPF001 3 x dims, Dismedian, Ninter,
+    VisitFlag, ...), updated copies are returned.  ``Spots`` (experimental centroids) feed
+    the grain-centre fit of :126-161, which is not part of this build: pass None (the
+    reference then takes Spot_L = 20 px, :201-206).  ``minEucDis``, ``dety0`` and ``detz0``
+    must equal the scorer's options (0.5 px threshold, detector centre); ``OutputFolder`` is
+    not written.  Returns (indexing_final (n x 18), pos_list_new (n x 3), DS_out,
+    Nr_indexed_voxel (n)).  Runs on the module context of ``grainrecon_b200.forward``, which
+    keeps the distance map resident between this engine and the region grower.
+    """
+    from . import forward as FW
+    ctx = FW.context()
+    pos_list = np.asarray(pos_list, np.float64).reshape(-1, 3)
+    n = len(pos_list)
+    DSo = {k: np.array(v, copy=True) for k, v in DS.items()}
+    Comp, VisitFlag, GrainId = DSo["Completeness"], DSo["VisitFlag"], DSo["GrainId"]
+    Mask = DSo["Mask"]
+    sz = Comp.shape
+    hkl = FW._hkl(Ahkl, nrhkl)
+    param = FW._param(hkl.shape[0], len(rot_angles), Lsam2sou, Lsam2det, P0y, P0z, dety00, detz00, pixelysize,
+                      pixelzsize, detysize, detzsize, BeamStopY, BeamStopZ, thetamax, lambda_min, lambda_max,
+                      RotAxisOffset)
+    ctx.set_geometry(G.flat_rowmajor(S), G.flat_rowmajor(B), G.flat_hkl(hkl), np.asarray(rot_angles, np.float32),
+                     G.flat_rowmajor(RotDet), param)
+    flat = FW._map_for_call(proj_bin_bw)
+    if flat is not None:
+        a = np.asarray(proj_bin_bw)
+        ctx.upload_masks(flat, a.shape[0], a.shape[1], a.shape[2])
+    indexer = SeedIndexer(ctx, OR["q"], Nr_seed)
+    indexing_final = np.zeros((n, 18))
+    pos_list_new = np.zeros((n, 3))
+    Nr_indexed_voxel = np.zeros(n)
+    candidate_id = np.zeros(n)
+    fit_all_track = np.zeros(n)
+    SeedIndexing = np.zeros((n, 15))
+    replace_count = np.zeros(n, np.int64)
+    spec = {}
+    ind_trusted = None
+
+    def trusted_indices():
+        idx = np.argwhere(Comp >= TrustComp) + 1
+        if len(idx) == 0:
+            idx = np.argwhere(Comp >= min(minComp * 1.5, TrustComp * 0.8)) + 1
+        return idx
+
+    if check_fit_all == 1:
+        ind_trusted = trusted_indices()
+
+    def skip(pi, count):
+        c, v = Comp[tuple(pi - 1)], VisitFlag[tuple(pi - 1)]
+        return not ((c < TrustComp or (count > 0 and c >= TrustComp)) and v != 1)
+
+    def fit_all_for(pi):
+        if check_fit_all != 1 or ind_trusted is None or len(ind_trusted) == 0:
+            return False
+        return bool(np.min(np.sqrt(((ind_trusted - pi) ** 2).sum(1))) > 2)
+
+    def speculate(i0):
+        """Index the next window of seeds that would be processed now, in one batch."""
+        ids, fa = [], []
+        for j in range(i0, min(n, i0 + batch)):
+            if j in spec:
+                continue
+            pi = pos2ind(pos_list[j], tomo_scale, VoxSize, RecVolumePixel, sz, simap_data_flag)
+            if j == i0 or not skip(pi, 0):
+                ids.append(j)
+                fa.append(fit_all_for(pi))
+        for flag in (False, True):
+            sel = [j for j, f in zip(ids, fa) if f == flag]
+            if sel:
+                rows, cid = indexer.index([j + 1 for j in sel], pos_list[sel], fit_all=flag)
+                for r, j in enumerate(sel):
+                    spec[j] = (rows[r], cid[r], flag)
+
+    gid_prev = int((DS["GrainId"] > 0).sum())
+    for i in range(n):
+        stop = False
+        pos_indexing = pos_list[i].copy()
+        temp = None
+        while not stop and replace_count[i] <= 3:
+            pi = pos2ind(pos_indexing, tomo_scale, VoxSize, RecVolumePixel, sz, simap_data_flag)
+            if not skip(pi, replace_count[i]):
+                if replace_count[i] == 0:
+                    if i not in spec:
+                        speculate(i)
+                    row, cid, fa = spec.pop(i)
+                    indexing_final[i] = row
+                    candidate_id[i] = cid
+                    fit_all_track[i] = 1 if fa else 0
+                else:
+                    rows, _ = indexer.index_local(i + 1, pos_indexing, temp[14:18])
+                    indexing_final[i] = rows[0]
+                C, med = indexing_final[i, 6], indexing_final[i, 7]
+                if C < minComp or C < Comp[tuple(pi - 1)] or med > maxDmedian:
+                    stop = True
+                    pos_list_new[i] = pos_indexing
+                    VisitFlag[tuple(pi - 1)] = 0.8
+                else:
+                    temp = indexing_final[i].copy()
+                    replace_center = 0
+                    if temp[6] >= Comp[tuple(pi - 1)]:
+                        Comp[tuple(pi - 1)] = temp[6]
+                        UU = G.quat_to_u(temp[14:18])
+                        J, C_out, D_out, N_out, center, replace_center, idx = FW.grow_indexed_region_cuda(
+                            Comp, Mask, DSo["Dismedian"], DSo["Ninter"], pi, 20, drop_off, maxD, temp[6], UU,
+                            proj_bin_bw, rot_angles, S, B, Ahkl, nrhkl, RotDet, thetamax, lambda_min, lambda_max,
+                            Lsam2sou, Lsam2det, dety00, detz00, P0y, P0z, RotAxisOffset, pixelysize, pixelzsize,
+                            detysize, detzsize, BeamStopY, BeamStopZ, RecVolumePixel, tomo_scale, VoxSize,
+                            simap_data_flag, maxDmedian)
+                        ix = tuple((idx - 1).T)
+                        Nr_indexed_voxel[i] = len(idx)
+                        gid = i + FirstGrainID
+                        GrainId[ix] = gid
+                        if "Rodrigues" in DSo:
+                            DSo["Rodrigues"][(slice(None),) + ix] = temp[11:14, None]
+                        if "IPF001" in DSo:
+                            DSo["IPF001"][(slice(None),) + ix] = (temp[8:11] / np.linalg.norm(temp[8:11]))[:, None]
+                        if "EulerZXZ" in DSo:
+                            DSo["EulerZXZ"][(slice(None),) + ix] = temp[8:11, None]
+                        VisitFlag[ix] = 0.5
+                        VisitFlag[tuple(pi - 1)] = 1
+                        Comp[ix] = C_out[ix]
+                        DSo["Dismedian"][ix] = D_out[ix]
+                        DSo["Ninter"][ix] = N_out[ix]
+                        center = np.asarray(center, np.float64)
+                        if replace_center == 1 and GrainId[tuple(center.astype(np.int64) - 1)] != gid:
+                            # ind2sub(find(GrainId == gid)): column-major order, so the first
+                            # nearest voxel is the reference's
+                            all_id = np.argwhere(GrainId.transpose(2, 1, 0) == gid)[:, ::-1] + 1
+                            center = all_id[np.argmin(np.sqrt(((all_id - center) ** 2).sum(1)))].astype(np.float64)
+                            replace_center = 1 if np.sqrt(((center - pi) ** 2).sum()) > maxD else 0
+                    if replace_center == 0:
+                        stop = True
+                        pos_list_new[i] = pos_indexing
+                    else:
+                        replace_count[i] += 1
+                        rvp = np.asarray(RecVolumePixel, np.float64)[:, 0]
+                        newp = ((center + rvp - 1) - np.asarray(tomo_scale["Dimension"], np.float64) / 2) * VoxSize \
+                            + np.asarray(tomo_scale["Center"], np.float64)
+                        if simap_data_flag == 1:
+                            newp[0], newp[1] = -newp[0], -newp[1]
+                        pos_list_new[i] = newp
+                        pos_indexing = newp
+            else:
+                stop = True
+                pos_list_new[i] = pos_indexing
+        spec.pop(i, None)
+        n_gid = int((GrainId > 0).sum())
+        SeedIndexing[i] = [*indexing_final[i, :11], Nr_indexed_voxel[i], n_gid - gid_prev, candidate_id[i],
+                           fit_all_track[i]]
+        gid_prev = n_gid
+        # :300-316: switch the fit-all mode on (and stop early) when seeds stop producing grains
+        if check_fit_all != 1 and i + 1 > 200 and np.any(SeedIndexing[i - 180:i + 1, 0] > 0):
+            w = SeedIndexing[i - 180:i + 1]
+            if (w[:, 12] > 0).sum() / (w[:, 0] > 0).sum() < 0.05:
+                check_fit_all = 1
+                ind_trusted = np.argwhere(DS["GrainId"] > 0) + 1
+                spec.clear()
+        if check_fit_all == 1 and i + 1 > 200 and np.any(SeedIndexing[i - 50:i + 1, 0] > 0):
+            w = SeedIndexing[i - 50:i + 1]
+            if (w[:, 12] > 0).sum() / (w[:, 0] > 0).sum() < 0.05:
+                break
+    DSo["SeedIndexing"] = SeedIndexing
+    DSo["indexer_stats"] = indexer.stats
+    return indexing_final, pos_list_new, DSo, Nr_indexed_voxel

@@ -151,6 +151,40 @@ int grc_compete_device(grc_ctx *ctx, const float *d_rows5, int64_t m, const floa
                        float *d_trial_out);
 
 /*
+ * Trial list in FP64 on device buffers: trial t scores voxel d_trial_voxel[t] (a row of
+ * d_pos, 3 doubles per voxel [mm]) against orientation d_trial_orient[t] (a row of d_q,
+ * 4 doubles [q0 q1 q2 q3] per orientation, used as given).  Both index arrays NULL:
+ * trial t = (voxel t, orientation t) and n_vox = n_q = n_trials.  d_out: 4 floats per
+ * trial as grc_forward_comp.  This is the scorer called with an FP64 orientation --
+ * forward_comp(UU, proj_bin_bw, pos, ...) of GrainMapping_engine_gpu_comp.m:155 and the
+ * objective of fit_OR_fun_local.m:2-98 -- batched over any (voxel, orientation) pairs:
+ * the local refine grids of fit_OR_constrain_with_local_comp_cuda.m:19-49 (Nr_seed x 730
+ * orientations at one voxel) and the final scoring of fitted orientations.  An index out
+ * of range is GRC_EINVAL.
+ */
+int grc_score_trials_device(grc_ctx *ctx, const double *d_pos, int64_t n_vox, const double *d_q, int64_t n_q,
+                            const int32_t *d_trial_voxel, const int32_t *d_trial_orient, int64_t n_trials,
+                            float *d_out);
+
+/*
+ * Batched orientation fit of the seeding stage: for each of n seeds, a bounded
+ * Nelder-Mead (fminsearchbnd over (q1, q2, q3), bounds max(x0-hw,-1)..min(x0+hw,1),
+ * q0 = sqrt(1 - q1^2 - q2^2 - q3^2)) minimising 1 - completeness at the seed position.
+ * Replaces the per-seed fminsearchbnd(fit_OR_fun_local, ...) call of
+ * fit_OR_constrain_with_local_comp_cuda.m:115-126 (hw 0.02, MaxFunEvals = MaxIter = 2000,
+ * TolFun 1e-10, TolX 1e-4 in fminsearch's default).  Every simplex follows the sequential
+ * fminsearch rules (reflection 1, expansion 2, contractions 1/2, shrink 1/2, initial
+ * simplex x0 and 5% steps, the 2*pi shift of the sine transform); all seeds advance
+ * together, one scorer launch per step.  d_pos: 3 doubles per seed [mm]; d_x0: 3 doubles
+ * per seed.  Outputs (device): d_x (3 per seed, the fitted q1..q3), d_fval (1 - C at d_x's
+ * simplex vertex), and optionally d_evals, d_iters, d_flag (int32: 1 converged by
+ * TolFun/TolX, 0 stopped by MaxFunEvals/MaxIter).  Returns after the work has finished.
+ */
+int grc_fit_orientation_nm(grc_ctx *ctx, const double *d_pos, const double *d_x0, int64_t n, double half_width,
+                           int max_evals, int max_iter, double tol_f, double tol_x, double *d_x, double *d_fval,
+                           int32_t *d_evals, int32_t *d_iters, int32_t *d_flag);
+
+/*
  * Allocation-free seeding scan (no counterpart in the reference: the MEX functions
  * always allocate their gpuArray output).  For callers that must not allocate GPU
  * memory while they score -- a MEX shim inside MATLAB's gpuArray memory manager, a
