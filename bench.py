@@ -381,6 +381,113 @@ def run_grow(args):
     return 0
 
 
+def seed_cpu_baseline(s, host_map, pos, q, nr_seed, evals_per_seed, n_scan=2048, nm_evals=300):
+    """Oracle time per seed for the same indexing work: the scan and local-refine trials at the
+    oracle's multi-core rate (a sample of ``n_scan`` orientations), the Nelder-Mead evaluations at
+    its one-core rate (a sample of ``nm_evals`` evaluations: fminsearchbnd is sequential)."""
+    from oracle import oracle as O
+    from oracle import seed_oracle as SO
+    S9, B9, hkl, rot, R9, p = s.mex_arrays()
+    sc = SO.Scene(S9, B9, hkl, rot, R9, p, host_map)
+    t0 = time.perf_counter()
+    sc.scan(pos[0], q[:n_scan])
+    t_trial = (time.perf_counter() - t0) / n_scan
+    f = SO.nm_objective(sc, pos[0].astype(np.float64))
+    x = np.asarray(q[0], np.float64)[1:]
+    t0 = time.perf_counter()
+    for k in range(nm_evals):
+        f(x + 1e-5 * k)
+    t_eval = (time.perf_counter() - t0) / nm_evals
+    trials = len(q) + nr_seed * 730 + 1
+    per_seed = trials * t_trial + evals_per_seed * t_eval
+    return {"value": 1.0 / per_seed, "unit": "seeds/s", "cores": O.max_threads(), "kind": "port",
+            "sample": (f"{n_scan} scan trials on {O.max_threads()} threads ({1 / t_trial:.0f} trials/s) and "
+                       f"{nm_evals} Nelder-Mead evaluations on one thread ({1 / t_eval:.0f} evals/s), scaled to "
+                       f"{trials} trials + {evals_per_seed:.0f} evaluations per seed"),
+            "seconds_per_seed": per_seed}
+
+
+def run_seed(args):
+    """Seeding stage per seed: scan of the 32,768-orientation grid, top Nr_seed, local refine of
+    every candidate (730 orientations each), batched fminsearchbnd, final scoring."""
+    import torch
+    from grainrecon_b200 import seeding as SD
+    from grainrecon_b200 import synth
+    from grainrecon_b200._lib import Context
+
+    rank, world, local = env_rank()
+    torch.cuda.set_device(local)
+    s, pos, q = build_problem("al400", args.seed)
+    ctx = Context(local)
+    want_cpu = rank == 0 and not args.no_cpu_baseline
+    host_map = synth.device_maps(s, ctx, keep_host_map=want_cpu)
+    ix = SD.SeedIndexer(ctx, q, nr_seed=args.nr_seed)
+    n = args.seed_batch
+    pos64 = pos.astype(np.float64)
+
+    def batch(k):
+        lo = (k * n) % (len(pos64) - n)
+        return list(range(lo + 1, lo + n + 1)), pos64[lo:lo + n]
+
+    for k in range(args.warmup):
+        ix.index(*batch(k))
+    torch.cuda.synchronize()
+    # phase split of one batch (separately synchronised, untimed)
+    ids, p = batch(args.warmup)
+    ph = {}
+    t0 = time.perf_counter()
+    out = ix.scan(p)
+    cand = ix.top(out, ix.q)
+    torch.cuda.synchronize()
+    ph["scan_top_s"] = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    best_q, best_c = ix.local_best(p, cand)
+    order = SD.sort_desc_nan_first(best_c, dim=1)[:, :1]
+    x0 = torch.gather(best_q, 1, order[:, :, None].expand(-1, -1, 4))[:, :, 1:].contiguous()
+    torch.cuda.synchronize()
+    ph["local_refine_s"] = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    x, fval, ev, it, fl = ix.fit_nm(p, x0)
+    torch.cuda.synchronize()
+    ph["nelder_mead_s"] = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    ix.final(p, x)
+    torch.cuda.synchronize()
+    ph["final_s"] = time.perf_counter() - t0
+    evals = ev.double().mean().item()
+    with ClockSampler(local) as clk:
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        rows = None
+        for k in range(args.steps):
+            rows, _ = ix.index(*batch(args.warmup + 1 + k))
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+    dt = max_over_ranks(dt, torch.device("cuda", local))
+    seeds = n * args.steps * world
+    line = {"metric": "seeds indexed/s", "value": seeds / dt, "unit": "seeds/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": (f"seeding stage: FCC Al 400 grains, 2048x2048 detector, 361 projections; "
+                                    f"{n} seeds per step x ({N_ORIENT} scan + {args.nr_seed} x 730 local-refine "
+                                    f"trials + fminsearchbnd (<= 2000 evaluations) + 1 final)"),
+                       "nr_seed": args.nr_seed, "seeds_per_step": n,
+                       "l2": "inputs larger than L2: the resident map is read by every step"},
+            "clocks": clk.summary(),
+            "e2e": {"value": seeds / dt, "unit": "seeds/s", "h2d_bytes_per_step": n * 3 * 8,
+                    "d2h_bytes_per_step": n * 18 * 8,
+                    "note": "host seed positions in, host indexing rows out: the timed steps are end to end"},
+            "phases_one_batch_s": ph, "nm_mean_evaluations": evals, "nm_converged": float((fl == 1).double().mean()),
+            "mean_C": float(np.nanmean(rows[:, 6])) if rows is not None else None,
+            "trials_per_seed": N_ORIENT + args.nr_seed * 730 + 1 + evals}
+    if want_cpu:
+        line["cpu_baseline"] = seed_cpu_baseline(s, host_map, pos, q, args.nr_seed, evals)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    return 0
+
+
 def verify_fitted_completeness(ctx, fitted_geo10, seed, n_vox=64, n_or=1024):
     """Score the al400 sample's masks with the true and with the fitted geometry.
 
@@ -460,7 +567,10 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="al400", choices=["al400", "fe6", "al400-grow", "fe-fit", "al-geofit"])
+    ap.add_argument("--config", default="al400", choices=["al400", "fe6", "al400-grow", "fe-fit", "al-geofit",
+                                                                "al400-seed"])
+    ap.add_argument("--nr-seed", type=int, default=400, help="al400-seed: candidates refined per seed")
+    ap.add_argument("--seed-batch", type=int, default=16, help="al400-seed: seeds per step")
     ap.add_argument("--fit-grains", type=int, default=0, help="0: 5,000 (fe-fit) or 2,000 (al-geofit)")
     ap.add_argument("--no-verify", action="store_true", help="al-geofit: skip the completeness re-check")
     ap.add_argument("--nm-iters", type=int, default=400)
@@ -480,6 +590,8 @@ def main():
         return run_grow(args)
     if args.config in ("fe-fit", "al-geofit"):
         return run_fit(args)
+    if args.config == "al400-seed":
+        return run_seed(args)
     return run_ours(args)
 
 
