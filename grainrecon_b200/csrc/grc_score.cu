@@ -243,13 +243,18 @@ __device__ __forceinline__ int64_t landing_fp32(const Geo &g, const RowF &r, con
         // far off the detector (or NaN): certain rejection only for finite values
         return (isfinite(u) && isfinite(v)) ? -1 : -2;
     }
-    // nearest integer; within the ambiguity band of a half-pixel the item goes to the
-    // exact path, so the tie rule of rintf never decides anything
-    const float ru = rintf(u), rv = rintf(v);
+    // nearest integer by the 1.5*2^23 addition (|u|, |v| < 2^22 here): the sum's low mantissa
+    // bits hold the rounded value, read back as an integer without a conversion instruction.
+    // Within the ambiguity band of a half-pixel the item goes to the exact path, so the tie
+    // rule of the rounding never decides anything.
+    constexpr float kRound = 12582912.0f;
+    const float tu = __fadd_rn(u, kRound), tv = __fadd_rn(v, kRound);
+    const float ru = __fsub_rn(tu, kRound), rv = __fsub_rn(tv, kRound);
     if (fabsf(u - ru) > 0.5f - kAmbigPx || fabsf(v - rv) > 0.5f - kAmbigPx) return -2;
-    if (!(ru >= 1.0f && ru <= (float)g.detysize && rv >= 1.0f && rv <= (float)g.detzsize)) return -1;
+    const int iu = __float_as_int(tu) - 0x4B400000, iv = __float_as_int(tv) - 0x4B400000;
+    if (!(iu >= 1 && iu <= g.detysize && iv >= 1 && iv <= g.detzsize)) return -1;
     if (ru >= g.bsy0f && ru <= g.bsy1f && rv >= g.bsz0f && rv <= g.bsz1f) return -1;
-    const uint32_t in_plane = (uint32_t)((int)ru - 1) * (uint32_t)g.detzsize + (uint32_t)((int)rv - 1);
+    const uint32_t in_plane = (uint32_t)(iu - 1) * (uint32_t)g.detzsize + (uint32_t)(iv - 1);
     return (int64_t)iw * g.plane + in_plane;
 }
 
@@ -672,7 +677,6 @@ __global__ void __launch_bounds__(kThreads, 2) mark_kernel(Geo g, ScoreBufs b, W
 // map pixels being read belong to a few projections at a time and stay in L2.
 constexpr int kSlots = 64;
 constexpr int kWin = 8;
-constexpr int kSlotsPerWarp = kSlots / kWarps;
 constexpr int kHist8Words = 128;  // 256 u16 bins per slot, two per word
 
 __device__ __forceinline__ int64_t voxel_of(const Work &w, int64_t t) {
@@ -761,7 +765,7 @@ __global__ void __launch_bounds__(kThreads, GRC_SWEEP_BLOCKS) sweep_kernel(Geo g
     const int nslot = (int)min((int64_t)slots, n_trials - cta_base);
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const SweepSmem sm = sweep_carve(smem_raw, g.nhkl, rows_cap);
-    __shared__ int s_nv;
+    __shared__ int s_nv, s_next;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const unsigned lt = (1u << lane) - 1u;
     uint32_t *wq = sm.queue + warp * kQueueCap;
@@ -848,6 +852,7 @@ __global__ void __launch_bounds__(kThreads, GRC_SWEEP_BLOCKS) sweep_kernel(Geo g
             f.pad = 0.f;
             sm.rows[vl * kWin + wl] = f;
         }
+        if (tid == 0) s_next = 0;
         __syncthreads();
         int qn = 0, fn = 0;
         auto fast = [&](uint32_t item, bool valid) {
@@ -909,8 +914,12 @@ __global__ void __launch_bounds__(kThreads, GRC_SWEEP_BLOCKS) sweep_kernel(Geo g
                 }
             }
         };
-        for (int k = 0; k < kSlotsPerWarp; ++k) {
-            const int s = warp + kWarps * k;
+        // slots are handed out one at a time, so the warps of a CTA reach the end-of-window
+        // barrier together however unevenly the selected reflections fall on the slots
+        for (;;) {
+            int s = 0;
+            if (lane == 0) s = atomicAdd(&s_next, 1);
+            s = __shfl_sync(kFull, s, 0);
             if (s >= nslot) break;
             const float *sf = sm.subf + 12 * s;
             float gx[HPL], gy[HPL], gz[HPL], lo[HPL], hi[HPL];
