@@ -30,8 +30,13 @@ EXPORTS = [
     "grc_batch_capture", "grc_batch_replay", "grc_batch_autotune", "grc_batch_info", "grc_batch_destroy",
     "grc_fit_spot_count", "grc_fit_spot_fill", "grc_centroid_residual_adjoint", "grc_fit_grains_lm",
     "grc_fit_grains_nm", "grc_fit_grains_rms", "grc_fit_geometry_lm", "grc_fit_geometry_cost",
-    "grc_fit_geometry_rms", "grc_score_trials_device", "grc_fit_orientation_nm",
+    "grc_fit_geometry_rms", "grc_score_trials_device", "grc_fit_orientation_nm", "grc_pair_spots",
 ]
+
+# grc_spot_pair of the C header
+PAIR_DTYPE = np.dtype([("trial", "<i4"), ("iw", "<i4"), ("ih", "<i4"), ("spot", "<i4"), ("dety", "<f8"),
+                       ("detz", "<f8"), ("exp_y", "<f8"), ("exp_z", "<f8"), ("area", "<f8"), ("energy_kev", "<f8"),
+                       ("dis", "<f8")])
 NOALLOC_MAX_ORIENTATIONS = 65536
 
 
@@ -109,6 +114,7 @@ def load(path: str | None = None):
         "grc_fit_geometry_rms": [vp, f, i, f, f, f, f, f, f, i64, f],
         "grc_score_trials_device": [vp, f, i64, f, i64, f, f, i64, f],
         "grc_fit_orientation_nm": [vp, f, f, i64, d, i, i, d, d, f, f, f, f, f],
+        "grc_pair_spots": [vp, f, f, i64, f, i64, f, f, i64, C.POINTER(i64)],
     }
     for name, args in sig.items():
         fn = getattr(L, name)
@@ -286,6 +292,24 @@ class Context:
         self._dev(self.L.grc_fit_orientation_nm, _ptr(d_pos), _ptr(d_x0), n, half_width, max_evals, max_iter,
                                                   tol_f, tol_x, _ptr(d_x), _ptr(d_fval), _ptr(d_evals), _ptr(d_iters),
                                                   _ptr(d_flag))
+
+    def pair_spots(self, d_pos, d_q, n: int, d_spots, n_spots: int, d_proj_offsets, max_pairs: int = 0):
+        """Spot pairing (see the C header): returns a host structured array of PAIR_DTYPE, in
+        (trial, projection, reflection) order.  The device buffer grows when max_pairs is short."""
+        import torch
+        cap = max(int(max_pairs), 1024)
+        while True:
+            buf = torch.empty(cap * PAIR_DTYPE.itemsize, dtype=torch.uint8, device="cuda")
+            npairs = C.c_int64()
+            torch.cuda.current_stream().synchronize()
+            rc = self.L.grc_pair_spots(self.h, _ptr(d_pos), _ptr(d_q), n, _ptr(d_spots), n_spots,
+                                       _ptr(d_proj_offsets), _ptr(buf), cap, C.byref(npairs))
+            if rc == GRC_ECAPACITY and npairs.value > cap:
+                cap = int(npairs.value)
+                continue
+            self._check(rc)
+            m = int(npairs.value)
+            return buf[: m * PAIR_DTYPE.itemsize].cpu().numpy().view(PAIR_DTYPE).copy()
 
     def forward_comp_noalloc(self, pos, d_q, n_q: int, d_out):
         """Allocation-free seeding scan: host pos (3 floats), device d_q / d_out; see the C header."""

@@ -42,7 +42,7 @@ struct grc_ctx {
     grc::MapCodes mc{};
     int64_t mz = 0, my = 0, mrot = 0;
     std::vector<float> h_vals;
-    DevBuf fgeo, fne, ftrial, fcost0, fcost1, fimp, fhw, geo_dev, rot_cs, hkl, pos, U, res, tvoxel, rlist, in1, in2, in3, out, items, torient, counts, offsets, tmp, counter, p1, bad, nm;
+    DevBuf fgeo, fne, ftrial, fcost0, fcost1, fimp, fhw, geo_dev, rot_cs, hkl, pos, U, res, tvoxel, rlist, in1, in2, in3, out, items, torient, counts, offsets, tmp, counter, p1, bad, nm, sp_keys, sp_ids, sp_keys2, sp_ids2, cell_cnt, cell_off, pr_raw, pr_keys, pr_keys2, pr_ids, pr_ids2, pcount;
     grc::Geo *geo_pinned = nullptr;  // staging of the per-launch geometry copy
     int *nm_active = nullptr;        // pinned: seeds still running in the orientation fit
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -492,7 +492,7 @@ int grc_ctx_destroy(grc_ctx *ctx) {
         cudaStreamSynchronize(ctx->stream);
         cudaFreeHost(ctx->geo_pinned);
         if (ctx->nm_active) cudaFreeHost(ctx->nm_active);
-        DevBuf *all[] = {&ctx->nm, &ctx->fgeo, &ctx->fne, &ctx->ftrial, &ctx->fcost0, &ctx->fcost1, &ctx->fimp, &ctx->fhw,
+        DevBuf *all[] = {&ctx->nm, &ctx->sp_keys, &ctx->sp_ids, &ctx->sp_keys2, &ctx->sp_ids2, &ctx->cell_cnt, &ctx->cell_off, &ctx->pr_raw, &ctx->pr_keys, &ctx->pr_keys2, &ctx->pr_ids, &ctx->pr_ids2, &ctx->pcount, &ctx->fgeo, &ctx->fne, &ctx->ftrial, &ctx->fcost0, &ctx->fcost1, &ctx->fimp, &ctx->fhw,
                          &ctx->tvoxel, &ctx->rlist, &ctx->geo_dev, &ctx->rot_cs, &ctx->hkl, &ctx->pos, &ctx->U, &ctx->res, &ctx->in1, &ctx->in2,
                          &ctx->in3, &ctx->out, &ctx->items, &ctx->torient, &ctx->counts, &ctx->offsets,
                          &ctx->tmp, &ctx->counter, &ctx->p1, &ctx->bad};
@@ -790,6 +790,105 @@ int grc_fit_orientation_nm(grc_ctx *ctx, const double *d_pos, const double *d_x0
     ctx->stats.trials = steps * T;
     ctx->stats.kernel_launches = (int64_t)graphs * kSteps * (2 + launches / kSteps) + 2;
     ctx->stats.path = 1;
+    return GRC_OK;
+}
+
+static_assert(sizeof(grc_spot_pair) == sizeof(grc::PairRec), "grc_spot_pair layout");
+
+int grc_pair_spots(grc_ctx *ctx, const double *d_pos, const double *d_q, int64_t n, const double *d_spots,
+                   int64_t n_spots, const int64_t *d_proj_offsets, grc_spot_pair *d_pairs, int64_t max_pairs,
+                   int64_t *n_pairs) {
+    if (!ctx) return GRC_EINVAL;
+    Lock l(ctx);
+    if (!n_pairs) return fail(ctx, GRC_EINVAL, "pair: NULL n_pairs");
+    *n_pairs = 0;
+    TRY(check_ready(ctx));
+    ctx->stats = grc_stats{};
+    if (n < 0 || n_spots < 0 || max_pairs < 0) return fail(ctx, GRC_EINVAL, "negative size");
+    if (n == 0) return GRC_OK;
+    if (!d_pos || !d_q || !d_proj_offsets || (n_spots > 0 && !d_spots) || (max_pairs > 0 && !d_pairs))
+        return fail(ctx, GRC_EINVAL, "pair: NULL buffer");
+    if (n > (int64_t)INT32_MAX || n_spots > (int64_t)INT32_MAX)
+        return fail(ctx, GRC_ECAPACITY, "pair: more than 2^31-1 trials or spots");
+    const grc::Geo &g = ctx->geo;
+    constexpr int kCell = 16;
+    const int ncy = (g.detysize + kCell - 1) / kCell, ncz = (g.detzsize + kCell - 1) / kCell;
+    const int64_t ncell = (int64_t)g.nrot * ncy * ncz;
+    cudaStream_t s = ctx->stream;
+    // the projection offsets must describe the spot list
+    std::vector<int64_t> off(g.nrot + 1);
+    CU(cudaMemcpyAsync(off.data(), d_proj_offsets, sizeof(int64_t) * (g.nrot + 1), cudaMemcpyDeviceToHost, s));
+    CU(cudaStreamSynchronize(s));
+    if (off[0] != 0 || off[g.nrot] != n_spots)
+        return fail(ctx, GRC_EINVAL, "pair: projection offsets must run from 0 to n_spots");
+    for (int i = 0; i < g.nrot; ++i)
+        if (off[i + 1] < off[i]) return fail(ctx, GRC_EINVAL, "pair: projection offsets decrease at %d", i);
+    TRY(ensure(ctx, ctx->U, sizeof(double) * 9 * n));
+    TRY(ensure(ctx, ctx->pos, sizeof(double) * 3 * n));
+    TRY(ensure(ctx, ctx->cell_cnt, sizeof(int64_t) * (ncell + 1)));
+    TRY(ensure(ctx, ctx->cell_off, sizeof(int64_t) * (ncell + 1)));
+    TRY(ensure(ctx, ctx->sp_keys, sizeof(int32_t) * (n_spots + 1)));
+    TRY(ensure(ctx, ctx->sp_ids, sizeof(int32_t) * (n_spots + 1)));
+    TRY(ensure(ctx, ctx->sp_keys2, sizeof(int32_t) * (n_spots + 1)));
+    TRY(ensure(ctx, ctx->sp_ids2, sizeof(int32_t) * (n_spots + 1)));
+    TRY(ensure(ctx, ctx->pcount, sizeof(unsigned long long)));
+    TRY(ensure(ctx, ctx->pr_raw, sizeof(grc::PairRec) * (max_pairs > 0 ? max_pairs : 1)));
+    CU(grc::launch_quat_to_u_d(d_q, n, (double *)ctx->U.p, s));
+    CU(cudaMemcpyAsync(ctx->pos.p, d_pos, sizeof(double) * 3 * n, cudaMemcpyDeviceToDevice, s));
+    CU(cudaMemsetAsync(ctx->cell_cnt.p, 0, sizeof(int64_t) * (ncell + 1), s));
+    int end_bit = 1;
+    while (end_bit < 31 && ((int64_t)1 << end_bit) < ncell) ++end_bit;
+    if (n_spots > 0) {
+        CU(grc::launch_spot_keys(d_spots, d_proj_offsets, g.nrot, ncy, ncz, kCell, (int32_t *)ctx->sp_keys.p,
+                                 (int32_t *)ctx->sp_ids.p, (int64_t *)ctx->cell_cnt.p, s));
+        size_t tb = 0;
+        CU(cub::DeviceRadixSort::SortPairs(nullptr, tb, (const int32_t *)ctx->sp_keys.p, (int32_t *)ctx->sp_keys2.p,
+                                           (const int32_t *)ctx->sp_ids.p, (int32_t *)ctx->sp_ids2.p, n_spots, 0,
+                                           end_bit, s));
+        TRY(ensure(ctx, ctx->tmp, tb));
+        CU(cub::DeviceRadixSort::SortPairs(ctx->tmp.p, tb, (const int32_t *)ctx->sp_keys.p, (int32_t *)ctx->sp_keys2.p,
+                                           (const int32_t *)ctx->sp_ids.p, (int32_t *)ctx->sp_ids2.p, n_spots, 0,
+                                           end_bit, s));
+    }
+    {
+        size_t tb = 0;
+        CU(cub::DeviceScan::ExclusiveSum(nullptr, tb, (int64_t *)ctx->cell_cnt.p, (int64_t *)ctx->cell_off.p,
+                                         ncell + 1, s));
+        TRY(ensure(ctx, ctx->tmp, tb));
+        CU(cub::DeviceScan::ExclusiveSum(ctx->tmp.p, tb, (int64_t *)ctx->cell_cnt.p, (int64_t *)ctx->cell_off.p,
+                                         ncell + 1, s));
+    }
+    grc::SpotIndex si{d_spots, (const int64_t *)ctx->cell_off.p, (const int32_t *)ctx->sp_ids2.p, ncy, ncz, kCell};
+    CU(cudaMemsetAsync(ctx->pcount.p, 0, sizeof(unsigned long long), s));
+    TRY(stage_geo(ctx));
+    CU(grc::launch_pair(g, bufs(ctx), n, si, (grc::PairRec *)ctx->pr_raw.p, max_pairs,
+                        (unsigned long long *)ctx->pcount.p, ctx->num_sms, s));
+    unsigned long long cnt = 0;
+    CU(cudaMemcpyAsync(&cnt, ctx->pcount.p, sizeof(cnt), cudaMemcpyDeviceToHost, s));
+    CU(cudaStreamSynchronize(s));
+    *n_pairs = (int64_t)cnt;
+    if ((int64_t)cnt > max_pairs) return fail(ctx, GRC_ECAPACITY, "pair: %llu pairs exceed max_pairs", cnt);
+    if (cnt > 0) {
+        // atomics leave the pairs in arbitrary order: sort by (trial, projection, reflection)
+        const int64_t m = (int64_t)cnt;
+        TRY(ensure(ctx, ctx->pr_keys, sizeof(int64_t) * m));
+        TRY(ensure(ctx, ctx->pr_keys2, sizeof(int64_t) * m));
+        TRY(ensure(ctx, ctx->pr_ids, sizeof(int32_t) * m));
+        TRY(ensure(ctx, ctx->pr_ids2, sizeof(int32_t) * m));
+        CU(grc::launch_pair_keys((const grc::PairRec *)ctx->pr_raw.p, m, g.nrot, g.nhkl, (int64_t *)ctx->pr_keys.p,
+                                 (int32_t *)ctx->pr_ids.p, s));
+        size_t tb = 0;
+        CU(cub::DeviceRadixSort::SortPairs(nullptr, tb, (const int64_t *)ctx->pr_keys.p, (int64_t *)ctx->pr_keys2.p,
+                                           (const int32_t *)ctx->pr_ids.p, (int32_t *)ctx->pr_ids2.p, m, 0, 64, s));
+        TRY(ensure(ctx, ctx->tmp, tb));
+        CU(cub::DeviceRadixSort::SortPairs(ctx->tmp.p, tb, (const int64_t *)ctx->pr_keys.p, (int64_t *)ctx->pr_keys2.p,
+                                           (const int32_t *)ctx->pr_ids.p, (int32_t *)ctx->pr_ids2.p, m, 0, 64, s));
+        CU(grc::launch_pair_gather((const grc::PairRec *)ctx->pr_raw.p, (const int32_t *)ctx->pr_ids2.p, m,
+                                   (grc::PairRec *)d_pairs, s));
+        CU(cudaStreamSynchronize(s));
+    }
+    ctx->stats.trials = n;
+    ctx->stats.kernel_launches = 6 + (cnt > 0 ? 3 : 0);
     return GRC_OK;
 }
 

@@ -126,6 +126,27 @@ cudaError_t launch_simulate_work(const Geo &g, const ScoreBufs &b, const Work &w
                                  cudaStream_t s);
 cudaError_t launch_edt(const uint8_t *mask, int64_t nz, int64_t ny, int64_t nrot, float *map, cudaStream_t s);
 
+// Spot pairing (grc_score.cu: pair_kernel; index built in grc_seed.cu).  Same layout as the
+// public grc_spot_pair.
+struct PairRec {
+    int32_t trial, iw, ih, spot;
+    double dety, detz, exp_y, exp_z, area, energy_kev, dis;
+};
+struct SpotIndex {
+    const double *yza;        // 3 per spot: centroid dety, detz [pixel], area [pixel^2]
+    const int64_t *cell_off;  // [nrot * ncy * ncz + 1]
+    const int32_t *cell_ids;  // spot ids in (projection, cell, list) order
+    int ncy, ncz, cell_px;
+};
+cudaError_t launch_pair(const Geo &g, const ScoreBufs &b, int64_t n, const SpotIndex &si, PairRec *out, int64_t cap,
+                        unsigned long long *count, int num_sms, cudaStream_t s);
+// Cell index of a spot list: per spot its cell key ((iw * ncy + cy) * ncz + cz), then counts.
+cudaError_t launch_spot_keys(const double *yza, const int64_t *proj_off, int nrot, int ncy, int ncz, int cell_px,
+                             int32_t *keys, int32_t *ids, int64_t *cell_counts, cudaStream_t s);
+cudaError_t launch_pair_keys(const PairRec *p, int64_t n, int nrot, int nhkl, int64_t *keys, int32_t *ids,
+                             cudaStream_t s);
+cudaError_t launch_pair_gather(const PairRec *in, const int32_t *order, int64_t n, PairRec *out, cudaStream_t s);
+
 // FP64 trial lists (grc_seed.cu): U from double quaternions, work items from (voxel, orientation)
 // index pairs (bad |= 1 for an index out of range; that item is left empty).
 cudaError_t launch_quat_to_u_d(const double *q, int64_t n, double *U, cudaStream_t s);

@@ -156,11 +156,12 @@ __device__ void build_gw(const Geo &g, const double *__restrict__ hkl, const dou
 // forward_comp.m:28-59: sin(theta) = -cos(beta), cos(theta) = sin(beta), sin(phiy)
 // expanded, and the ray/plane intersection without normalising K_out.
 __device__ __forceinline__ int64_t landing_fp64(const Geo &g, const OmegaRow &r, double gxw, double gyw,
-                                                double gzw, int iw) {
+                                                double gzw, int iw, double *lam_out = nullptr) {
     const double G = sqrt(gxw * gxw + gyw * gyw + gzw * gzw);
     const double Gtx = r.c * gxw - r.s * gyw, Gty = r.s * gxw + r.c * gyw, Gtz = gzw;
     const double x = (r.kx * Gtx + r.ky * Gty + r.kz * Gtz) / G;  // cos(beta)
     const double lam = 2.0 * (2.0 * CUDART_PI / G) * (-x);        // 2 d sin(theta)
+    if (lam_out) *lam_out = lam;
     if (!(x < 0.0 && x > g.cbmax && lam > g.lmin && lam < g.lmax)) return -1;
     const double st = -x, ct = sqrt(1.0 - x * x);
     const double s2 = 2.0 * st * ct, c2 = 1.0 - 2.0 * st * st;
@@ -1171,6 +1172,75 @@ cudaError_t launch_mark_t(const Geo &g, const ScoreBufs &b, const Work &w, int n
     return cudaGetLastError();
 }
 
+
+// ---- spot pairing (forward_comp_pair_spots.m:60-85) ------------------------------------------
+// For every selected reflection of a trial whose pixel is a hit, the nearest measured spot
+// centroid of that projection (first in list order among equal distances) is paired when it
+// lies closer than min(sqrt(area), 15) pixels.  The spot index holds, per projection, the spots
+// of each cell of cell_px x cell_px pixels in list order.
+template <typename CodeT>
+__global__ void __launch_bounds__(128) pair_kernel(Geo g, ScoreBufs b, int64_t n, SpotIndex si, PairRec *out,
+                                                   int64_t cap, unsigned long long *count) {
+    __shared__ double sub[9];
+    const CodeT *codes = (const CodeT *)b.codes;
+    for (int64_t t = blockIdx.x; t < n; t += gridDim.x) {
+        __syncthreads();
+        if (threadIdx.x == 0) sub_matrix(g, b.U + 9 * t, sub);
+        __syncthreads();
+        const double *vp = b.vpos + 3 * t;
+        for (int iw = threadIdx.x; iw < g.nrot; iw += blockDim.x) {
+            const OmegaRow r = omega_row(g, b.rot_cs[iw], vp);
+            for (int ih = 0; ih < g.nhkl; ++ih) {
+                const double h = b.hkl[3 * ih], k = b.hkl[3 * ih + 1], l = b.hkl[3 * ih + 2];
+                const double x = sub[0] * h + sub[1] * k + sub[2] * l;
+                const double y = sub[3] * h + sub[4] * k + sub[5] * l;
+                const double z = sub[6] * h + sub[7] * k + sub[8] * l;
+                double lam = 0.0;
+                const int64_t idx = landing_fp64(g, r, x, y, z, iw, &lam);
+                if (idx < 0) continue;
+                const uint32_t code = (uint32_t)codes[idx];
+                if (code >= g.n_hit) continue;
+                const int64_t in_plane = idx - (int64_t)iw * g.plane;
+                const int dety = (int)(in_plane / g.detzsize) + 1, detz = (int)(in_plane % g.detzsize) + 1;
+                const int cy0 = max(0, (dety - 16) / si.cell_px), cy1 = min(si.ncy - 1, (dety + 14) / si.cell_px);
+                const int cz0 = max(0, (detz - 16) / si.cell_px), cz1 = min(si.ncz - 1, (detz + 14) / si.cell_px);
+                int best = -1;
+                double bd = 0.0;
+                for (int cy = cy0; cy <= cy1; ++cy)
+                    for (int cz = cz0; cz <= cz1; ++cz) {
+                        const int64_t cell = ((int64_t)iw * si.ncy + cy) * si.ncz + cz;
+                        for (int64_t q = si.cell_off[cell]; q < si.cell_off[cell + 1]; ++q) {
+                            const int id = si.cell_ids[q];
+                            const double dy = __dsub_rn(si.yza[3 * id], (double)dety);
+                            const double dz = __dsub_rn(si.yza[3 * id + 1], (double)detz);
+                            const double d = sqrt(__dadd_rn(__dmul_rn(dy, dy), __dmul_rn(dz, dz)));
+                            if (best < 0 || d < bd || (d == bd && id < best)) {
+                                best = id;
+                                bd = d;
+                            }
+                        }
+                    }
+                if (best < 0 || !(bd < fmin(sqrt(si.yza[3 * best + 2]), 15.0))) continue;
+                const unsigned long long slot = atomicAdd(count, 1ull);
+                if ((int64_t)slot < cap) {
+                    PairRec p;
+                    p.trial = (int32_t)t;
+                    p.iw = iw;
+                    p.ih = ih;
+                    p.spot = best;
+                    p.dety = dety;
+                    p.detz = detz;
+                    p.exp_y = si.yza[3 * best];
+                    p.exp_z = si.yza[3 * best + 1];
+                    p.area = si.yza[3 * best + 2];
+                    p.energy_kev = 12.398 / lam;
+                    p.dis = (double)b.vals[min(code, g.n_vals - 1u)];
+                    out[slot] = p;
+                }
+            }
+        }
+    }
+}
 }  // namespace
 
 size_t score_smem_bytes(int nrot, int nhkl) {
@@ -1234,6 +1304,17 @@ cudaError_t launch_sweep(const Geo &g, const ScoreBufs &b, const Work &w, int64_
     GRC_DISPATCH(4)
 #undef GRC_DISPATCH
     return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_pair(const Geo &g, const ScoreBufs &b, int64_t n, const SpotIndex &si, PairRec *out, int64_t cap,
+                        unsigned long long *count, int num_sms, cudaStream_t s) {
+    if (n <= 0) return cudaSuccess;
+    const int grid = (int)(n < (int64_t)num_sms * 16 ? n : (int64_t)num_sms * 16);
+    if (g.code_bits <= 16)
+        pair_kernel<uint16_t><<<grid, 128, 0, s>>>(g, b, n, si, out, cap, count);
+    else
+        pair_kernel<uint32_t><<<grid, 128, 0, s>>>(g, b, n, si, out, cap, count);
+    return cudaGetLastError();
 }
 
 }  // namespace grc

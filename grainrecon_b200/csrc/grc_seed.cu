@@ -60,6 +60,36 @@ __global__ void trial_items_k(const int32_t *tv, const int32_t *to, int64_t n, i
     }
 }
 
+// ---- spot index and pair ordering ----------------------------------------------------------
+
+// One block per projection: cell key and count of every spot (centroids outside the detector
+// fall into the border cells).
+__global__ void spot_keys_k(const double *yza, const int64_t *proj_off, int ncy, int ncz, int cell_px,
+                            int32_t *keys, int32_t *ids, int64_t *cell_counts) {
+    const int iw = blockIdx.x;
+    for (int64_t i = proj_off[iw] + threadIdx.x; i < proj_off[iw + 1]; i += blockDim.x) {
+        const double cy = floor((yza[3 * i] - 1.0) / cell_px), cz = floor((yza[3 * i + 1] - 1.0) / cell_px);
+        const int y = cy < 0.0 ? 0 : (cy > ncy - 1 ? ncy - 1 : (int)cy);
+        const int z = cz < 0.0 ? 0 : (cz > ncz - 1 ? ncz - 1 : (int)cz);
+        const int32_t key = (iw * ncy + y) * ncz + z;
+        keys[i] = key;
+        ids[i] = (int32_t)i;
+        atomicAdd((unsigned long long *)(cell_counts + key), 1ull);
+    }
+}
+
+__global__ void pair_keys_k(const PairRec *p, int64_t n, int nrot, int nhkl, int64_t *keys, int32_t *ids) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        keys[i] = ((int64_t)p[i].trial * nrot + p[i].iw) * nhkl + p[i].ih;
+        ids[i] = (int32_t)i;
+    }
+}
+
+__global__ void pair_gather_k(const PairRec *in, const int32_t *order, int64_t n, PairRec *out) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        out[i] = in[order[i]];
+}
+
 // ---- batched fminsearchbnd -------------------------------------------------------------
 
 enum : int { kInit = 0, kNormal = 1, kShrink = 2, kDone = 3 };
@@ -295,6 +325,23 @@ cudaError_t launch_quat_to_u_d(const double *q, int64_t n, double *U, cudaStream
 cudaError_t launch_trial_items(const int32_t *tv, const int32_t *to, int64_t n, int64_t n_vox, int64_t n_q,
                                longlong4 *items, int *bad, cudaStream_t s) {
     trial_items_k<<<blocks_for(n), kB, 0, s>>>(tv, to, n, n_vox, n_q, items, bad);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_spot_keys(const double *yza, const int64_t *proj_off, int nrot, int ncy, int ncz, int cell_px,
+                             int32_t *keys, int32_t *ids, int64_t *cell_counts, cudaStream_t s) {
+    spot_keys_k<<<nrot, kB, 0, s>>>(yza, proj_off, ncy, ncz, cell_px, keys, ids, cell_counts);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_pair_keys(const PairRec *p, int64_t n, int nrot, int nhkl, int64_t *keys, int32_t *ids,
+                             cudaStream_t s) {
+    pair_keys_k<<<blocks_for(n), kB, 0, s>>>(p, n, nrot, nhkl, keys, ids);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_pair_gather(const PairRec *in, const int32_t *order, int64_t n, PairRec *out, cudaStream_t s) {
+    pair_gather_k<<<blocks_for(n), kB, 0, s>>>(in, order, n, out);
     return cudaGetLastError();
 }
 

@@ -297,6 +297,120 @@ class SeedIndexer:
         return self.fit_candidates([seed_id], p, cand)
 
 
+# ---- measured spots: pairing and the grain-centre fit ------------------------------------------------
+
+def spot_arrays(Spots, nrot: int):
+    """(spots (m x 3) float64 [dety, detz, area], offsets (nrot + 1) int64) from per-projection spot
+    tables: either the reference's Spots{i} rows (centroid in columns 9-10, area in column 11,
+    get_spots.m:106-109) or (m x 3) arrays [dety, detz, area]."""
+    rows, off = [], [0]
+    for i in range(nrot):
+        a = np.asarray(Spots[i] if i < len(Spots) else np.zeros((0, 3)), np.float64)
+        if a.ndim == 1:
+            a = a.reshape(-1, 3) if a.size % 3 == 0 and a.size < 11 else a.reshape(1, -1)
+        a = a[:, 8:11] if a.shape[1] >= 11 else a[:, :3]
+        rows.append(a)
+        off.append(off[-1] + len(a))
+    sp = np.concatenate(rows) if off[-1] else np.zeros((0, 3))
+    return np.ascontiguousarray(sp), np.asarray(off, np.int64)
+
+
+def pair_spots(ctx, pos, quats, Spots, nrot: int):
+    """Pairs of every (pos, quaternion) trial with the measured spots (grc_pair_spots)."""
+    import torch
+    sp, off = spot_arrays(Spots, nrot)
+    d = lambda a: torch.as_tensor(np.ascontiguousarray(a), device="cuda")
+    pos = np.asarray(pos, np.float64).reshape(-1, 3)
+    q = np.asarray(quats, np.float64).reshape(-1, 4)
+    d_sp = d(sp.reshape(-1)) if len(sp) else torch.zeros(3, dtype=torch.float64, device="cuda")
+    return ctx.pair_spots(d(pos.reshape(-1)), d(q.reshape(-1)), len(pos), d_sp, len(sp), d(off))
+
+
+def hitted_spots_rows(pairs, U, pos, hkl, rot_angles):
+    """HittedSpots rows of forward_comp_pair_spots.m:78-79: [reshape(U,1,9) pos hkl Energy omega
+    exp_y exp_z area dety detz dis] (23 columns)."""
+    U = np.asarray(U, np.float64)
+    hkl = np.asarray(hkl, np.float64).reshape(-1, 3)
+    rows = np.zeros((len(pairs), 23))
+    rows[:, 0:9] = U.reshape(3, 3).T.reshape(-1)   # column-major, as reshape(U,1,9)
+    rows[:, 9:12] = np.asarray(pos, np.float64)
+    rows[:, 12:15] = hkl[pairs["ih"]]
+    rows[:, 15] = pairs["energy_kev"]
+    rows[:, 16] = np.asarray(rot_angles, np.float64)[pairs["iw"]]
+    rows[:, 17], rows[:, 18], rows[:, 19] = pairs["exp_y"], pairs["exp_z"], pairs["area"]
+    rows[:, 20], rows[:, 21], rows[:, 22] = pairs["dety"], pairs["detz"], pairs["dis"]
+    return rows
+
+
+def det_tilts(RotDet) -> tuple:
+    """Tilts (degrees) with get_det_R.m's RotDet = Rz(tz) Ry(ty) Rx(tx)."""
+    R = np.asarray(RotDet, np.float64).reshape(3, 3)
+    ty = -math.asin(max(-1.0, min(1.0, R[2, 0])))
+    tx = math.atan2(R[2, 1], R[2, 2])
+    tz = math.atan2(R[1, 0], R[0, 0])
+    return tuple(math.degrees(a) for a in (tx, ty, tz))
+
+
+def fit_grain_COM(ctx, pairs, pos, quat, geo10, iters: int = 20):
+    """Grain centre + orientation from paired spots (replaces fit_grain_COM.m:5-30).
+
+    The reference minimises the mean distance between rounded simulated pixels and the paired
+    centroids with Nelder-Mead over (pos, Euler); here Levenberg-Marquardt fits the continuous
+    landings (grc_fit_grains_lm) from (pos, quat).  Returns (FitOutput = [pos(3) Euler ZXZ deg(3)],
+    RMS residual [pixel], quaternion)."""
+    import torch
+    from . import fit as F
+    m = len(pairs)
+    d = lambda a, t: torch.as_tensor(np.ascontiguousarray(a), dtype=t, device="cuda")
+    spots = F.Spots(d(np.zeros(m, np.int32), torch.int32), d(pairs["iw"], torch.int32), d(pairs["ih"], torch.int32),
+                    d(np.stack([pairs["exp_y"], pairs["exp_z"]], 1).reshape(-1), torch.float64),
+                    d(np.array([0, m], np.int64), torch.int64))
+    q = np.asarray(quat, np.float64)
+    g6 = np.concatenate([F.quat_to_rod(q * np.sign(q[0] if q[0] != 0 else 1.0)), np.asarray(pos, np.float64)])
+    d_g = d(g6, torch.float64)
+    lam = torch.full((1,), 1e-3, dtype=torch.float64, device="cuda")
+    for _ in range(iters):
+        if F.grains_lm(ctx, geo10, d_g, spots, lam, 1) == 0:
+            break
+    g6 = d_g.cpu().numpy()
+    res, _ = F.residual_jacobian(ctx, 0, geo10, d_g, spots)
+    rms = float(torch.sqrt((res ** 2).sum(1).mean()).item()) if m else float("nan")
+    qf = F.rod_to_quat(g6[:3])
+    ang = [a * 180 / math.pi for a in rod2angle_zxz(quat2rod(qf))]
+    ang = [a + 360 if a < 0 else a for a in ang]
+    return np.concatenate([g6[3:6], ang]), rms, qf
+
+
+def forward_comp_pair_spots(U, proj_bin_bw, Spots, pos, rot_angles, S, B, Ahkl, nrhkl, RotDet, thetamax, lambda_min,
+                            lambda_max, Lsam2sou, Lsam2det, minEucDis, dety00, detz00, P0y, P0z, RotAxisOffset,
+                            pixelysize, pixelzsize, dety0, detz0, detysize, detzsize, BeamStopY, BeamStopZ):
+    """forward_comp_pair_spots.m:3-93: (Nr_simu, Nr_intersect, dis_median, SimuSpots, HittedSpots).
+
+    Counts and median come from the scorer, the pairs from grc_pair_spots; SimuSpots (the list of
+    every selected reflection) is not produced (None).  ``minEucDis``, ``dety0`` and ``detz0``
+    must equal the scorer's options."""
+    import torch
+    from . import forward as FW
+    ctx = FW.context()
+    hkl = FW._hkl(Ahkl, nrhkl)
+    param = FW._param(hkl.shape[0], len(rot_angles), Lsam2sou, Lsam2det, P0y, P0z, dety00, detz00, pixelysize,
+                      pixelzsize, detysize, detzsize, BeamStopY, BeamStopZ, thetamax, lambda_min, lambda_max,
+                      RotAxisOffset)
+    ctx.set_geometry(G.flat_rowmajor(S), G.flat_rowmajor(B), G.flat_hkl(hkl), np.asarray(rot_angles, np.float32),
+                     G.flat_rowmajor(RotDet), param)
+    flat = FW._map_for_call(proj_bin_bw)
+    if flat is not None:
+        a = np.asarray(proj_bin_bw)
+        ctx.upload_masks(flat, a.shape[0], a.shape[1], a.shape[2])
+    q = G.u_to_quat(np.asarray(U, np.float64))
+    d = lambda a: torch.as_tensor(np.ascontiguousarray(a, np.float64), device="cuda")
+    out = torch.empty(4, dtype=torch.float32, device="cuda")
+    ctx.score_trials_device(d(np.asarray(pos).reshape(-1)), 1, d(q), 1, None, None, 1, out)
+    o = out.cpu().numpy().astype(np.float64)
+    pairs = pair_spots(ctx, np.asarray(pos).reshape(1, 3), q.reshape(1, 4), Spots, len(rot_angles))
+    return o[0], o[1], o[3], None, hitted_spots_rows(pairs, U, pos, hkl, rot_angles)
+
+
 # ---- the engine -----------------------------------------------------------------------------------
 
 def pos2ind(pos_indexing, tomo_scale, VoxSize, RecVolumePixel, sz, simap_data_flag):
@@ -323,11 +437,13 @@ def GrainMapping_engine_gpu_comp(pos_list, OR, RotDet, Spots, proj_bin_bw, rot_a
 
     ``OR``: dict with 'q' (N x 4); ``DS``: dict of the sample maps (Mask, Completeness,
     GrainId, Rodrigues 3 x dims, EulerZXZ 3 x dims, IPF001 3 x dims, Dismedian, Ninter,
-    VisitFlag, ...), updated copies are returned.  ``Spots`` (experimental centroids) feed
-    the grain-centre fit of :126-161, which is not part of this build: pass None (the
-    reference then takes Spot_L = 20 px, :201-206).  ``minEucDis``, ``dety0`` and ``detz0``
-    must equal the scorer's options (0.5 px threshold, detector centre); ``OutputFolder`` is
-    not written.  Returns (indexing_final (n x 18), pos_list_new (n x 3), DS_out,
+    VisitFlag, ...), updated copies are returned.  ``Spots``: per projection the measured spots
+    (the reference's Spots{i} rows, or [dety, detz, area] rows), or None.  With spots, each new
+    seed's orientation is paired with them (grc_pair_spots), the grain centre and orientation are
+    fitted to the pairs (``fit_grain_COM``, :126-161) and the growth box follows the spot size
+    (Spot_L, :201-206; without spots Spot_L = 20 px as in the reference).  ``minEucDis``,
+    ``dety0`` and ``detz0`` must equal the scorer's options (0.5 px threshold, detector centre);
+    ``OutputFolder`` is not written.  Returns (indexing_final (n x 18), pos_list_new (n x 3), DS_out,
     Nr_indexed_voxel (n)).  Runs on the module context of ``grainrecon_b200.forward``, which
     keeps the distance map resident between this engine and the region grower.
     """
@@ -395,6 +511,34 @@ def GrainMapping_engine_gpu_comp(pos_list, OR, RotDet, Spots, proj_bin_bw, rot_a
                 for r, j in enumerate(sel):
                     spec[j] = (rows[r], cid[r], flag)
 
+    spots_pair = {}
+    geo10 = np.array([Lsam2sou, Lsam2det, dety00, detz00, *det_tilts(RotDet), P0y, P0z, RotAxisOffset], np.float64)
+
+    def _recentre_on_spots(i, pairs, pos_indexing, pi):
+        """:126-161: fit the grain centre to the paired spots and move the seed there when the move
+        exceeds maxD voxels and the new voxel is in the mask and less complete."""
+        fit_out, _, _ = fit_grain_COM(ctx, pairs, pos_indexing, indexing_final[i, 14:18], geo10)
+        if np.sqrt(((fit_out[:3] - indexing_final[i, 1:4]) ** 2).sum()) / VoxSize <= maxD:
+            return pos_indexing, pi
+        pt = pos2ind(fit_out[:3], tomo_scale, VoxSize, RecVolumePixel, sz, simap_data_flag)
+        if not (Comp[tuple(pt - 1)] < indexing_final[i, 6] and Mask[tuple(pt - 1)] == 1):
+            return pos_indexing, pi
+        eul = fit_out[3:6]
+        rod = angle2rod_zxz(*(a * math.pi / 180 for a in eul))
+        indexing_final[i, 1:4] = fit_out[:3]
+        indexing_final[i, 8:11] = eul
+        indexing_final[i, 11:14] = rod
+        indexing_final[i, 14:18] = rod2quat(rod)
+        import torch
+        q = G.u_to_quat(G.euler_to_u(*(a * math.pi / 180 for a in eul)))
+        dd = lambda a: torch.as_tensor(np.ascontiguousarray(a, np.float64), device="cuda")
+        o = torch.empty(4, dtype=torch.float32, device="cuda")
+        ctx.score_trials_device(dd(fit_out[:3]), 1, dd(q), 1, None, None, 1, o)
+        o = o.cpu().numpy().astype(np.float64)
+        indexing_final[i, 4], indexing_final[i, 5], indexing_final[i, 7] = o[0], o[1], o[3]
+        indexing_final[i, 6] = o[1] / o[0] if o[0] > 0 else math.nan
+        return fit_out[:3].copy(), pt
+
     gid_prev = int((DS["GrainId"] > 0).sum())
     for i in range(n):
         stop = False
@@ -410,6 +554,11 @@ def GrainMapping_engine_gpu_comp(pos_list, OR, RotDet, Spots, proj_bin_bw, rot_a
                     indexing_final[i] = row
                     candidate_id[i] = cid
                     fit_all_track[i] = 1 if fa else 0
+                    if Spots is not None:
+                        pairs = pair_spots(ctx, pos_indexing, indexing_final[i, 14:18], Spots, len(rot_angles))
+                        spots_pair[i] = pairs
+                        if len(pairs):
+                            pos_indexing, pi = _recentre_on_spots(i, pairs, pos_indexing, pi)
                 else:
                     rows, _ = indexer.index_local(i + 1, pos_indexing, temp[14:18])
                     indexing_final[i] = rows[0]
@@ -424,8 +573,14 @@ def GrainMapping_engine_gpu_comp(pos_list, OR, RotDet, Spots, proj_bin_bw, rot_a
                     if temp[6] >= Comp[tuple(pi - 1)]:
                         Comp[tuple(pi - 1)] = temp[6]
                         UU = G.quat_to_u(temp[14:18])
+                        pr = spots_pair.get(i)
+                        if pr is not None and len(pr):  # :201-203, bounding half length of the spots
+                            a = pr["area"]
+                            spot_l = math.sqrt((a.mean() + 2 * (a.std(ddof=1) if len(a) > 1 else 0.0)) / math.pi)
+                        else:
+                            spot_l = 20.0
                         J, C_out, D_out, N_out, center, replace_center, idx = FW.grow_indexed_region_cuda(
-                            Comp, Mask, DSo["Dismedian"], DSo["Ninter"], pi, 20, drop_off, maxD, temp[6], UU,
+                            Comp, Mask, DSo["Dismedian"], DSo["Ninter"], pi, spot_l, drop_off, maxD, temp[6], UU,
                             proj_bin_bw, rot_angles, S, B, Ahkl, nrhkl, RotDet, thetamax, lambda_min, lambda_max,
                             Lsam2sou, Lsam2det, dety00, detz00, P0y, P0z, RotAxisOffset, pixelysize, pixelzsize,
                             detysize, detzsize, BeamStopY, BeamStopZ, RecVolumePixel, tomo_scale, VoxSize,
@@ -485,4 +640,5 @@ def GrainMapping_engine_gpu_comp(pos_list, OR, RotDet, Spots, proj_bin_bw, rot_a
                 break
     DSo["SeedIndexing"] = SeedIndexing
     DSo["indexer_stats"] = indexer.stats
+    DSo["spots_pair"] = spots_pair
     return indexing_final, pos_list_new, DSo, Nr_indexed_voxel

@@ -185,6 +185,33 @@ int grc_fit_orientation_nm(grc_ctx *ctx, const double *d_pos, const double *d_x0
                            int32_t *d_evals, int32_t *d_iters, int32_t *d_flag);
 
 /*
+ * Spot pairing of forward_comp_pair_spots.m:60-85 (called by the orientation fit,
+ * fit_OR_constrain_with_local_comp_cuda.m:150-153, and the grain-centre fit): for every trial
+ * (FP64 position, quaternion as grc_score_trials_device) and every selected reflection whose
+ * pixel is a hit, the nearest measured spot centroid of that projection is paired when it lies
+ * closer than min(sqrt(area), 15) pixels (the first spot in list order among equal distances).
+ * d_spots: 3 doubles per spot [dety centroid, detz centroid, area] (Spots{i}(:,9:11)), the spots
+ * of projection i (0-based) at [d_proj_offsets[i], d_proj_offsets[i+1]) (nrot+1 int64 values).
+ * d_pairs receives the pairs in the reference's order (trial, projection, reflection);
+ * *n_pairs the number found.  More than max_pairs is GRC_ECAPACITY with *n_pairs set to the
+ * number needed.  Returns after the work has finished.
+ */
+typedef struct grc_spot_pair {
+    int32_t trial;      /* 0-based trial */
+    int32_t iw;         /* 0-based projection */
+    int32_t ih;         /* 0-based reflection (row of hkl) */
+    int32_t spot;       /* 0-based index into d_spots */
+    double dety, detz;  /* simulated pixel, 1-based (dety, detz of forward_comp.m:58-59) */
+    double exp_y, exp_z;/* the paired centroid */
+    double area;        /* its area [pixel^2] */
+    double energy_kev;  /* 12.398 / lambda of the reflection */
+    double dis;         /* distance-map value at the simulated pixel */
+} grc_spot_pair;
+int grc_pair_spots(grc_ctx *ctx, const double *d_pos, const double *d_q, int64_t n, const double *d_spots,
+                   int64_t n_spots, const int64_t *d_proj_offsets, grc_spot_pair *d_pairs, int64_t max_pairs,
+                   int64_t *n_pairs);
+
+/*
  * Allocation-free seeding scan (no counterpart in the reference: the MEX functions
  * always allocate their gpuArray output).  For callers that must not allocate GPU
  * memory while they score -- a MEX shim inside MATLAB's gpuArray memory manager, a

@@ -265,3 +265,28 @@ def index_seed(scene, pos, q_grid, nr_seed, seed_id=1, fit=True, nr_local=8, gri
     C = r[1] / r[0] if r[0] > 0 else math.nan
     row = np.array([seed_id, *pos, r[0], r[1], C, r[2], *ang, *rod, *quat])
     return row, b0[2] + 1, edges_seen, {"x": np.array(x), "evals": evals}
+
+
+def pair_spots(scene, U, pos, spots, thr=0.5):
+    """forward_comp_pair_spots.m:60-85 for one (U, pos): list of (iw, ih, spot index within the
+    projection, dety, detz, exp_y, exp_z, area, energy_kev, dis) and the edge count of the hits.
+
+    ``spots``: per projection an (m x 3) array [dety centroid, detz centroid, area]."""
+    rec, _ = O.landings(np.asarray(U, np.float64), np.asarray(pos, np.float64), scene.S9, scene.B9, scene.hkl,
+                        scene.dmap, scene.rot, scene.R9, scene.param)
+    out, edges = [], 0
+    for k in range(len(rec["iw"])):
+        if not rec["sel"][k] or not (rec["dis"][k] <= thr):
+            continue
+        edges += int(rec["edge"][k])
+        iw, ih = int(rec["iw"][k]), int(rec["ih"][k])
+        dety = float(np.sign(rec["u"][k]) * np.floor(abs(rec["u"][k]) + 0.5))
+        detz = float(np.sign(rec["v"][k]) * np.floor(abs(rec["v"][k]) + 0.5))
+        sp = np.asarray(spots[iw], np.float64).reshape(-1, 3)
+        if len(sp) == 0:
+            continue
+        d = np.sqrt((sp[:, 0] - dety) ** 2 + (sp[:, 1] - detz) ** 2)
+        j = int(np.argmin(d))
+        if d[j] < min(math.sqrt(sp[j, 2]), 15.0):
+            out.append((iw, ih, j, dety, detz, sp[j, 0], sp[j, 1], sp[j, 2], 12.398 / rec["lam"][k], rec["dis"][k]))
+    return out, edges

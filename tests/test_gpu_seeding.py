@@ -15,6 +15,7 @@ from grainrecon_b200 import seeding as S
 from grainrecon_b200 import synth
 from grainrecon_b200._lib import Context, GrcError
 from oracle import seed_oracle as SO
+from spot_fixtures import measured_spots
 
 pytestmark = pytest.mark.gpu
 
@@ -181,3 +182,32 @@ def test_engine_indexes_the_sample(scene):
     assert len(ids) >= 1 and np.all(nvox[ids.astype(int) - 1] > 0)
     assert out[:, 6].max() > 0.9
     assert DSo["indexer_stats"]["fit_seeds"] >= 1
+
+
+def test_engine_with_measured_spots(scene):
+    """With spots, every accepted seed is paired, its centre fitted to the pairs, and the growth box
+    follows the spot size; the indexed orientations are still the sample's."""
+    s, _, sc, dmap = scene
+    g = s.geom
+    dims = s.grain_id.shape
+    DS = {"Mask": (s.grain_id > 0).astype(np.float64), "Completeness": np.zeros(dims),
+          "GrainId": np.zeros(dims), "Dismedian": np.zeros(dims) + 10, "Ninter": np.zeros(dims),
+          "VisitFlag": np.zeros(dims), "EulerZXZ": np.zeros((3,) + dims)}
+    vox, pos = _voxels(s, 6, 9)
+    q_grid = np.concatenate([s.grain_q, G.cubic_fz_orientations(300, 17)]).astype(np.float32)
+    ts = {"Center": np.array(s.vol.center), "Dimension": np.array(s.vol.dimension)}
+    rvp = np.array([[1, dims[0]], [1, dims[1]], [1, dims[2]]])
+    spots = measured_spots(s, sc, 0.3, 11)
+    out, pos_new, DSo, nvox = S.GrainMapping_engine_gpu_comp(
+        pos, {"q": q_grid}, g.rot_det, spots, dmap.transpose(2, 1, 0), g.rot_angles, s.S, s.B, s.hkl, len(s.hkl),
+        g.theta_max, g.lambda_min, g.lambda_max, g.lss, g.lsd, 0.85, 0.5, 0.5 * g.pxy, g.dety00, g.detz00, g.p0y,
+        g.p0z, g.rot_axis_offset, g.pxy, g.pxz, g.detysize / 2 + 0.5, g.detzsize / 2 + 0.5, g.detysize, g.detzsize,
+        g.beamstop_y, g.beamstop_z, 0.05, 3, DS, ts, s.vol.vox_size, rvp, 1, s.vol.simap, 10, 3, batch=4)
+    pairs = DSo["spots_pair"]
+    assert len(pairs) >= 1 and all(len(p) > 20 for p in pairs.values())
+    got = DSo["GrainId"] > 0
+    assert got[s.grain_id > 0].mean() > 0.5
+    Ug = [G.quat_to_u(q) for q in s.grain_q]
+    for k in range(int(got.sum())):
+        e = DSo["EulerZXZ"][:, got][:, k]
+        assert min(_misori_deg(U, G.euler_to_u(*np.radians(e))) for U in Ug) < 1.0
