@@ -676,7 +676,8 @@ __global__ void __launch_bounds__(kThreads, 2) mark_kernel(Geo g, ScoreBufs b, W
 // shared memory (counters, a 256-bin histogram of the 8-bit saturated codes, S*U*B)
 // and every CTA walks the projections in windows of kWin at the same pace, so the
 // map pixels being read belong to a few projections at a time and stay in L2.
-constexpr int kSlots = 64;
+constexpr int kSlots = 96;      // most trials a CTA holds in one round
+constexpr int kSlotsBulk = 64;  // tile of multi-round work and of explicit voxel lists
 constexpr int kWin = 8;
 constexpr int kHist8Words = 128;  // 256 u16 bins per slot, two per word
 
@@ -689,18 +690,19 @@ __device__ __forceinline__ int64_t voxel_of(const Work &w, int64_t t) {
 struct SweepSmem {
     RowF *rows;       // [rows_cap * kWin] rows of the current window, indexed vloc * kWin + wl
     float4 *hk;       // [nhkl] h as float
-    uint32_t *hist;   // [kSlots * kHist8Words]
-    uint32_t *cnt;    // [kSlots] Nr_simu | Nr_intersect << 16
-    float *subf;      // [kSlots * 12]
-    double *subd;     // [kSlots * 9]
-    int *vloc;        // [kSlots]
-    int64_t *vglob;   // [kSlots]
-    int64_t *vlist;   // [kSlots]
+    uint32_t *hist;   // [slots * kHist8Words]
+    uint32_t *cnt;    // [slots] Nr_simu | Nr_intersect << 16
+    float *subf;      // [slots * 12]
+    double *subd;     // [slots * 9]
+    int *vloc;        // [slots]
+    int64_t *vglob;   // [slots]
+    int64_t *vlist;   // [slots]
     uint32_t *queue;  // [kWarps * kQueueCap]
     uint32_t *fqueue; // [kWarps * kFallbackCap]
 };
 
-__host__ __device__ inline size_t sweep_smem_layout(int nhkl, int rows_cap, size_t *offs) {
+// Shared-memory layout of one CTA holding `slots` trials and rows of `rows_cap` voxels.
+__host__ __device__ inline size_t sweep_smem_layout(int nhkl, int rows_cap, int slots, size_t *offs) {
     size_t o = 0, i = 0;
     auto put = [&](size_t bytes) {
         o = (o + 15) & ~size_t(15);
@@ -709,21 +711,21 @@ __host__ __device__ inline size_t sweep_smem_layout(int nhkl, int rows_cap, size
     };
     put(sizeof(RowF) * rows_cap * kWin);
     put(sizeof(float4) * nhkl);
-    put(sizeof(uint32_t) * kSlots * kHist8Words);
-    put(sizeof(uint32_t) * kSlots);
-    put(sizeof(float) * kSlots * 12);
-    put(sizeof(double) * kSlots * 9);
-    put(sizeof(int) * kSlots);
-    put(sizeof(int64_t) * kSlots);
-    put(sizeof(int64_t) * kSlots);
+    put(sizeof(uint32_t) * slots * kHist8Words);
+    put(sizeof(uint32_t) * slots);
+    put(sizeof(float) * slots * 12);
+    put(sizeof(double) * slots * 9);
+    put(sizeof(int) * slots);
+    put(sizeof(int64_t) * slots);
+    put(sizeof(int64_t) * slots);
     put(sizeof(uint32_t) * kWarps * kQueueCap);
     put(sizeof(uint32_t) * kWarps * kFallbackCap);
     return (o + 15) & ~size_t(15);
 }
 
-__device__ __forceinline__ SweepSmem sweep_carve(unsigned char *base, int nhkl, int rows_cap) {
+__device__ __forceinline__ SweepSmem sweep_carve(unsigned char *base, int nhkl, int rows_cap, int slots) {
     size_t offs[11];
-    sweep_smem_layout(nhkl, rows_cap, offs);
+    sweep_smem_layout(nhkl, rows_cap, slots, offs);
     SweepSmem m;
     m.rows = (RowF *)(base + offs[0]);
     m.hk = (float4 *)(base + offs[1]);
@@ -765,7 +767,7 @@ __global__ void __launch_bounds__(kThreads, GRC_SWEEP_BLOCKS) sweep_kernel(Geo g
     if (cta_base >= n_trials) return;
     const int nslot = (int)min((int64_t)slots, n_trials - cta_base);
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    const SweepSmem sm = sweep_carve(smem_raw, g.nhkl, rows_cap);
+    const SweepSmem sm = sweep_carve(smem_raw, g.nhkl, rows_cap, slots);
     __shared__ int s_nv, s_next;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const unsigned lt = (1u << lane) - 1u;
@@ -787,7 +789,7 @@ __global__ void __launch_bounds__(kThreads, GRC_SWEEP_BLOCKS) sweep_kernel(Geo g
         sm.vglob[tid] = v;
         sm.cnt[tid] = 0;
     }
-    for (int i = tid; i < kSlots * kHist8Words; i += kThreads) sm.hist[i] = 0;
+    for (int i = tid; i < slots * kHist8Words; i += kThreads) sm.hist[i] = 0;
     for (int i = tid; i < g.nhkl; i += kThreads)
         sm.hk[i] = make_float4((float)b.hkl[3 * i], (float)b.hkl[3 * i + 1], (float)b.hkl[3 * i + 2], 0.f);
     __syncthreads();
@@ -1121,28 +1123,53 @@ cudaError_t launch_score_t(const Geo &g, const ScoreBufs &b, const Work &w, int 
 template <int HPL, typename CodeT>
 cudaError_t launch_sweep_t(const Geo &g, const ScoreBufs &b, const Work &w, int64_t n_trials, int num_sms,
                            cudaStream_t s, cudaEvent_t ev0, cudaEvent_t ev1, int *launches, int max_slots) {
-    // distinct voxels one CTA can meet among its kSlots consecutive trials
-    int rows_cap = kSlots;
-    if (!w.trial_voxel && !w.diag && w.n_or > 0) rows_cap = (int)(w.n_or >= kSlots ? 2 : kSlots / w.n_or + 2);
-    if (rows_cap > kSlots) rows_cap = kSlots;
+    // The tile is kSlotsBulk trials per CTA.  An implicit seeding list (a few voxels per CTA) may
+    // take up to kSlots when that fits the whole call into one round -- a one-seed scan of 32,768
+    // orientations then runs as one round of 74 trials per CTA instead of two of 37.  Explicit
+    // voxel lists keep one row set per trial in shared memory and stay at kSlotsBulk unless the
+    // caller asks for another tile.  Shared memory is sized by the tile actually used.
+    const bool explicit_voxels = w.trial_voxel || w.diag || w.n_or <= 0;
+    const bool caller_tile = max_slots >= 1 && max_slots <= kSlots;
+    if (!caller_tile) max_slots = kSlotsBulk;
+    auto rows_for = [&](int sl) {  // distinct voxels one CTA can meet among sl consecutive trials
+        int rc = explicit_voxels ? sl : (int)(w.n_or >= sl ? 2 : sl / w.n_or + 2);
+        return rc > sl ? sl : rc;
+    };
     size_t offs[11];
-    const size_t smem = sweep_smem_layout(g.nhkl, rows_cap, offs);
+    const size_t smem_max = sweep_smem_layout(g.nhkl, rows_for(max_slots), max_slots, offs);
     const size_t smem_r = refine_smem_bytes(g.nrot, g.nhkl);
     int per_sm = 0;
-    cudaError_t e = cudaFuncSetAttribute(sweep_kernel<HPL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = cudaFuncSetAttribute(sweep_kernel<HPL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem_max);
     if (e != cudaSuccess) return e;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sweep_kernel<HPL>, kThreads, smem);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sweep_kernel<HPL>, kThreads, smem_max);
     if (e != cudaSuccess) return e;
     if (per_sm < 1) return cudaErrorInvalidConfiguration;
     int grid_r = 0;
     e = prep_launch(refine_list_kernel<HPL, CodeT>, smem_r, num_sms, (int64_t)num_sms * 4, &grid_r);
     if (e != cudaSuccess) return e;
     const int64_t grid = (int64_t)per_sm * num_sms;
+    if (!caller_tile && !explicit_voxels && n_trials > grid * max_slots && n_trials <= grid * kSlots) {
+        // one round of up to kSlots trials per CTA, if the larger tile keeps the same CTAs per SM
+        int per_sm1 = 0;
+        const size_t smem1 = sweep_smem_layout(g.nhkl, rows_for(kSlots), kSlots, offs);
+        if (cudaFuncSetAttribute(sweep_kernel<HPL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem1) ==
+                cudaSuccess &&
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm1, sweep_kernel<HPL>, kThreads, smem1) ==
+                cudaSuccess &&
+            per_sm1 == per_sm) {
+            max_slots = kSlots;
+        } else {
+            e = cudaFuncSetAttribute(sweep_kernel<HPL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_max);
+            if (e != cudaSuccess) return e;
+        }
+    }
     // rounds of equal size: slots per CTA chosen so the last round is not a sliver
-    if (max_slots < 1 || max_slots > kSlots) max_slots = kSlots;
     const int64_t rounds = (n_trials + grid * max_slots - 1) / (grid * max_slots);
     int slots = (int)((n_trials + rounds * grid - 1) / (rounds * grid));
     if (slots < 1) slots = 1;
+    const int rows_cap = rows_for(slots);
+    const size_t smem = sweep_smem_layout(g.nhkl, rows_cap, slots, offs);
     const int64_t per_round = grid * slots;
     e = cudaMemsetAsync(b.work_counter, 0, 8 * sizeof(int), s);
     if (e != cudaSuccess) return e;
@@ -1287,7 +1314,7 @@ cudaError_t launch_simulate_work(const Geo &g, const ScoreBufs &b, const Work &w
 int64_t sweep_round_trials(const Geo &g, int num_sms) {
     // 16-bit per-slot counters and histogram bins; hit codes must stay below the saturation code
     if (g.n_hit >= 255u || g.nhkl > 128 || (int64_t)g.nrot * g.nhkl > 65535) return 0;
-    return (int64_t)num_sms * GRC_SWEEP_BLOCKS * kSlots;
+    return (int64_t)num_sms * GRC_SWEEP_BLOCKS * kSlotsBulk;
 }
 
 cudaError_t launch_sweep(const Geo &g, const ScoreBufs &b, const Work &w, int64_t n_trials, int num_sms,
