@@ -83,3 +83,35 @@ def test_pos2ind_inverts_voxel_positions():
         pos = vol.pos_of_index(idx)
         got = S.pos2ind(pos, ts, vol.vox_size, rvp, (20, 20, 20), 1)
         assert np.all(np.abs(got - idx) <= 1) and np.all((got >= 1) & (got <= 20))
+
+
+def test_seed_positions_keep_their_distance():
+    from grainrecon_b200 import mapping as M
+    dim = 40
+    ax = np.arange(1, dim + 1)
+    X, Y, Z = np.meshgrid(ax, ax, ax, indexing="ij")
+    inside = (X - 20.5) ** 2 + (Y - 20.5) ** 2 <= 400
+    allv = np.argwhere(inside) + 1
+    ts = {"Center": np.zeros(3), "Dimension": np.array([dim] * 3)}
+    for it in (1, 6, 11):
+        pos = M.generate_seeding_indexing_pos(it, allv, ts, 0.005, 0, np.random.default_rng(it))
+        vol = M.SEED_VOL_MIN[it - 1]
+        dmin = max(0.25 * (3 * vol / (4 * np.pi)) ** (1 / 3) * 2, 3.0)
+        idx = pos / 0.005 + dim / 2
+        assert len(pos) >= 1 and len(pos) <= max(1, round(len(allv) / vol), round(len(allv) / 8))
+        assert np.allclose(idx, np.round(idx))
+        d = np.sqrt(((idx[:, None] - idx[None]) ** 2).sum(-1))
+        assert len(pos) == 1 or d[np.triu_indices(len(pos), 1)].min() > dmin
+        assert {tuple(r) for r in np.round(idx).astype(int)} <= {tuple(r) for r in allv}
+    pos = M.generate_seeding_indexing_pos(1, allv, ts, 0.005, 1, np.random.default_rng(0))
+    assert np.all(-pos[:, 0] / 0.005 + dim / 2 >= 1)  # the simap frame flips x and y
+
+
+def test_init_ds_marks_the_sample():
+    from grainrecon_b200 import mapping as M
+    m = np.zeros((5, 6, 7))
+    m[1:4, 2:5, 3:6] = 1
+    DS = M.init_DS(m)
+    assert DS["VisitFlag"][m > 0].min() == 0 and DS["VisitFlag"][m == 0].max() == -1
+    assert DS["Dismedian"][m > 0].min() == 20 and DS["Dismedian"][m == 0].max() == 10
+    assert DS["EulerZXZ"].shape == (3, 5, 6, 7)
