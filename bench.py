@@ -268,10 +268,22 @@ def run_ours(args):
     peak = peak or 6650.0
     kernel = "sweep_kernel" if path == 2 else "score_kernel"
     traffic = None
+    issue = None
+    clocks = clk.summary()
     try:
-        # DRAM bytes per selected reflection measured by ncu on the same kernel (profiles/)
+        # DRAM bytes per selected reflection and warp instructions per trial measured by ncu on
+        # the same kernel (profiles/)
         prof = json.load(open(os.path.join(ROOT, "profiles", f"{kernel}_dram.json")))
         traffic = float(np.mean(lookups)) * prof["dram_bytes_per_lookup"]
+        if "warp_instructions_per_trial" in prof:
+            # issue roofline: one warp instruction per scheduler per clock, 4 schedulers per SM
+            sm_mhz = clocks.get("sm_mhz") or 1965.0
+            nsm = torch.cuda.get_device_properties(local).multi_processor_count
+            peak_issue = nsm * 4 * sm_mhz * 1e6
+            ach_issue = value / world * prof["warp_instructions_per_trial"]
+            issue = {"achieved": ach_issue, "peak": peak_issue, "unit": "warp instructions/s",
+                     "frac": ach_issue / peak_issue, "instructions_per_trial": prof["warp_instructions_per_trial"],
+                     "peak_source": f"{nsm} SMs x 4 schedulers x {sm_mhz:.0f} MHz (sampled under load)"}
     except (OSError, KeyError, ValueError):
         pass
     cpu = None
@@ -282,7 +294,7 @@ def run_ours(args):
         line = {"metric": METRIC, "value": value, "unit": "trials/s", "n_gpus": world, "steps": K, "warmup": W,
                 "ms_per_step": max_ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
                 "dtype": "f64", "data": "synthetic", "config": workload_desc(s, S),
-                "clocks": clk.summary(),
+                "clocks": clocks,
                 "e2e": {"value": e2e_val, "unit": "trials/s",
                         "h2d_bytes_per_step": S * (12 + N_ORIENT * 16), "d2h_bytes_per_step": S * N_ORIENT * 16,
                         "note": f"{e2e_steps} steps of {S} grc_forward_comp calls (one per seed voxel)"},
@@ -292,7 +304,8 @@ def run_ours(args):
                              "kernel": kernel, "peak_source": peak_note,
                              "algorithmic_bytes": "32 B (one sector) per selected reflection's map lookup",
                              "lookups_per_launch": float(np.mean(lookups)),
-                             "score_ms_per_launch": float(np.mean(score_ms))},
+                             "score_ms_per_launch": float(np.mean(score_ms)),
+                             "issue": issue},
                 "cpu_baseline": cpu, "setup_s": setup_s}
         print(json.dumps(line), flush=True)
     ctx.close()
