@@ -233,3 +233,107 @@ def grow_unindexed_compete_comp_cuda(DS_in, wait_revising_voxels, id_neigb_all, 
         DS_out["Ninter"][ix] = out[i, 6]
         DS_out["VisitFlag"][ix] = 0.5
     return DS_out, out
+
+
+_NEIGB = np.array([[1, 1, 0], [1, -1, 0], [1, 0, 1], [1, 0, -1], [1, 0, 0], [0, 1, 0], [0, -1, 0], [0, 1, 1],
+                   [0, 0, 1], [0, -1, 1], [0, 1, -1], [0, 0, -1], [0, -1, -1], [-1, 1, 0], [-1, -1, 0], [-1, 0, 1],
+                   [-1, 0, -1], [-1, 0, 0]], np.int64)  # grow_indexed_region.m:26-29, 18 neighbours
+
+
+def best_first_growth(score, I, Imask, DisMedian, Ninter, pos_indices, drop_off, maxD, indexed_comp, maxDmedian):
+    """The region walk of grow_indexed_region.m:6-137 with a pluggable scorer.
+
+    ``score(vox)`` maps (k x 3) 1-based voxel indices to rows [Nr_simu, Nr_intersect, dis_median].
+    From the current voxel every unvisited in-mask neighbour is scored (one batch per step; the
+    scores do not depend on the region) and kept when it beats the map -- ``C > I`` with
+    ``dis_median <= min(DisMedian, maxDmedian)``, or ``|C - I| <= 0.01`` with more
+    intersections than ``Ninter`` (:50-52).  The walk then moves to the best kept voxel while its
+    completeness stays above ``seed_comp * (1 - drop_off)``.  Returns (J, Completeness_out,
+    DisMedian_out, Ninter_out, center, replace_center, indexed_indices)."""
+    I = np.array(I, dtype=np.float64, copy=True)
+    x, y, z = (int(p) for p in pos_indices)
+    I[x - 1, y - 1, z - 1] = indexed_comp
+    J = np.zeros(I.shape, np.int8)
+    C_out = I.copy()
+    D_out = np.array(DisMedian, dtype=np.float64, copy=True)
+    N_out = np.array(Ninter, dtype=np.float64, copy=True)
+    dims = np.array(I.shape)
+    seed_comp = I[x - 1, y - 1, z - 1]
+    csum = seed_comp
+    cpos = seed_comp * np.array([x, y, z], np.float64)
+    center0 = cpos / csum
+    n_mask = int((np.asarray(Imask) > 0).sum())
+    neg = []  # [x y z C dis_median Nr_intersect]
+    reg_size = 0
+    Imask = np.asarray(Imask)
+    while True:
+        nb = np.array([x, y, z]) + _NEIGB
+        ins = np.all((nb >= 1) & (nb <= dims), axis=1)
+        nb = nb[ins]
+        keep = (J[tuple((nb - 1).T)] == 0) & (Imask[tuple((nb - 1).T)] > 0)
+        nb = nb[keep]
+        if len(nb):
+            r = np.asarray(score(nb), np.float64).reshape(-1, 3)
+            with np.errstate(invalid="ignore", divide="ignore"):
+                c = r[:, 1] / r[:, 0]
+            ix = tuple((nb - 1).T)
+            i0, d0, n0 = I[ix], np.asarray(DisMedian, np.float64)[ix], np.asarray(Ninter, np.float64)[ix]
+            ok = ((c > i0) & (r[:, 2] <= np.minimum(d0, maxDmedian))) | ((np.abs(c - i0) <= 0.01) & (r[:, 1] > n0))
+            for k in np.nonzero(ok)[0]:
+                neg.append([*nb[k], c[k], r[k, 2], r[k, 1]])
+                J[tuple(nb[k] - 1)] = 1
+        J[x - 1, y - 1, z - 1] = 2
+        if not neg:
+            break
+        dist = np.array([e[3] for e in neg]) / seed_comp
+        index = int(np.nanargmax(dist))
+        reg_size += 1
+        if dist[index] > 1 - drop_off and reg_size < n_mask - 1:
+            e = neg[index]
+            csum += e[3]
+            cpos += e[3] * np.array(e[:3], np.float64)
+            xi, yi, zi = (int(v) - 1 for v in e[:3])
+            C_out[xi, yi, zi], D_out[xi, yi, zi], N_out[xi, yi, zi] = e[3], e[4], e[5]
+            x, y, z = xi + 1, yi + 1, zi + 1
+            neg[index] = neg[-1]
+            neg.pop()
+        else:
+            break
+    Jb = J > 1
+    idx = np.argwhere(Jb.transpose(2, 1, 0))[:, ::-1] + 1
+    center1 = cpos / csum
+    if np.sqrt(((center1 - center0) ** 2).sum()) > max(maxD, maxD / 10000 * len(idx)):
+        center, replace_center = np.round(center1), 1
+    else:
+        center, replace_center = center0, 0
+    return Jb, C_out, D_out, N_out, center, replace_center, idx
+
+
+def grow_indexed_region(I, Imask, DisMedian, Ninter, pos_indices, drop_off, maxD, indexed_comp, UU, proj_bin_bw,
+                        rot_angles, S, B, Ahkl, nrhkl, RotDet, thetamax, lambda_min, lambda_max, Lsam2sou, Lsam2det,
+                        minEucDis, dety00, detz00, P0y, P0z, RotAxisOffset, pixelysize, pixelzsize, dety0, detz0,
+                        detysize, detzsize, BeamStopY, BeamStopZ, RecVolumePixel, tomo_scale, VoxSize,
+                        simap_data_flag, maxDmedian):
+    """grow_indexed_region.m:1-145: best-first growth from the seed voxel, each step's neighbours
+    scored on the GPU in one call.  ``minEucDis``, ``dety0`` and ``detz0`` must equal the scorer's
+    options (0.5 px threshold, detector centre)."""
+    hkl = _hkl(Ahkl, nrhkl)
+    param = _param(hkl.shape[0], len(rot_angles), Lsam2sou, Lsam2det, P0y, P0z, dety00, detz00, pixelysize,
+                   pixelzsize, detysize, detzsize, BeamStopY, BeamStopZ, thetamax, lambda_min, lambda_max,
+                   RotAxisOffset)
+    param1 = np.array([*np.asarray(RecVolumePixel)[:, 0], simap_data_flag, VoxSize, *tomo_scale["Center"],
+                       *tomo_scale["Dimension"], 0, 0, maxDmedian], dtype=np.float32)
+    ctx = context()
+    args = (G.flat_rowmajor(UU), G.flat_rowmajor(S), G.flat_rowmajor(B), G.flat_hkl(hkl))
+    first = [_map_for_call(proj_bin_bw)]
+
+    def score(vox):
+        rows = np.zeros((len(vox), 6), np.float32)
+        rows[:, :3] = vox
+        out = ctx.grow_indexed_region(rows, *args, first[0], np.asarray(rot_angles, np.float32),
+                                      G.flat_rowmajor(RotDet), param, param1).reshape(-1, 7)
+        first[0] = None  # the map stays resident after the first call
+        return out[:, 3:6]
+
+    return best_first_growth(score, I, Imask, DisMedian, Ninter, pos_indices, drop_off, maxD, indexed_comp,
+                             maxDmedian)

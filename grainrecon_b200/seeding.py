@@ -440,8 +440,9 @@ def GrainMapping_engine_gpu_comp(pos_list, OR, RotDet, Spots, proj_bin_bw, rot_a
     VisitFlag, ...), updated copies are returned.  ``Spots``: per projection the measured spots
     (the reference's Spots{i} rows, or [dety, detz, area] rows), or None.  With spots, each new
     seed's orientation is paired with them (grc_pair_spots), the grain centre and orientation are
-    fitted to the pairs (``fit_grain_COM``, :126-161) and the growth box follows the spot size
-    (Spot_L, :201-206; without spots Spot_L = 20 px as in the reference).  ``minEucDis``,
+    fitted to the pairs (``fit_grain_COM``, :126-161) and the growth follows the spot size
+    (Spot_L, :201-231: best-first growth for spots of at most 2 px, else growth within a
+    bounding volume; without spots Spot_L = 20 px as in the reference).  ``minEucDis``,
     ``dety0`` and ``detz0`` must equal the scorer's options (0.5 px threshold, detector centre);
     ``OutputFolder`` is not written.  Returns (indexing_final (n x 18), pos_list_new (n x 3), DS_out,
     Nr_indexed_voxel (n)).  Runs on the module context of ``grainrecon_b200.forward``, which
@@ -579,12 +580,20 @@ def GrainMapping_engine_gpu_comp(pos_list, OR, RotDet, Spots, proj_bin_bw, rot_a
                             spot_l = math.sqrt((a.mean() + 2 * (a.std(ddof=1) if len(a) > 1 else 0.0)) / math.pi)
                         else:
                             spot_l = 20.0
-                        J, C_out, D_out, N_out, center, replace_center, idx = FW.grow_indexed_region_cuda(
-                            Comp, Mask, DSo["Dismedian"], DSo["Ninter"], pi, spot_l, drop_off, maxD, temp[6], UU,
-                            proj_bin_bw, rot_angles, S, B, Ahkl, nrhkl, RotDet, thetamax, lambda_min, lambda_max,
-                            Lsam2sou, Lsam2det, dety00, detz00, P0y, P0z, RotAxisOffset, pixelysize, pixelzsize,
-                            detysize, detzsize, BeamStopY, BeamStopZ, RecVolumePixel, tomo_scale, VoxSize,
-                            simap_data_flag, maxDmedian)
+                        if spot_l <= 2:  # :207-214, small spots: best-first growth voxel by voxel
+                            J, C_out, D_out, N_out, center, replace_center, idx = FW.grow_indexed_region(
+                                Comp, Mask, DSo["Dismedian"], DSo["Ninter"], pi, drop_off, maxD, temp[6], UU,
+                                proj_bin_bw, rot_angles, S, B, Ahkl, nrhkl, RotDet, thetamax, lambda_min,
+                                lambda_max, Lsam2sou, Lsam2det, minEucDis, dety00, detz00, P0y, P0z, RotAxisOffset,
+                                pixelysize, pixelzsize, dety0, detz0, detysize, detzsize, BeamStopY, BeamStopZ,
+                                RecVolumePixel, tomo_scale, VoxSize, simap_data_flag, maxDmedian)
+                        else:  # growth within a bounding volume around the seed
+                            J, C_out, D_out, N_out, center, replace_center, idx = FW.grow_indexed_region_cuda(
+                                Comp, Mask, DSo["Dismedian"], DSo["Ninter"], pi, spot_l, drop_off, maxD, temp[6],
+                                UU, proj_bin_bw, rot_angles, S, B, Ahkl, nrhkl, RotDet, thetamax, lambda_min,
+                                lambda_max, Lsam2sou, Lsam2det, dety00, detz00, P0y, P0z, RotAxisOffset, pixelysize,
+                                pixelzsize, detysize, detzsize, BeamStopY, BeamStopZ, RecVolumePixel, tomo_scale,
+                                VoxSize, simap_data_flag, maxDmedian)
                         ix = tuple((idx - 1).T)
                         Nr_indexed_voxel[i] = len(idx)
                         gid = i + FirstGrainID

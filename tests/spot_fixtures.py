@@ -5,7 +5,7 @@ from grainrecon_b200 import geometry as G
 from oracle import oracle as O
 
 
-def measured_spots(s, sc, noise_px, seed, spurious=20, exact=False, grains=None):
+def measured_spots(s, sc, noise_px, seed, spurious=20, exact=False, grains=None, area=(4, 40)):
     rng = np.random.default_rng(seed)
     g = s.geom
     idx = s.voxel_indices()
@@ -20,7 +20,7 @@ def measured_spots(s, sc, noise_px, seed, spurious=20, exact=False, grains=None)
             u, v = rec["u"][j], rec["v"][j]
             if not exact:
                 u, v = u + rng.normal(0, noise_px), v + rng.normal(0, noise_px)
-            per[rec["iw"][j]].append((u, v, rng.uniform(4, 40)))
+            per[rec["iw"][j]].append((u, v, rng.uniform(*area)))
     for iw in range(g.nrot):
         for _ in range(spurious):
             per[iw].append((rng.uniform(1, g.detysize), rng.uniform(1, g.detzsize), 10.0))

@@ -211,3 +211,34 @@ def test_engine_with_measured_spots(scene):
     for k in range(int(got.sum())):
         e = DSo["EulerZXZ"][:, got][:, k]
         assert min(_misori_deg(U, G.euler_to_u(*np.radians(e))) for U in Ug) < 1.0
+
+
+def test_engine_small_spots_take_the_best_first_growth(scene):
+    """Spots of 1-3 px^2 give Spot_L <= 2 px, so every accepted seed grows voxel by voxel
+    (grow_indexed_region) instead of within a bounding volume."""
+    s, _, sc, dmap = scene
+    g = s.geom
+    dims = s.grain_id.shape
+    DS = {"Mask": (s.grain_id > 0).astype(np.float64), "Completeness": np.zeros(dims),
+          "GrainId": np.zeros(dims), "Dismedian": np.zeros(dims) + 10, "Ninter": np.zeros(dims),
+          "VisitFlag": np.zeros(dims), "EulerZXZ": np.zeros((3,) + dims)}
+    vox, pos = _voxels(s, 4, 13)
+    q_grid = np.concatenate([s.grain_q, G.cubic_fz_orientations(300, 17)]).astype(np.float32)
+    ts = {"Center": np.array(s.vol.center), "Dimension": np.array(s.vol.dimension)}
+    rvp = np.array([[1, dims[0]], [1, dims[1]], [1, dims[2]]])
+    spots = measured_spots(s, sc, 0.2, 12, area=(1, 3))
+    out, pos_new, DSo, nvox = S.GrainMapping_engine_gpu_comp(
+        pos, {"q": q_grid}, g.rot_det, spots, dmap.transpose(2, 1, 0), g.rot_angles, s.S, s.B, s.hkl, len(s.hkl),
+        g.theta_max, g.lambda_min, g.lambda_max, g.lss, g.lsd, 0.85, 0.5, 0.5 * g.pxy, g.dety00, g.detz00, g.p0y,
+        g.p0z, g.rot_axis_offset, g.pxy, g.pxz, g.detysize / 2 + 0.5, g.detzsize / 2 + 0.5, g.detysize, g.detzsize,
+        g.beamstop_y, g.beamstop_z, 0.05, 3, DS, ts, s.vol.vox_size, rvp, 1, s.vol.simap, 10, 3, batch=4)
+    pairs = DSo["spots_pair"]
+    assert pairs and all(np.sqrt((p["area"].mean() + 2 * p["area"].std(ddof=1)) / np.pi) <= 2 for p in pairs.values())
+    got = DSo["GrainId"] > 0
+    assert got.sum() > 5 and not got[s.grain_id == 0].any()
+    for gid in np.unique(DSo["GrainId"][got]):
+        region = DSo["GrainId"] == gid
+        # best-first growth walks through face/edge neighbours: one connected region per seed
+        from scipy import ndimage
+        lab, n = ndimage.label(region, structure=ndimage.generate_binary_structure(3, 2))
+        assert n == 1

@@ -143,3 +143,53 @@ def test_compete(scene):
     np.testing.assert_allclose(out[clean, 7], ref[clean, 7], rtol=1e-6)
     for i, v in enumerate(vox):
         assert DS_out["GrainId"][tuple(v - 1)] == out[i, 4] and DS_out["VisitFlag"][tuple(v - 1)] == 0.5
+
+
+def test_best_first_growth_matches_oracle_walk(scene):
+    """grow_indexed_region (the CPU-path growth) on the GPU scorer against the same walk scored by
+    the oracle: identical regions, maps and centre unless the oracle met an edge reflection."""
+    s, dmap, pbb = scene
+    g = s.geom
+    dims = s.grain_id.shape
+    ts, rvp = _tomo(s)
+    S9, B9, hkl, rot, R9, p = s.mex_arrays()
+    idx = s.voxel_indices()
+    k = 3
+    U = G.quat_to_u(s.grain_q[k - 1])
+    seed = idx[s.grain_id[tuple((idx - 1).T)] == k][5]
+    I = np.zeros(dims)
+    Imask = (s.grain_id > 0).astype(np.float64)
+    Dm = np.zeros(dims) + 20
+    Ni = np.zeros(dims)
+    geo = _geo_args(s)
+    gpu = FW.grow_indexed_region(
+        I, Imask, Dm, Ni, seed, 0.05, 3, 0.95, U, pbb, g.rot_angles, s.S, s.B, s.hkl, len(s.hkl), g.rot_det,
+        geo["thetamax"], geo["lambda_min"], geo["lambda_max"], g.lss, g.lsd, 0.5 * g.pxy, g.dety00, g.detz00, g.p0y,
+        g.p0z, g.rot_axis_offset, g.pxy, g.pxz, g.detysize / 2 + 0.5, g.detzsize / 2 + 0.5, g.detysize, g.detzsize,
+        g.beamstop_y, g.beamstop_z, rvp, ts, s.vol.vox_size, s.vol.simap, 10)
+    p1 = np.array([*rvp[:, 0], s.vol.simap, s.vol.vox_size, *s.vol.center, *s.vol.dimension, 0, 0, 10], np.float32)
+    edges_seen = [0]
+
+    def oracle_score(vox):
+        rows6 = np.zeros((len(vox), 6), np.float32)
+        rows6[:, :3] = vox
+        out, edges = O.grow(rows6, G.flat_rowmajor(U), S9, B9, hkl, dmap, rot, R9, p, p1)
+        edges_seen[0] += int(edges.sum())
+        return out.reshape(-1, 7)[:, 3:6]
+
+    ref = FW.best_first_growth(oracle_score, I, Imask, Dm, Ni, seed, 0.05, 3, 0.95, 10)
+    J, C, D, N, center, rc, grown = gpu
+    assert J[tuple(seed - 1)] and len(grown) > 5
+    if edges_seen[0] == 0:
+        np.testing.assert_array_equal(J, ref[0])
+        np.testing.assert_array_equal(grown, ref[6])
+        np.testing.assert_array_equal(center, ref[4])
+        assert rc == ref[5]
+        m = J & (C > 0)
+        np.testing.assert_array_equal(C[m], ref[1][m])
+        np.testing.assert_array_equal(N[m], ref[3][m])
+        np.testing.assert_allclose(D[m], ref[2][m], rtol=1e-6)
+    else:  # the walks may part at an edge reflection, but only there
+        assert ref[0][tuple(seed - 1)]
+        jac = (J & ref[0]).sum() / (J | ref[0]).sum()
+        assert jac > 0.9, (jac, edges_seen[0])
