@@ -48,8 +48,11 @@ def _map_for_call(proj_bin_bw):
     """The flat map when it must be (re)uploaded, else None (resident map is reused)."""
     global _map_key
     a = np.asarray(proj_bin_bw)
-    sample = a.reshape(-1)[:: max(1, a.size // 4096)]
-    key = (id(proj_bin_bw), a.shape, a.dtype.str, hash(np.asarray(sample, np.float32).tobytes()))
+    # every (size/4096)-th element in C order, gathered by index: reshape(-1) of a transposed
+    # view would copy the whole map on every call
+    at = np.arange(0, a.size, max(1, a.size // 4096))
+    sample = a[np.unravel_index(at, a.shape)] if a.ndim > 1 else a.reshape(-1)[at]
+    key =(id(proj_bin_bw), a.shape, a.dtype.str, hash(np.asarray(sample, np.float32).tobytes()))
     if key == _map_key:
         return None
     _map_key = key
@@ -149,19 +152,18 @@ def grow_indexed_region_cuda(I, Imask, DisMedian, Ninter, pos_indices, Spot_L, d
                                         np.asarray(rot_angles, np.float32), G.flat_rowmajor(RotDet), param,
                                         param1).reshape(-1, 7)
     acc = out[out[:, 6] == 1]                                                        # :117
-    for r in acc:                                                                    # :118-128
-        xi, yi, zi = int(r[0]) - 1, int(r[1]) - 1, int(r[2]) - 1
-        J[xi, yi, zi] = 2
-        Completeness_out[xi, yi, zi] = r[4] / r[3]
-        DisMedian_out[xi, yi, zi] = r[5]
-        Ninter_out[xi, yi, zi] = r[4]
+    ix = tuple(acc[:, :3].astype(np.int64).T - 1)                                    # :118-128
+    J[ix] = 2
+    Completeness_out[ix] = acc[:, 4] / acc[:, 3]
+    DisMedian_out[ix] = acc[:, 5]
+    Ninter_out[ix] = acc[:, 4]
     J = J > 1                                                                        # :131
     idx = np.argwhere(np.asfortranarray(J).transpose(2, 1, 0)).astype(np.int64)[:, ::-1] + 1  # ind2sub(find(J)) order
     if len(idx) > 1:                                                                 # :134-142
-        for p in idx:
-            c = Completeness_out[p[0] - 1, p[1] - 1, p[2] - 1]
-            csum += c
-            cpos += c * p
+        c = Completeness_out[tuple((idx - 1).T)]
+        # running sums in find() order (add.accumulate adds one term at a time, as the loop does)
+        csum = np.add.accumulate(np.concatenate([[csum], c]))[-1]
+        cpos = np.add.accumulate(np.concatenate([cpos[None], c[:, None] * idx]), axis=0)[-1]
     center1 = cpos / csum                                                            # :144
     if np.sqrt(((center1 - center0) ** 2).sum()) > max(maxD, maxD / 10000 * len(idx)):
         center, replace_center = np.round(center1), 1
@@ -191,11 +193,10 @@ def Forward_calc_comp_allvoxel_cuda(I, Imask, DisMedian, Ninter, voxel_waiting_g
                                         np.asarray(rot_angles, np.float32), G.flat_rowmajor(RotDet), param,
                                         param1).reshape(-1, 7)
     with np.errstate(invalid="ignore", divide="ignore"):
-        for r in out:                                                                # :69-76
-            xi, yi, zi = int(r[0]) - 1, int(r[1]) - 1, int(r[2]) - 1
-            Completeness_out[xi, yi, zi] = r[4] / r[3]
-            DisMedian_out[xi, yi, zi] = r[5]
-            Ninter_out[xi, yi, zi] = r[4]
+        ix = tuple(out[:, :3].astype(np.int64).T - 1)                                # :69-76
+        Completeness_out[ix] = out[:, 4] / out[:, 3]
+        DisMedian_out[ix] = out[:, 5]
+        Ninter_out[ix] = out[:, 4]
         Comp_max = np.nanmax(out[:, 4] / out[:, 3]) if len(out) else np.nan          # :77
     return Completeness_out, DisMedian_out, Ninter_out, Comp_max
 
@@ -225,13 +226,12 @@ def grow_unindexed_compete_comp_cuda(DS_in, wait_revising_voxels, id_neigb_all, 
                                          G.flat_rowmajor(B), G.flat_hkl(hkl), _map_for_call(proj_bin_bw),
                                          np.asarray(rot_angles, np.float32), G.flat_rowmajor(RotDet), param,
                                          param1).reshape(-1, 8)
-    for i, v in enumerate(np.asarray(wait_revising_voxels, np.int64)):                # :51-64
-        ix = (v[0] - 1, v[1] - 1, v[2] - 1)
-        DS_out["Completeness"][ix] = out[i, 5]
-        DS_out["GrainId"][ix] = out[i, 4]
-        DS_out["Dismedian"][ix] = out[i, 7]
-        DS_out["Ninter"][ix] = out[i, 6]
-        DS_out["VisitFlag"][ix] = 0.5
+    ix = tuple(np.asarray(wait_revising_voxels, np.int64).T - 1)                      # :51-64
+    DS_out["Completeness"][ix] = out[:, 5]
+    DS_out["GrainId"][ix] = out[:, 4]
+    DS_out["Dismedian"][ix] = out[:, 7]
+    DS_out["Ninter"][ix] = out[:, 6]
+    DS_out["VisitFlag"][ix] = 0.5
     return DS_out, out
 
 
@@ -263,9 +263,11 @@ def best_first_growth(score, I, Imask, DisMedian, Ninter, pos_indices, drop_off,
     cpos = seed_comp * np.array([x, y, z], np.float64)
     center0 = cpos / csum
     n_mask = int((np.asarray(Imask) > 0).sum())
-    neg = []  # [x y z C dis_median Nr_intersect]
+    neg = np.empty((64, 6))  # kept voxels [x y z C dis_median Nr_intersect], first n rows live
+    n = 0
     reg_size = 0
     Imask = np.asarray(Imask)
+    D_in, N_in = np.asarray(DisMedian, np.float64), np.asarray(Ninter, np.float64)
     while True:
         nb = np.array([x, y, z]) + _NEIGB
         ins = np.all((nb >= 1) & (nb <= dims), axis=1)
@@ -277,26 +279,33 @@ def best_first_growth(score, I, Imask, DisMedian, Ninter, pos_indices, drop_off,
             with np.errstate(invalid="ignore", divide="ignore"):
                 c = r[:, 1] / r[:, 0]
             ix = tuple((nb - 1).T)
-            i0, d0, n0 = I[ix], np.asarray(DisMedian, np.float64)[ix], np.asarray(Ninter, np.float64)[ix]
+            i0, d0, n0 = I[ix], D_in[ix], N_in[ix]
             ok = ((c > i0) & (r[:, 2] <= np.minimum(d0, maxDmedian))) | ((np.abs(c - i0) <= 0.01) & (r[:, 1] > n0))
-            for k in np.nonzero(ok)[0]:
-                neg.append([*nb[k], c[k], r[k, 2], r[k, 1]])
-                J[tuple(nb[k] - 1)] = 1
+            k = np.nonzero(ok)[0]
+            if len(k):
+                if n + len(k) > len(neg):
+                    neg = np.concatenate([neg, np.empty((max(len(neg), len(k)), 6))])
+                neg[n:n + len(k), :3] = nb[k]
+                neg[n:n + len(k), 3] = c[k]
+                neg[n:n + len(k), 4] = r[k, 2]
+                neg[n:n + len(k), 5] = r[k, 1]
+                n += len(k)
+                J[tuple((nb[k] - 1).T)] = 1
         J[x - 1, y - 1, z - 1] = 2
-        if not neg:
+        if n == 0:
             break
-        dist = np.array([e[3] for e in neg]) / seed_comp
+        dist = neg[:n, 3] / seed_comp
         index = int(np.nanargmax(dist))
         reg_size += 1
         if dist[index] > 1 - drop_off and reg_size < n_mask - 1:
-            e = neg[index]
+            e = neg[index].copy()
             csum += e[3]
-            cpos += e[3] * np.array(e[:3], np.float64)
+            cpos += e[3] * e[:3]
             xi, yi, zi = (int(v) - 1 for v in e[:3])
             C_out[xi, yi, zi], D_out[xi, yi, zi], N_out[xi, yi, zi] = e[3], e[4], e[5]
             x, y, z = xi + 1, yi + 1, zi + 1
-            neg[index] = neg[-1]
-            neg.pop()
+            neg[index] = neg[n - 1]  # the last kept voxel takes the chosen one's place
+            n -= 1
         else:
             break
     Jb = J > 1
@@ -327,7 +336,7 @@ def grow_indexed_region(I, Imask, DisMedian, Ninter, pos_indices, drop_off, maxD
     args = (G.flat_rowmajor(UU), G.flat_rowmajor(S), G.flat_rowmajor(B), G.flat_hkl(hkl))
     first = [_map_for_call(proj_bin_bw)]
 
-    def score(vox):
+    def score_rows(vox):
         rows = np.zeros((len(vox), 6), np.float32)
         rows[:, :3] = vox
         out = ctx.grow_indexed_region(rows, *args, first[0], np.asarray(rot_angles, np.float32),
@@ -335,5 +344,40 @@ def grow_indexed_region(I, Imask, DisMedian, Ninter, pos_indices, drop_off, maxD
         first[0] = None  # the map stays resident after the first call
         return out[:, 3:6]
 
-    return best_first_growth(score, I, Imask, DisMedian, Ninter, pos_indices, drop_off, maxD, indexed_comp,
-                             maxDmedian)
+    return best_first_growth(BlockScorer(score_rows, Imask), I, Imask, DisMedian, Ninter, pos_indices, drop_off,
+                             maxD, indexed_comp, maxDmedian)
+
+
+class BlockScorer:
+    """Memoised voxel scorer for one orientation.
+
+    A voxel's [Nr_simu, Nr_intersect, dis_median] depends only on the voxel and U, not on the
+    region grown so far, so the walk may read it from a cache.  A request with unscored voxels
+    scores, in one GPU call, every unscored in-mask voxel of the box that reaches ``halo`` voxels
+    beyond the requested ones: the walk then makes one call per few thousand voxels instead of
+    one per step, with the same values."""
+
+    def __init__(self, score_rows, Imask, halo: int = 6):
+        self.score_rows = score_rows
+        self.mask = np.asarray(Imask) > 0
+        self.have = np.zeros(self.mask.shape, bool)
+        self.val = np.zeros(self.mask.shape + (3,), np.float64)
+        self.halo = halo
+        self.calls = 0
+
+    def __call__(self, vox):
+        vox = np.asarray(vox, np.int64).reshape(-1, 3)
+        ix = tuple((vox - 1).T)
+        miss = ~self.have[ix]
+        if miss.any():
+            m = vox[miss]
+            lo = np.maximum(m.min(axis=0) - self.halo, 1)
+            hi = np.minimum(m.max(axis=0) + self.halo, self.mask.shape)
+            box = tuple(slice(a - 1, b) for a, b in zip(lo, hi))
+            todo = self.mask[box] & ~self.have[box]
+            blk = np.argwhere(todo) + lo
+            blk = np.unique(np.concatenate([blk, m]), axis=0)  # requested voxels outside the mask too
+            self.val[tuple((blk - 1).T)] = np.asarray(self.score_rows(blk), np.float64).reshape(-1, 3)
+            self.have[tuple((blk - 1).T)] = True
+            self.calls += 1
+        return self.val[ix]
