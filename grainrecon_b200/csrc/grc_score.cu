@@ -138,10 +138,11 @@ __device__ __forceinline__ float4 window_of(const Geo &g, float G_f);
 __device__ void build_gw(const Geo &g, const double *__restrict__ hkl, const double *__restrict__ U, float4 *gw,
                          float4 *win, double *sub) {
     const int ih = threadIdx.x;
-    if (ih >= g.nhkl) return;
+    if (ih >= g.nhkl && ih >= 9) return;
     double SUB[9];
     sub_matrix(g, U, SUB);
-    if (ih < 9) sub[ih] = SUB[ih];
+    if (ih < 9) sub[ih] = SUB[ih];  // threads 0..8 write SUB even when nhkl < 9
+    if (ih >= g.nhkl) return;
     const double h = hkl[3 * ih], k = hkl[3 * ih + 1], l = hkl[3 * ih + 2];
     const double x = SUB[0] * h + SUB[1] * k + SUB[2] * l;
     const double y = SUB[3] * h + SUB[4] * k + SUB[5] * l;
