@@ -118,6 +118,10 @@ void apply_options(grc_ctx *ctx) {
     g.dety0 = std::isnan(ctx->opt_dety0) ? g.detysize / 2.0 + 0.5 : ctx->opt_dety0;
     g.detz0 = std::isnan(ctx->opt_detz0) ? g.detzsize / 2.0 + 0.5 : ctx->opt_detz0;
     for (int i = 0; i < 9; ++i) g.Rf[i] = (float)g.R[i];
+    g.Ruf[0] = (float)(g.R[4] / g.pxy);
+    g.Ruf[1] = (float)(g.R[7] / g.pxy);
+    g.Rvf[0] = (float)(g.R[5] / g.pxz);
+    g.Rvf[1] = (float)(g.R[8] / g.pxz);
     g.dety0f = (float)g.dety0;
     g.detz0f = (float)g.detz0;
     g.rpxyf = (float)(1.0 / g.pxy);
@@ -145,6 +149,9 @@ int set_geometry(grc_ctx *ctx, const float *S, const float *B, const float *hkl,
         return fail(ctx, GRC_ECAPACITY, "nr_rot=%g exceeds GRC_MAX_NROT=%d", param[1], GRC_MAX_NROT);
     if (!is_int(param[10]) || !is_int(param[11]) || param[10] < 1 || param[11] < 1)
         return fail(ctx, GRC_EINVAL, "detysize/detzsize must be positive integers");
+    if (param[10] > 1e6f || param[11] > 1e6f || (double)param[10] * (double)param[11] > 2147483647.0)
+        return fail(ctx, GRC_ECAPACITY, "detector %gx%g: at most 10^6 pixels per side and 2^31-1 in all",
+                    param[10], param[11]);
     if (!(param[8] > 0) || !(param[9] > 0)) return fail(ctx, GRC_EINVAL, "pixel sizes must be positive");
     const int nhkl = (int)param[0], nrot = (int)param[1];
     std::vector<float> key;

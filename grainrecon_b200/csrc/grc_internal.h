@@ -25,6 +25,7 @@ struct Geo {
     double S[9], B[9], R[9]; // row-major
     // FP32 copies for the fast landing chain
     float Rf[9];
+    float Ruf[2], Rvf[2];    // R[4]/pxy, R[7]/pxy and R[5]/pxz, R[8]/pxz (ray K -> pixel u, v)
     float dety0f, detz0f, rpxyf, rpxzf;
     float bsy0f, bsy1f, bsz0f, bsz1f;
     float lo4pif, hi4pif, cbmaxf;   // lambda_min/(4 pi), lambda_max/(4 pi), cos(beta_max)

@@ -50,12 +50,14 @@ struct OmegaRow {
     double r2d, r3d, c, s;  // RotDet(:,2).d, RotDet(:,3).d with d = SamposW - D0; cos/sin omega
 };
 
-// The same row rounded to FP32 plus k_w = Omega^T k_in (prefilter), kept in shared memory.
+// The same row for the FP32 chain, kept in shared memory: the terms that do not depend on
+// the reflection are folded in (RotDet(1,:) * ax and the pixel scale), plus
+// k_w = Omega^T k_in for the prefilter.
 struct __align__(16) RowF {
-    float kx, ky, kz, L2;
-    float ax, ay, az, num;
-    float r2d, r3d, c, s;
-    float wx, wy, wz, pad;
+    float cN, ky, kz, L2;   // cN = R(1,1) ax
+    float cY, ay, az, num;  // cY = R(1,2) ax / pxy
+    float u0, v0, c, s;     // u0 = dety0 - r2d / pxy, v0 = detz0 - r3d / pxz
+    float wx, wy, wz, cZ;   // k_w; cZ = R(1,3) ax / pxz
 };
 static_assert(sizeof(RowF) == 64, "RowF layout");
 
@@ -99,21 +101,27 @@ __device__ __forceinline__ OmegaRow omega_row(const Geo &g, const double2 cs, co
     return r;
 }
 
+// FP32 row from the FP64 one (the folded constants are formed in FP64 and rounded once).
+__device__ __forceinline__ RowF row_f32(const Geo &g, const OmegaRow &r) {
+    RowF f;
+    f.cN = (float)(g.R[0] * r.ax);
+    f.ky = (float)r.ky; f.kz = (float)r.kz; f.L2 = (float)r.L2;
+    f.cY = (float)(g.R[1] * r.ax / g.pxy);
+    f.ay = (float)r.ay; f.az = (float)r.az; f.num = (float)r.num;
+    f.u0 = (float)(g.dety0 - r.r2d / g.pxy);
+    f.v0 = (float)(g.detz0 - r.r3d / g.pxz);
+    f.c = (float)r.c; f.s = (float)r.s;
+    f.wx = (float)(r.c * r.kx + r.s * r.ky);
+    f.wy = (float)(-r.s * r.kx + r.c * r.ky);
+    f.wz = (float)r.kz;
+    f.cZ = (float)(g.R[2] * r.ax / g.pxz);
+    return f;
+}
+
 // Omega table of one voxel in shared memory (all threads of the CTA).
 __device__ void build_rows(const Geo &g, const double2 *__restrict__ rot_cs, const double *__restrict__ vp,
                            RowF *rows) {
-    for (int iw = threadIdx.x; iw < g.nrot; iw += blockDim.x) {
-        const OmegaRow r = omega_row(g, rot_cs[iw], vp);
-        RowF f;
-        f.kx = (float)r.kx; f.ky = (float)r.ky; f.kz = (float)r.kz; f.L2 = (float)r.L2;
-        f.ax = (float)r.ax; f.ay = (float)r.ay; f.az = (float)r.az; f.num = (float)r.num;
-        f.r2d = (float)r.r2d; f.r3d = (float)r.r3d; f.c = (float)r.c; f.s = (float)r.s;
-        f.wx = (float)(r.c * r.kx + r.s * r.ky);
-        f.wy = (float)(-r.s * r.kx + r.c * r.ky);
-        f.wz = (float)r.kz;
-        f.pad = 0.f;
-        rows[iw] = f;
-    }
+    for (int iw = threadIdx.x; iw < g.nrot; iw += blockDim.x) rows[iw] = row_f32(g, omega_row(g, rot_cs[iw], vp));
 }
 
 // SUB = S*U*B (FP64, 9 values) of one trial.
@@ -213,15 +221,16 @@ __device__ __forceinline__ float4 window_of(const Geo &g, float G_f) {
     return make_float4((float)(lo - m), (float)(hi + m), (float)(lo + m), (float)(hi - m));
 }
 
-// FP32 landing chain (same algebra as landing_fp64).  Returns the map index, -1 for a
-// certain rejection, or -2 when the item lies within the ambiguity band of a
-// decision boundary and must be decided by landing_exact.
-__device__ __forceinline__ int64_t landing_fp32(const Geo &g, const RowF &r, const float4 gw, float lo_in, float hi_in,
-                                                int iw) {
-    const float Gtx = r.c * gw.x - r.s * gw.y, Gty = r.s * gw.x + r.c * gw.y, Gtz = gw.z;
-    const float dot = r.kx * Gtx + r.ky * Gty + r.kz * Gtz;
+// FP32 landing chain (the algebra of landing_fp64 with the row's constant terms folded in).
+// Returns the in-plane map offset (dety-1)*detzsize + (detz-1), -1 for a certain rejection,
+// or -2 when the item lies within the ambiguity band of a decision boundary and must be
+// decided by landing_exact.
+__device__ __forceinline__ int landing_fp32(const Geo &g, const RowF &r, const float4 gw, float lo_in, float hi_in) {
+    // k_in . (Omega Gw) = (Omega^T k_in) . Gw: the prefilter's product, without rotating G
+    const float dot = r.wx * gw.x + r.wy * gw.y + r.wz * gw.z;
     const float t = -dot;
     if (!(t > lo_in && t < hi_in)) return -2;  // near the wavelength / Bragg-angle window edge
+    const float Gty = r.s * gw.x + r.c * gw.y, Gtz = gw.z;
     // gw.w holds 1/|G|; reciprocal and square-root intrinsics (a few ulp) stay far inside
     // the ambiguity band
     const float x = dot * gw.w;
@@ -235,13 +244,12 @@ __device__ __forceinline__ int64_t landing_fp32(const Geo &g, const RowF &r, con
     const float sphx = p * rsqrtf(p);
     const float sphy = sphx * c2 - cphx * s2;
     const float diff = __fdividef(r.L2 * s2, sphy);
-    const float Kx = r.ax, Ky = r.ay + diff * gy, Kz = r.az + diff * gz;
-    const float nK = g.Rf[0] * Kx + g.Rf[3] * Ky + g.Rf[6] * Kz;
+    const float Ky = r.ay + diff * gy, Kz = r.az + diff * gz;  // K_x = ax lives in cN, cY, cZ
+    const float nK = r.cN + g.Rf[3] * Ky + g.Rf[6] * Kz;
     const float f = __fdividef(r.num, nK);
-    const float y2 = f * (g.Rf[1] * Kx + g.Rf[4] * Ky + g.Rf[7] * Kz) + r.r2d;
-    const float z2 = f * (g.Rf[2] * Kx + g.Rf[5] * Ky + g.Rf[8] * Kz) + r.r3d;
-    const float u = g.dety0f - y2 * g.rpxyf, v = g.detz0f - z2 * g.rpxzf;
-    if (!(fabsf(u) < 1e6f && fabsf(v) < 1e6f)) {
+    const float u = r.u0 - f * (r.cY + g.Ruf[0] * Ky + g.Ruf[1] * Kz);
+    const float v = r.v0 - f * (r.cZ + g.Rvf[0] * Ky + g.Rvf[1] * Kz);
+    if (!(fabsf(u) < 2e6f && fabsf(v) < 2e6f)) {  // detectors have at most 10^6 pixels per side
         // far off the detector (or NaN): certain rejection only for finite values
         return (isfinite(u) && isfinite(v)) ? -1 : -2;
     }
@@ -256,8 +264,7 @@ __device__ __forceinline__ int64_t landing_fp32(const Geo &g, const RowF &r, con
     const int iu = __float_as_int(tu) - 0x4B400000, iv = __float_as_int(tv) - 0x4B400000;
     if (!(iu >= 1 && iu <= g.detysize && iv >= 1 && iv <= g.detzsize)) return -1;
     if (ru >= g.bsy0f && ru <= g.bsy1f && rv >= g.bsz0f && rv <= g.bsz1f) return -1;
-    const uint32_t in_plane = (uint32_t)(iu - 1) * (uint32_t)g.detzsize + (uint32_t)(iv - 1);
-    return (int64_t)iw * g.plane + in_plane;
+    return (int)((uint32_t)(iu - 1) * (uint32_t)g.detzsize + (uint32_t)(iv - 1));  // < 2^31 pixels per plane
 }
 
 // Counts + histogram of codes below kHistBins (scoring pass).
@@ -353,7 +360,8 @@ __device__ __forceinline__ void run_trial(const Geo &g, const TrialCtx &tc, Sink
         if (valid) {
             const float4 gv = tc.gw[ihi];
             const float4 w = tc.win[ihi];
-            r = landing_fp32(g, tc.rows[iwi], gv, w.z, w.w, iwi);
+            const int ip = landing_fp32(g, tc.rows[iwi], gv, w.z, w.w);
+            r = ip >= 0 ? (int64_t)iwi * g.plane + ip : (int64_t)ip;
         }
         const bool amb = r == -2;
         const unsigned m = __ballot_sync(kFull, amb);
@@ -691,8 +699,7 @@ __device__ __forceinline__ int64_t voxel_of(const Work &w, int64_t t) {
 struct SweepSmem {
     RowF *rows;       // [rows_cap * kWin] rows of the current window, indexed vloc * kWin + wl
     float4 *hk;       // [nhkl] h as float
-    uint32_t *hist;   // [slots * kHist8Words]
-    uint32_t *cnt;    // [slots] Nr_simu | Nr_intersect << 16
+    uint32_t *hist;   // [slots * kHist8Words]; Nr_simu and Nr_intersect are read from it
     float *subf;      // [slots * 12]
     double *subd;     // [slots * 9]
     int *vloc;        // [slots]
@@ -702,7 +709,9 @@ struct SweepSmem {
     uint32_t *fqueue; // [kWarps * kFallbackCap]
 };
 
-// Shared-memory layout of one CTA holding `slots` trials and rows of `rows_cap` voxels.
+// Shared-memory layout of one CTA holding `slots` trials and rows of `rows_cap` voxels:
+// kSweepParts arrays, offsets returned in offs[].
+constexpr int kSweepParts = 10;
 __host__ __device__ inline size_t sweep_smem_layout(int nhkl, int rows_cap, int slots, size_t *offs) {
     size_t o = 0, i = 0;
     auto put = [&](size_t bytes) {
@@ -713,7 +722,6 @@ __host__ __device__ inline size_t sweep_smem_layout(int nhkl, int rows_cap, int 
     put(sizeof(RowF) * rows_cap * kWin);
     put(sizeof(float4) * nhkl);
     put(sizeof(uint32_t) * slots * kHist8Words);
-    put(sizeof(uint32_t) * slots);
     put(sizeof(float) * slots * 12);
     put(sizeof(double) * slots * 9);
     put(sizeof(int) * slots);
@@ -725,20 +733,19 @@ __host__ __device__ inline size_t sweep_smem_layout(int nhkl, int rows_cap, int 
 }
 
 __device__ __forceinline__ SweepSmem sweep_carve(unsigned char *base, int nhkl, int rows_cap, int slots) {
-    size_t offs[11];
+    size_t offs[kSweepParts];
     sweep_smem_layout(nhkl, rows_cap, slots, offs);
     SweepSmem m;
     m.rows = (RowF *)(base + offs[0]);
     m.hk = (float4 *)(base + offs[1]);
     m.hist = (uint32_t *)(base + offs[2]);
-    m.cnt = (uint32_t *)(base + offs[3]);
-    m.subf = (float *)(base + offs[4]);
-    m.subd = (double *)(base + offs[5]);
-    m.vloc = (int *)(base + offs[6]);
-    m.vglob = (int64_t *)(base + offs[7]);
-    m.vlist = (int64_t *)(base + offs[8]);
-    m.queue = (uint32_t *)(base + offs[9]);
-    m.fqueue = (uint32_t *)(base + offs[10]);
+    m.subf = (float *)(base + offs[3]);
+    m.subd = (double *)(base + offs[4]);
+    m.vloc = (int *)(base + offs[5]);
+    m.vglob = (int64_t *)(base + offs[6]);
+    m.vlist = (int64_t *)(base + offs[7]);
+    m.queue = (uint32_t *)(base + offs[8]);
+    m.fqueue = (uint32_t *)(base + offs[9]);
     return m;
 }
 
@@ -788,7 +795,6 @@ __global__ void __launch_bounds__(kThreads, GRC_SWEEP_BLOCKS) sweep_kernel(Geo g
             sm.subf[12 * tid + i] = (float)SUB[i];
         }
         sm.vglob[tid] = v;
-        sm.cnt[tid] = 0;
     }
     for (int i = tid; i < slots * kHist8Words; i += kThreads) sm.hist[i] = 0;
     for (int i = tid; i < g.nhkl; i += kThreads)
@@ -816,63 +822,54 @@ __global__ void __launch_bounds__(kThreads, GRC_SWEEP_BLOCKS) sweep_kernel(Geo g
 
     // Selected pixels reach the histogram one batch late: the code of batch k is loaded
     // when batch k is evaluated and applied after batch k+1 has been computed, so the
-    // L2 latency of the gather overlaps the next landing computations.
-    int64_t pend_idx = -1;   // this lane's pending map index (or -1)
+    // L2 latency of the gather overlaps the next landing computations.  The histogram is
+    // the only per-selection update: Nr_simu is its total and Nr_intersect the total of its
+    // codes below n_hit (< 255, so the saturated bin never holds a hit).
+    int pend_off = -1;   // this lane's pending offset in the projection window (or -1)
     int pend_slot = 0;
     uint32_t pend_code = 0;
     auto apply_pending = [&]() {
-        const bool ok = pend_idx >= 0;
-        const uint32_t code = pend_code;
-        if (ok) atomicAdd(&sm.hist[pend_slot * kHist8Words + (code >> 1)], 1u << ((code & 1u) * 16));
-        // per-slot counters, one atomic per distinct slot of the warp
-        const unsigned peers = __match_any_sync(kFull, ok ? pend_slot : -1);
-        const unsigned mok = __ballot_sync(kFull, ok), mhit = __ballot_sync(kFull, ok && code < g.n_hit);
-        if (ok && (__ffs(peers) - 1) == lane)
-            atomicAdd(&sm.cnt[pend_slot], (uint32_t)__popc(peers & mok) + ((uint32_t)__popc(peers & mhit) << 16));
-        pend_idx = -1;
-    };
-    auto sink = [&](int64_t idx, int s) {  // warp-synchronous: every lane calls it once per batch
-        uint32_t code = 0;
-        if (idx >= 0) code = __ldg(b.codes8 + idx);
-        apply_pending();
-        pend_idx = idx;
-        pend_slot = s;
-        pend_code = code;
+        if (pend_off >= 0)
+            atomicAdd(&sm.hist[pend_slot * kHist8Words + (pend_code >> 1)], 1u << ((pend_code & 1u) * 16));
+        pend_off = -1;
     };
 
     for (int w0 = 0; w0 < g.nrot; w0 += kWin) {
         const int nw = min(kWin, g.nrot - w0);
+        // codes of the window's first pixel; offsets within the window fit 32 bits
+        // (kWin * plane < 2^31, sweep_round_trials)
+        const uint8_t *wcodes = b.codes8 + (int64_t)w0 * g.plane;
+        auto sink = [&](int off, int s) {  // warp-synchronous: every lane calls it once per batch
+            uint32_t code = 0;
+            if (off >= 0) code = __ldg(wcodes + off);
+            apply_pending();
+            pend_off = off;
+            pend_slot = s;
+            pend_code = code;
+        };
         // ---- omega rows of this window for every voxel of the round
         for (int i = tid; i < nv * nw; i += kThreads) {
             const int vl = i / nw, wl = i - vl * nw;
-            const OmegaRow r = omega_row(g, b.rot_cs[w0 + wl], b.vpos + 3 * sm.vlist[vl]);
-            RowF f;
-            f.kx = (float)r.kx; f.ky = (float)r.ky; f.kz = (float)r.kz; f.L2 = (float)r.L2;
-            f.ax = (float)r.ax; f.ay = (float)r.ay; f.az = (float)r.az; f.num = (float)r.num;
-            f.r2d = (float)r.r2d; f.r3d = (float)r.r3d; f.c = (float)r.c; f.s = (float)r.s;
-            f.wx = (float)(r.c * r.kx + r.s * r.ky);
-            f.wy = (float)(-r.s * r.kx + r.c * r.ky);
-            f.wz = (float)r.kz;
-            f.pad = 0.f;
-            sm.rows[vl * kWin + wl] = f;
+            sm.rows[vl * kWin + wl] = row_f32(g, omega_row(g, b.rot_cs[w0 + wl], b.vpos + 3 * sm.vlist[vl]));
         }
         if (tid == 0) s_next = 0;
         __syncthreads();
         int qn = 0, fn = 0;
         auto fast = [&](uint32_t item, bool valid) {
-            int64_t r = -1;
+            int r = -1;
             const int s = (int)(item >> 16), wl = (int)((item >> 8) & 255u), ih = (int)(item & 255u);
             if (valid) {
                 const float4 gv = gw_of(sm.subf + 12 * s, sm.hk[ih]);
                 const float4 win = window_f(g, gv);
-                r = landing_fp32(g, sm.rows[sm.vloc[s] * kWin + wl], gv, win.z, win.w, w0 + wl);
+                const int ip = landing_fp32(g, sm.rows[sm.vloc[s] * kWin + wl], gv, win.z, win.w);
+                r = ip >= 0 ? wl * (int)g.plane + ip : ip;
 #ifdef GRC_AUDIT
                 // audit build: every certain FP32 decision is re-decided by the FP64 path
                 if (r != -2) {
                     const int64_t r64 = landing_exact(b.geo, b.rot_cs, b.vpos + 3 * sm.vglob[s], b.hkl,
                                                       sm.subd + 9 * s, w0 + wl, ih);
                     atomicAdd((unsigned long long *)(b.work_counter + 6), 1ull);
-                    if (r64 != r) atomicAdd(b.work_counter + 5, 1);
+                    if ((r64 >= 0 ? (int)(r64 - (int64_t)w0 * g.plane) : -1) != r) atomicAdd(b.work_counter + 5, 1);
                 }
 #endif
             }
@@ -884,9 +881,12 @@ __global__ void __launch_bounds__(kThreads, GRC_SWEEP_BLOCKS) sweep_kernel(Geo g
         };
         auto exact = [&](uint32_t item, bool valid) {
             const int s = (int)(item >> 16), wl = (int)((item >> 8) & 255u), ih = (int)(item & 255u);
-            int64_t r = -1;
-            if (valid)
-                r = landing_exact(b.geo, b.rot_cs, b.vpos + 3 * sm.vglob[s], b.hkl, sm.subd + 9 * s, w0 + wl, ih);
+            int r = -1;
+            if (valid) {
+                const int64_t r64 =
+                    landing_exact(b.geo, b.rot_cs, b.vpos + 3 * sm.vglob[s], b.hkl, sm.subd + 9 * s, w0 + wl, ih);
+                r = r64 >= 0 ? (int)(r64 - (int64_t)w0 * g.plane) : -1;
+            }
             sink(r, s);
         };
         auto drain = [&](bool all) {
@@ -963,21 +963,25 @@ __global__ void __launch_bounds__(kThreads, GRC_SWEEP_BLOCKS) sweep_kernel(Geo g
 
     // ---- finalize: one warp per slot, exact median from the 8-bit histogram
     for (int s = warp; s < nslot; s += kWarps) {
-        const uint32_t c = sm.cnt[s];
-        const int n = (int)(c & 0xffffu), inter = (int)(c >> 16);
         const uint32_t *h = sm.hist + s * kHist8Words;
         // lane owns bins [8*lane, 8*lane+8)
         uint32_t bins[8];
-        uint32_t local = 0;
+        uint32_t local = 0, hits = 0;
 #pragma unroll
         for (int i = 0; i < 4; ++i) {
             const uint32_t wv = h[4 * lane + i];
             bins[2 * i] = wv & 0xffffu;
             bins[2 * i + 1] = wv >> 16;
         }
-        if (lane == 31) bins[7] = 0;  // bin 255 = saturated codes, not part of the exact range
+        const uint32_t sat = __shfl_sync(kFull, bins[7], 31);  // bin 255: saturated codes (>= 255)
+        if (lane == 31) bins[7] = 0;  // not part of the exact range
 #pragma unroll
-        for (int i = 0; i < 8; ++i) local += bins[i];
+        for (int i = 0; i < 8; ++i) {
+            local += bins[i];
+            if ((uint32_t)(8 * lane + i) < g.n_hit) hits += bins[i];
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) hits += __shfl_xor_sync(kFull, hits, o);
         uint32_t incl = local;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
@@ -985,6 +989,7 @@ __global__ void __launch_bounds__(kThreads, GRC_SWEEP_BLOCKS) sweep_kernel(Geo g
             if (lane >= o) incl += y;
         }
         const uint32_t inr = __shfl_sync(kFull, incl, 31);
+        const int n = (int)(inr + sat), inter = (int)hits;  // Nr_simu, Nr_intersect
         const uint32_t excl = incl - local;
         const uint32_t ra = (uint32_t)(n + 1) / 2, rb = (uint32_t)n / 2 + 1;
         int ca = -1, cb = -1;
@@ -1136,7 +1141,7 @@ cudaError_t launch_sweep_t(const Geo &g, const ScoreBufs &b, const Work &w, int6
         int rc = explicit_voxels ? sl : (int)(w.n_or >= sl ? 2 : sl / w.n_or + 2);
         return rc > sl ? sl : rc;
     };
-    size_t offs[11];
+    size_t offs[kSweepParts];
     const size_t smem_max = sweep_smem_layout(g.nhkl, rows_for(max_slots), max_slots, offs);
     const size_t smem_r = refine_smem_bytes(g.nrot, g.nhkl);
     int per_sm = 0;
@@ -1314,7 +1319,10 @@ cudaError_t launch_simulate_work(const Geo &g, const ScoreBufs &b, const Work &w
 
 int64_t sweep_round_trials(const Geo &g, int num_sms) {
     // 16-bit per-slot counters and histogram bins; hit codes must stay below the saturation code
-    if (g.n_hit >= 255u || g.nhkl > 128 || (int64_t)g.nrot * g.nhkl > 65535) return 0;
+    // 32-bit offsets within a projection window
+    if (g.n_hit >= 255u || g.nhkl > 128 || (int64_t)g.nrot * g.nhkl > 65535 ||
+        (int64_t)kWin * g.plane > 2147483647LL)
+        return 0;
     return (int64_t)num_sms * GRC_SWEEP_BLOCKS * kSlotsBulk;
 }
 
