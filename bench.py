@@ -232,6 +232,11 @@ def run_ours(args):
         torch.cuda.synchronize()
     total_ms = ev0.elapsed_time(ev1)
     if args.profile:
+        # selected reflections (map lookups) per trial of the profiled steps: turns an ncu
+        # capture's DRAM bytes per launch into bytes per lookup
+        simu = d_out.view(K, -1, 4)[:, :, 0].double()
+        print(json.dumps({"profile": args.config, "lookups_per_trial": float(simu.mean()),
+                          "trials_per_step": S * N_ORIENT, "kernel_launches": launches}), flush=True)
         ctx.close()
         return 0
     max_ms = max_over_ranks(total_ms, device="cuda")
@@ -272,8 +277,8 @@ def run_ours(args):
     clocks = clk.summary()
     try:
         # DRAM bytes per selected reflection and warp instructions per trial measured by ncu on
-        # the same kernel (profiles/)
-        prof = json.load(open(os.path.join(ROOT, "profiles", f"{kernel}_dram.json")))
+        # the same kernel and workload (profiles/); absent for a workload that was not captured
+        prof = json.load(open(os.path.join(ROOT, "profiles", f"{kernel}_dram.json")))["workloads"][args.config]
         traffic = float(np.mean(lookups)) * prof["dram_bytes_per_lookup"]
         if "warp_instructions_per_trial" in prof:
             # issue roofline: one warp instruction per scheduler per clock, 4 schedulers per SM

@@ -808,15 +808,6 @@ __global__ void __launch_bounds__(kThreads, GRC_SWEEP_BLOCKS) sweep_kernel(Geo g
         }
         s_nv = nv;
     }
-    float hx[HPL], hy[HPL], hz[HPL];
-#pragma unroll
-    for (int j = 0; j < HPL; ++j) {
-        const int ih = lane + 32 * j;
-        const float4 h = ih < g.nhkl ? sm.hk[ih] : make_float4(0.f, 0.f, 0.f, 0.f);
-        hx[j] = h.x;
-        hy[j] = h.y;
-        hz[j] = h.z;
-    }
     __syncthreads();
     const int nv = s_nv;
 
@@ -929,7 +920,10 @@ __global__ void __launch_bounds__(kThreads, GRC_SWEEP_BLOCKS) sweep_kernel(Geo g
             float gx[HPL], gy[HPL], gz[HPL], lo[HPL], hi[HPL];
 #pragma unroll
             for (int j = 0; j < HPL; ++j) {
-                const float4 gv = gw_of(sf, make_float4(hx[j], hy[j], hz[j], 0.f));
+                // h re-read from shared memory at each slot: holding it in registers for the
+                // whole kernel costs spills of the 80-register budget
+                const int ihj = lane + 32 * j;
+                const float4 gv = gw_of(sf, ihj < g.nhkl ? sm.hk[ihj] : make_float4(0.f, 0.f, 0.f, 0.f));
                 const float4 win = window_f(g, gv);
                 const bool real = lane + 32 * j < g.nhkl;
                 gx[j] = gv.x;
