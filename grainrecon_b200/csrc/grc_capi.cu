@@ -693,14 +693,15 @@ int grc_score_trials_device(grc_ctx *ctx, const double *d_pos, int64_t n_vox, co
     grc::Work w{};
     if (d_tv) {
         TRY(ensure(ctx, ctx->items, sizeof(longlong4) * n_trials));
-        TRY(ensure(ctx, ctx->bad, sizeof(int)));
-        CU(cudaMemsetAsync(ctx->bad.p, 0, sizeof(int), ctx->stream));
+        TRY(ensure(ctx, ctx->bad, 2 * sizeof(int)));
+        CU(cudaMemsetAsync(ctx->bad.p, 0, 2 * sizeof(int), ctx->stream));
         CU(grc::launch_trial_items(d_tv, d_to, n_trials, n_vox, n_q, (longlong4 *)ctx->items.p, (int *)ctx->bad.p,
                                    ctx->stream));
-        int hbad = 0;
-        CU(cudaMemcpyAsync(&hbad, ctx->bad.p, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+        int hbad[2] = {0, 0};
+        CU(cudaMemcpyAsync(hbad, ctx->bad.p, 2 * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
         CU(cudaStreamSynchronize(ctx->stream));
-        if (hbad) return fail(ctx, GRC_EINVAL, "trials: a voxel or orientation index lies out of range");
+        if (hbad[0]) return fail(ctx, GRC_EINVAL, "trials: a voxel or orientation index lies out of range");
+        w.starts_per_32 = hbad[1];
         w.items = (const longlong4 *)ctx->items.p;
         w.trial_orient = d_to;
         w.trial_voxel = d_tv;

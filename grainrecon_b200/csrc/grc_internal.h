@@ -57,6 +57,10 @@ struct Work {
     int64_t chunks_per_voxel;
     int32_t chunk;
     int32_t diag;
+    // Explicit lists: the most voxel-run starts (t = 0 or trial_voxel[t] != trial_voxel[t-1]) in
+    // any aligned block of 32 trials, or 0 when unknown.  Bounds the distinct voxels a sweep tile
+    // meets, so seed-major lists need one omega-row set per voxel, not one per trial.
+    int32_t starts_per_32;
 };
 
 struct ScoreBufs {
@@ -151,6 +155,9 @@ cudaError_t launch_pair_gather(const PairRec *in, const int32_t *order, int64_t 
 // FP64 trial lists (grc_seed.cu): U from double quaternions, work items from (voxel, orientation)
 // index pairs (bad |= 1 for an index out of range; that item is left empty).
 cudaError_t launch_quat_to_u_d(const double *q, int64_t n, double *U, cudaStream_t s);
+// Checks the indices (bad[0] != 0 when one is out of range), builds the work items and sets
+// bad[1] to the most voxel-run starts in any aligned block of 32 trials (Work::starts_per_32);
+// bad[0..1] must be zero on entry.
 cudaError_t launch_trial_items(const int32_t *tv, const int32_t *to, int64_t n, int64_t n_vox, int64_t n_q,
                                longlong4 *items, int *bad, cudaStream_t s);
 

@@ -1132,7 +1132,12 @@ cudaError_t launch_sweep_t(const Geo &g, const ScoreBufs &b, const Work &w, int6
     const bool caller_tile = max_slots >= 1 && max_slots <= kSlots;
     if (!caller_tile) max_slots = kSlotsBulk;
     auto rows_for = [&](int sl) {  // distinct voxels one CTA can meet among sl consecutive trials
-        int rc = explicit_voxels ? sl : (int)(w.n_or >= sl ? 2 : sl / w.n_or + 2);
+        int rc = (int)(w.n_or >= sl ? 2 : (w.n_or > 0 ? sl / w.n_or + 2 : sl));
+        if (explicit_voxels) {
+            // sl consecutive trials overlap at most ceil(sl/32) + 1 aligned blocks of 32, each with
+            // at most starts_per_32 run starts: a seed-major list needs a few row sets, not sl
+            rc = w.starts_per_32 > 0 ? 1 + ((sl + 31) / 32 + 1) * w.starts_per_32 : sl;
+        }
         return rc > sl ? sl : rc;
     };
     size_t offs[kSweepParts];

@@ -52,11 +52,21 @@ __global__ void quat_to_u_d_k(const double *q, int64_t n, double *U) {
 
 __global__ void trial_items_k(const int32_t *tv, const int32_t *to, int64_t n, int64_t n_vox, int64_t n_q,
                               longlong4 *items, int *bad) {
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t v = tv[i], o = to[i];
-        const bool ok = v >= 0 && v < n_vox && o >= 0 && o < n_q;
-        if (!ok) atomicOr(bad, 1);
-        items[i] = make_longlong4(ok ? v : 0, i, ok ? i + 1 : i, 0);
+    // blockDim is a multiple of 32, so each warp walks aligned blocks of 32 trials; the loop test
+    // uses the block's first trial, so all lanes of a warp take part in every ballot
+    const int lane = threadIdx.x & 31;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i - lane < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const bool in = i < n;
+        bool start = false;
+        if (in) {
+            const int64_t v = tv[i], o = to[i];
+            const bool ok = v >= 0 && v < n_vox && o >= 0 && o < n_q;
+            if (!ok) atomicOr(bad, 1);
+            items[i] = make_longlong4(ok ? v : 0, i, ok ? i + 1 : i, 0);
+            start = i == 0 || tv[i] != tv[i - 1];
+        }
+        const int starts = __popc(__ballot_sync(0xffffffffu, start));
+        if (lane == 0 && starts > 0) atomicMax(bad + 1, starts);
     }
 }
 

@@ -89,6 +89,45 @@ def test_trial_list_matches_oracle(scene):
         ctx.score_trials_device(d(pos), 8, d(qs), 40, d(tv), d(bad), 300, out)
 
 
+def test_trial_list_voxel_orders(scene):
+    """The sweep sizes its per-tile voxel rows from the list's voxel-run starts (the most starts in
+    any aligned block of 32 trials).  Lists in several voxel orders -- seed-major (730 trials per
+    voxel, as the local refine builds them), runs of 10, runs of 1-3, two voxels alternating in
+    pairs, and all of them concatenated -- must score identically on the sweep and on the
+    per-trial kernel, which keeps no per-tile rows."""
+    import torch
+    s, ctx, sc, _ = scene
+    rng = np.random.default_rng(9)
+    vox, pos = _voxels(s, 40, 3)
+    qs = np.array([_near(s.grain_q[k % len(s.grain_q)], rng, 0.002 if k < 120 else 0.05) for k in range(730)])
+    n = 40 * 730
+    runs = np.repeat(np.arange(40), 10)
+    short = rng.integers(1, 4, n)
+    orders = {
+        "seed-major": np.repeat(np.arange(40), 730),
+        "runs of 10": np.resize(runs, n),
+        "runs of 1-3": np.resize(np.repeat(rng.integers(0, 40, n), short), n),
+        "alternating pairs": np.resize(np.array([5, 5, 9, 9]), n),
+    }
+    orders["concatenated"] = np.concatenate([v[: n // 4] for v in orders.values()])[:n]
+    d = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    try:
+        for name, tv in orders.items():
+            tv = tv.astype(np.int32)
+            to = rng.integers(0, 730, n).astype(np.int32)
+            res = {}
+            for path in (2, 1):
+                ctx.set_path(path)
+                out = torch.empty(n * 4, dtype=torch.float32, device="cuda")
+                ctx.score_trials_device(d(pos), 40, d(qs), 730, d(tv), d(to), n, out)
+                res[path] = out.view(-1, 4).cpu().numpy()
+                assert ctx.last_stats()["path"] == path, name
+            np.testing.assert_array_equal(res[2], res[1], err_msg=name)
+            assert np.nanmax(res[2][:, 2]) > 0.9, name  # near-true orientations are scored
+    finally:
+        ctx.set_path(0)
+
+
 def test_orientation_fit_matches_oracle_fminsearchbnd(scene):
     import torch
     s, ctx, sc, _ = scene
