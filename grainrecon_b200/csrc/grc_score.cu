@@ -682,12 +682,15 @@ __global__ void __launch_bounds__(kThreads, 2) mark_kernel(Geo g, ScoreBufs b, W
 
 // ---------------------------------------------------------------------------------
 // Projection-window sweep.  One launch = one round: each CTA holds kSlots trials in
-// shared memory (counters, a 256-bin histogram of the 8-bit saturated codes, S*U*B)
-// and every CTA walks the projections in windows of kWin at the same pace, so the
-// map pixels being read belong to a few projections at a time and stay in L2.
+// shared memory (a 256-bin histogram of the 8-bit saturated codes, S*U*B) and every CTA
+// walks the projections in windows of nwin at the same pace, so the map pixels being read
+// belong to a few projections at a time and stay in L2.  The window is 32, 16 or 8
+// projections: the widest whose omega rows keep the CTAs per SM of the 8-wide layout
+// (fewer window barriers and row rebuilds per trial).
 constexpr int kSlots = 96;      // most trials a CTA holds in one round
 constexpr int kSlotsBulk = 64;  // tile of multi-round work and of explicit voxel lists
-constexpr int kWin = 8;
+constexpr int kWinMin = 8;      // narrowest projection window
+constexpr int kWinWide[2] = {32, 16};  // wider windows tried first (instantiated for these)
 constexpr int kHist8Words = 128;  // 256 u16 bins per slot, two per word
 
 __device__ __forceinline__ int64_t voxel_of(const Work &w, int64_t t) {
@@ -697,7 +700,7 @@ __device__ __forceinline__ int64_t voxel_of(const Work &w, int64_t t) {
 }
 
 struct SweepSmem {
-    RowF *rows;       // [rows_cap * kWin] rows of the current window, indexed vloc * kWin + wl
+    RowF *rows;       // [rows_cap * nwin] rows of the current window, indexed vloc * nwin + wl
     float4 *hk;       // [nhkl] h as float
     uint32_t *hist;   // [slots * kHist8Words]; Nr_simu and Nr_intersect are read from it
     float *subf;      // [slots * 12]
@@ -712,14 +715,14 @@ struct SweepSmem {
 // Shared-memory layout of one CTA holding `slots` trials and rows of `rows_cap` voxels:
 // kSweepParts arrays, offsets returned in offs[].
 constexpr int kSweepParts = 10;
-__host__ __device__ inline size_t sweep_smem_layout(int nhkl, int rows_cap, int slots, size_t *offs) {
+__host__ __device__ inline size_t sweep_smem_layout(int nhkl, int rows_cap, int slots, int nwin, size_t *offs) {
     size_t o = 0, i = 0;
     auto put = [&](size_t bytes) {
         o = (o + 15) & ~size_t(15);
         offs[i++] = o;
         o += bytes;
     };
-    put(sizeof(RowF) * rows_cap * kWin);
+    put(sizeof(RowF) * rows_cap * nwin);
     put(sizeof(float4) * nhkl);
     put(sizeof(uint32_t) * slots * kHist8Words);
     put(sizeof(float) * slots * 12);
@@ -732,9 +735,9 @@ __host__ __device__ inline size_t sweep_smem_layout(int nhkl, int rows_cap, int 
     return (o + 15) & ~size_t(15);
 }
 
-__device__ __forceinline__ SweepSmem sweep_carve(unsigned char *base, int nhkl, int rows_cap, int slots) {
+__device__ __forceinline__ SweepSmem sweep_carve(unsigned char *base, int nhkl, int rows_cap, int slots, int nwin) {
     size_t offs[kSweepParts];
-    sweep_smem_layout(nhkl, rows_cap, slots, offs);
+    sweep_smem_layout(nhkl, rows_cap, slots, nwin, offs);
     SweepSmem m;
     m.rows = (RowF *)(base + offs[0]);
     m.hk = (float4 *)(base + offs[1]);
@@ -768,14 +771,15 @@ __device__ __forceinline__ float4 window_f(const Geo &g, const float4 gv) {
     return make_float4(lo - m, hi + m, lo + m, hi - m);
 }
 
-template <int HPL>
+template <int HPL, int WIN>
 __global__ void __launch_bounds__(kThreads, GRC_SWEEP_BLOCKS) sweep_kernel(Geo g, ScoreBufs b, Work w, int64_t round_base,
                                                             int64_t n_trials, int rows_cap, int slots) {
+    constexpr int nwin = WIN;  // projections per window
     const int64_t cta_base = round_base + (int64_t)blockIdx.x * slots;
     if (cta_base >= n_trials) return;
     const int nslot = (int)min((int64_t)slots, n_trials - cta_base);
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    const SweepSmem sm = sweep_carve(smem_raw, g.nhkl, rows_cap, slots);
+    const SweepSmem sm = sweep_carve(smem_raw, g.nhkl, rows_cap, slots, nwin);
     __shared__ int s_nv, s_next;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const unsigned lt = (1u << lane) - 1u;
@@ -825,10 +829,10 @@ __global__ void __launch_bounds__(kThreads, GRC_SWEEP_BLOCKS) sweep_kernel(Geo g
         pend_off = -1;
     };
 
-    for (int w0 = 0; w0 < g.nrot; w0 += kWin) {
-        const int nw = min(kWin, g.nrot - w0);
+    for (int w0 = 0; w0 < g.nrot; w0 += nwin) {
+        const int nw = min(nwin, g.nrot - w0);
         // codes of the window's first pixel; offsets within the window fit 32 bits
-        // (kWin * plane < 2^31, sweep_round_trials)
+        // (nwin * plane < 2^31, launch_sweep_t)
         const uint8_t *wcodes = b.codes8 + (int64_t)w0 * g.plane;
         auto sink = [&](int off, int s) {  // warp-synchronous: every lane calls it once per batch
             uint32_t code = 0;
@@ -841,7 +845,7 @@ __global__ void __launch_bounds__(kThreads, GRC_SWEEP_BLOCKS) sweep_kernel(Geo g
         // ---- omega rows of this window for every voxel of the round
         for (int i = tid; i < nv * nw; i += kThreads) {
             const int vl = i / nw, wl = i - vl * nw;
-            sm.rows[vl * kWin + wl] = row_f32(g, omega_row(g, b.rot_cs[w0 + wl], b.vpos + 3 * sm.vlist[vl]));
+            sm.rows[vl * nwin + wl] = row_f32(g, omega_row(g, b.rot_cs[w0 + wl], b.vpos + 3 * sm.vlist[vl]));
         }
         if (tid == 0) s_next = 0;
         __syncthreads();
@@ -852,7 +856,7 @@ __global__ void __launch_bounds__(kThreads, GRC_SWEEP_BLOCKS) sweep_kernel(Geo g
             if (valid) {
                 const float4 gv = gw_of(sm.subf + 12 * s, sm.hk[ih]);
                 const float4 win = window_f(g, gv);
-                const int ip = landing_fp32(g, sm.rows[sm.vloc[s] * kWin + wl], gv, win.z, win.w);
+                const int ip = landing_fp32(g, sm.rows[sm.vloc[s] * nwin + wl], gv, win.z, win.w);
                 r = ip >= 0 ? wl * (int)g.plane + ip : ip;
 #ifdef GRC_AUDIT
                 // audit build: every certain FP32 decision is re-decided by the FP64 path
@@ -932,7 +936,7 @@ __global__ void __launch_bounds__(kThreads, GRC_SWEEP_BLOCKS) sweep_kernel(Geo g
                 lo[j] = real ? win.x : CUDART_INF_F;
                 hi[j] = real ? win.y : -CUDART_INF_F;
             }
-            const RowF *vr = sm.rows + sm.vloc[s] * kWin;
+            const RowF *vr = sm.rows + sm.vloc[s] * nwin;
             for (int wl = 0; wl < nw; ++wl) {
                 const float4 kwv = reinterpret_cast<const float4 *>(vr + wl)[3];
                 const float kx = kwv.x, ky = kwv.y, kz = kwv.z;
@@ -1141,13 +1145,14 @@ cudaError_t launch_sweep_t(const Geo &g, const ScoreBufs &b, const Work &w, int6
         return rc > sl ? sl : rc;
     };
     size_t offs[kSweepParts];
-    const size_t smem_max = sweep_smem_layout(g.nhkl, rows_for(max_slots), max_slots, offs);
+    const size_t smem_max = sweep_smem_layout(g.nhkl, rows_for(max_slots), max_slots, kWinMin, offs);
     const size_t smem_r = refine_smem_bytes(g.nrot, g.nhkl);
     int per_sm = 0;
-    cudaError_t e = cudaFuncSetAttribute(sweep_kernel<HPL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)smem_max);
+    using SweepFn = void (*)(Geo, ScoreBufs, Work, int64_t, int64_t, int, int);
+    const SweepFn k8 = sweep_kernel<HPL, kWinMin>;
+    cudaError_t e = cudaFuncSetAttribute(k8, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_max);
     if (e != cudaSuccess) return e;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sweep_kernel<HPL>, kThreads, smem_max);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k8, kThreads, smem_max);
     if (e != cudaSuccess) return e;
     if (per_sm < 1) return cudaErrorInvalidConfiguration;
     int grid_r = 0;
@@ -1157,16 +1162,11 @@ cudaError_t launch_sweep_t(const Geo &g, const ScoreBufs &b, const Work &w, int6
     if (!caller_tile && !explicit_voxels && n_trials > grid * max_slots && n_trials <= grid * kSlots) {
         // one round of up to kSlots trials per CTA, if the larger tile keeps the same CTAs per SM
         int per_sm1 = 0;
-        const size_t smem1 = sweep_smem_layout(g.nhkl, rows_for(kSlots), kSlots, offs);
-        if (cudaFuncSetAttribute(sweep_kernel<HPL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem1) ==
-                cudaSuccess &&
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm1, sweep_kernel<HPL>, kThreads, smem1) ==
-                cudaSuccess &&
+        const size_t smem1 = sweep_smem_layout(g.nhkl, rows_for(kSlots), kSlots, kWinMin, offs);
+        if (cudaFuncSetAttribute(k8, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem1) == cudaSuccess &&
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm1, k8, kThreads, smem1) == cudaSuccess &&
             per_sm1 == per_sm) {
             max_slots = kSlots;
-        } else {
-            e = cudaFuncSetAttribute(sweep_kernel<HPL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_max);
-            if (e != cudaSuccess) return e;
         }
     }
     // rounds of equal size: slots per CTA chosen so the last round is not a sliver
@@ -1174,7 +1174,26 @@ cudaError_t launch_sweep_t(const Geo &g, const ScoreBufs &b, const Work &w, int6
     int slots = (int)((n_trials + rounds * grid - 1) / (rounds * grid));
     if (slots < 1) slots = 1;
     const int rows_cap = rows_for(slots);
-    const size_t smem = sweep_smem_layout(g.nhkl, rows_cap, slots, offs);
+    // the widest projection window whose rows keep the grid's CTAs per SM (and 32-bit map
+    // offsets within a window)
+    SweepFn kern = k8;
+    size_t smem = sweep_smem_layout(g.nhkl, rows_cap, slots, kWinMin, offs);
+    for (int cand : kWinWide) {
+        if ((int64_t)cand * g.plane > 2147483647LL) continue;
+        const SweepFn kc = cand == 32 ? (SweepFn)sweep_kernel<HPL, 32> : (SweepFn)sweep_kernel<HPL, 16>;
+        const size_t smem_c = sweep_smem_layout(g.nhkl, rows_cap, slots, cand, offs);
+        int per_c = 0;
+        if (cudaFuncSetAttribute(kc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_c) == cudaSuccess &&
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_c, kc, kThreads, smem_c) == cudaSuccess &&
+            per_c >= per_sm) {
+            kern = kc;
+            smem = smem_c;
+            break;
+        }
+    }
+    cudaGetLastError();  // a refused wider window is not an error of this launch
+    e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
     const int64_t per_round = grid * slots;
     e = cudaMemsetAsync(b.work_counter, 0, 8 * sizeof(int), s);
     if (e != cudaSuccess) return e;
@@ -1182,7 +1201,7 @@ cudaError_t launch_sweep_t(const Geo &g, const ScoreBufs &b, const Work &w, int6
     for (int64_t base = 0; base < n_trials; base += per_round) {
         const int64_t left = (n_trials - base + slots - 1) / slots;
         const int gr = (int)(left < grid ? left : grid);
-        sweep_kernel<HPL><<<gr, kThreads, smem, s>>>(g, b, w, base, n_trials, rows_cap, slots);
+        kern<<<gr, kThreads, smem, s>>>(g, b, w, base, n_trials, rows_cap, slots);
         ++*launches;
     }
     if (ev1) cudaEventRecord(ev1, s);
@@ -1320,7 +1339,7 @@ int64_t sweep_round_trials(const Geo &g, int num_sms) {
     // 16-bit per-slot counters and histogram bins; hit codes must stay below the saturation code
     // 32-bit offsets within a projection window
     if (g.n_hit >= 255u || g.nhkl > 128 || (int64_t)g.nrot * g.nhkl > 65535 ||
-        (int64_t)kWin * g.plane > 2147483647LL)
+        (int64_t)kWinMin * g.plane > 2147483647LL)
         return 0;
     return (int64_t)num_sms * GRC_SWEEP_BLOCKS * kSlotsBulk;
 }
