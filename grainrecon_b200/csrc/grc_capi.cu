@@ -330,8 +330,13 @@ int forward_device(grc_ctx *ctx, const float *d_pos, int64_t n_vox, const float 
     CU(grc::launch_pos_f3(d_pos, n_vox, (double *)ctx->pos.p, ctx->stream));
     grc::Work w{};
     w.n_or = n_q;
-    w.chunk = kSeedChunk;
-    w.chunks_per_voxel = (n_q + kSeedChunk - 1) / kSeedChunk;
+    // Small calls (the per-trial kernel's range) get one work item per trial until every
+    // resident CTA has one: an item's trials run one after another in one CTA.  Larger calls
+    // keep kSeedChunk orientations per item, which shares the item's omega table among them.
+    const int64_t fill = (int64_t)ctx->num_sms * 4;
+    const int64_t chunk = std::max<int64_t>(1, std::min<int64_t>(kSeedChunk, n_vox * n_q / fill));
+    w.chunk = (int32_t)chunk;
+    w.chunks_per_voxel = (n_q + chunk - 1) / chunk;
     w.n_items = n_vox * w.chunks_per_voxel;
     TRY(run_score(ctx, w, n_vox * n_q));
     CU(grc::launch_epi_forward((const grc::TrialRes *)ctx->res.p, n_vox * n_q, d_out, ctx->stream));
