@@ -302,12 +302,14 @@ int run_score(grc_ctx *ctx, const grc::Work &w, int64_t n_trials) {
     cudaEvent_t e0 = ctx->timing ? ctx->ev0 : nullptr, e1 = ctx->timing ? ctx->ev1 : nullptr;
     const int64_t round = ctx->force_path == 1 ? 0 : grc::sweep_round_trials(ctx->geo, ctx->num_sms);
     cudaError_t e;
-    // Implicit scan lists (voxels x orientations) go to the sweep from 1/16 of a round: a
-    // one-voxel scan of 2,048 orientations already takes 0.27 ms there against 0.36 ms on the
-    // per-trial kernel (8,192: 0.65 against 1.48 ms), while 1,024 favour the per-trial kernel.
-    // Explicit lists keep the half-round rule.
-    const bool implicit = !w.items && !w.trial_voxel && !w.diag && w.n_or > 0;
-    const int64_t from = implicit ? (round + 15) / 16 : (round + 1) / 2;
+    // Scan lists whose voxels carry at least a tile of orientations (a sweep tile then meets at
+    // most two voxels) go to the sweep from 1/16 of a round: a one-voxel scan of 2,048
+    // orientations already takes 0.27 ms there against 0.36 ms on the per-trial kernel (8,192:
+    // 0.65 against 1.48 ms), while 1,024 favour the per-trial kernel.  Lists with a voxel per
+    // trial or a few (grow rows, compete, trial lists) keep the half-round rule: there the two
+    // kernels are within 3% of each other up to 16,384 trials.
+    const bool shared_voxels = !w.items && !w.trial_voxel && !w.diag && w.n_or >= 64;
+    const int64_t from = shared_voxels ? (round + 15) / 16 : (round + 1) / 2;
     if (round > 0 && (ctx->force_path == 2 || n_trials >= from)) {
         // projection-window sweep (L2-resident map windows) for large trial counts
         TRY(ensure(ctx, ctx->rlist, sizeof(int64_t) * n_trials));
