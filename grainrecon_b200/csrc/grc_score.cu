@@ -1178,20 +1178,24 @@ cudaError_t launch_sweep_t(const Geo &g, const ScoreBufs &b, const Work &w, int6
     // offsets within a window)
     SweepFn kern = k8;
     size_t smem = sweep_smem_layout(g.nhkl, rows_cap, slots, kWinMin, offs);
+    bool refused = false;
     for (int cand : kWinWide) {
         if ((int64_t)cand * g.plane > 2147483647LL) continue;
         const SweepFn kc = cand == 32 ? (SweepFn)sweep_kernel<HPL, 32> : (SweepFn)sweep_kernel<HPL, 16>;
         const size_t smem_c = sweep_smem_layout(g.nhkl, rows_cap, slots, cand, offs);
         int per_c = 0;
-        if (cudaFuncSetAttribute(kc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_c) == cudaSuccess &&
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_c, kc, kThreads, smem_c) == cudaSuccess &&
-            per_c >= per_sm) {
+        if (cudaFuncSetAttribute(kc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_c) != cudaSuccess ||
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_c, kc, kThreads, smem_c) != cudaSuccess) {
+            refused = true;  // more shared memory than a CTA may have: not this window
+            continue;
+        }
+        if (per_c >= per_sm) {
             kern = kc;
             smem = smem_c;
             break;
         }
     }
-    cudaGetLastError();  // a refused wider window is not an error of this launch
+    if (refused) cudaGetLastError();  // the refused query is not an error of this launch
     e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     const int64_t per_round = grid * slots;
