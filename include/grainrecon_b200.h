@@ -335,8 +335,9 @@ int grc_last_stats(grc_ctx *ctx, grc_stats *out);
 int grc_set_timing(grc_ctx *ctx, int enable);
 /*
  * Scoring kernel selection: 0 = by size (default: the projection-window sweep, which
- * keeps the map windows L2-resident, once a call holds at least half a sweep round of
- * trials; the per-trial kernel below that), 1 = always the per-trial kernel,
+ * keeps the map windows L2-resident, once a call holds 1/16 of a sweep round of trials --
+ * 1,776 on 148 SMs -- when each voxel carries at least 64 orientations, or half a round
+ * otherwise; the per-trial kernel below that), 1 = always the per-trial kernel,
  * 2 = always the sweep.  Results are identical; only speed differs.
  */
 int grc_set_path(grc_ctx *ctx, int path);
