@@ -52,7 +52,7 @@ def _map_for_call(proj_bin_bw):
     # view would copy the whole map on every call
     at = np.arange(0, a.size, max(1, a.size // 4096))
     sample = a[np.unravel_index(at, a.shape)] if a.ndim > 1 else a.reshape(-1)[at]
-    key =(id(proj_bin_bw), a.shape, a.dtype.str, hash(np.asarray(sample, np.float32).tobytes()))
+    key = (id(proj_bin_bw), a.shape, a.dtype.str, hash(np.asarray(sample, np.float32).tobytes()))
     if key == _map_key:
         return None
     _map_key = key
@@ -137,7 +137,7 @@ def grow_indexed_region_cuda(I, Imask, DisMedian, Ninter, pos_indices, Spot_L, d
     xg, yg, zg = np.meshgrid(np.arange(box[0, 0], box[0, 1] + 1), np.arange(box[1, 0], box[1, 1] + 1),
                              np.arange(box[2, 0], box[2, 1] + 1))
     vox = np.stack([xg.ravel(order="F"), yg.ravel(order="F"), zg.ravel(order="F")], 1)  # :58-59
-    cp = np.round(box[:, 1] - box[:, 0]) / 2 + box[:, 0]                             # :61
+    cp = G.mround(box[:, 1] - box[:, 0]) / 2 + box[:, 0]                             # :61
     dis = np.sqrt(((vox - cp[None, :]) ** 2).sum(1))
     vox = vox[dis <= Box_L]                                                          # :66
     rows = _voxel_rows(I, Imask, DisMedian, vox)
@@ -166,7 +166,7 @@ def grow_indexed_region_cuda(I, Imask, DisMedian, Ninter, pos_indices, Spot_L, d
         cpos = np.add.accumulate(np.concatenate([cpos[None], c[:, None] * idx]), axis=0)[-1]
     center1 = cpos / csum                                                            # :144
     if np.sqrt(((center1 - center0) ** 2).sum()) > max(maxD, maxD / 10000 * len(idx)):
-        center, replace_center = np.round(center1), 1
+        center, replace_center = G.mround(center1), 1
     else:
         center, replace_center = center0, 0
     return J, Completeness_out, DisMedian_out, Ninter_out, center, replace_center, idx
@@ -312,7 +312,7 @@ def best_first_growth(score, I, Imask, DisMedian, Ninter, pos_indices, drop_off,
     idx = np.argwhere(Jb.transpose(2, 1, 0))[:, ::-1] + 1
     center1 = cpos / csum
     if np.sqrt(((center1 - center0) ** 2).sum()) > max(maxD, maxD / 10000 * len(idx)):
-        center, replace_center = np.round(center1), 1
+        center, replace_center = G.mround(center1), 1
     else:
         center, replace_center = center0, 0
     return Jb, C_out, D_out, N_out, center, replace_center, idx

@@ -126,6 +126,12 @@ def theta_max_deg(lsd, detysize, pxy, detzsize, pxz) -> float:
     return math.degrees(math.acos(c)) / 2.0
 
 
+def mround(x):
+    """MATLAB ``round``: halves away from zero (numpy's ``round`` takes them to even)."""
+    x = np.asarray(x, np.float64)
+    return np.sign(x) * np.floor(np.abs(x) + 0.5)
+
+
 def quat_to_u(q: Sequence[float]) -> np.ndarray:
     """Active rotation matrix from a quaternion (q0,q1,q2,q3) (quaternion2U.m:3-28)."""
     q0, q1, q2, q3 = (float(x) for x in q)

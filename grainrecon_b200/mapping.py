@@ -18,6 +18,8 @@ import math
 
 import numpy as np
 
+from . import geometry as G
+
 SEED_VOL_MIN = [v ** 3 for v in (45, 40, 35, 30, 25, 22, 19, 16, 13, 10, 6, 3)]  # generate_seeding_indexing_pos.m:2
 
 
@@ -40,22 +42,22 @@ def generate_seeding_indexing_pos(it: int, allVoxel_indices, tomo_scale, VoxSize
     allv = np.asarray(allVoxel_indices, np.int64).reshape(-1, 3)
     seed_vol_min = SEED_VOL_MIN[min(it, len(SEED_VOL_MIN)) - 1]
     total = len(allv)
-    seed_nr = int(np.round(total / seed_vol_min))
+    seed_nr = int(G.mround(total / seed_vol_min))
     if seed_nr < 1:
-        seed_nr = int(np.round(total / 8))
+        seed_nr = int(G.mround(total / 8))
     elif seed_nr > 10000:
         seed_nr = 10000
     dseed = (3 * seed_vol_min / (4 * math.pi)) ** (1 / 3) * 2
     dmin = max(0.25 * dseed, 3.0)
     allv = allv[rng.permutation(total)]
     if seed_nr < 1000:
-        sampling_nr = min(int(np.round(seed_nr)), total)
+        sampling_nr = min(int(G.mround(seed_nr)), total)
     elif seed_nr < 5000:
-        sampling_nr = min(int(np.round(seed_nr / 3)), total)
+        sampling_nr = min(int(G.mround(seed_nr / 3)), total)
     elif seed_nr < 8000:
-        sampling_nr = min(int(np.round(seed_nr / 6)), total)
+        sampling_nr = min(int(G.mround(seed_nr / 6)), total)
     else:
-        sampling_nr = min(int(np.round(seed_nr / 50)), total)
+        sampling_nr = min(int(G.mround(seed_nr / 50)), total)
     sample = allv[:sampling_nr]
     seeds = [sample[0]]
     temp = []

@@ -115,3 +115,10 @@ def test_init_ds_marks_the_sample():
     assert DS["VisitFlag"][m > 0].min() == 0 and DS["VisitFlag"][m == 0].max() == -1
     assert DS["Dismedian"][m > 0].min() == 20 and DS["Dismedian"][m == 0].max() == 10
     assert DS["EulerZXZ"].shape == (3, 5, 6, 7)
+
+
+def test_matlab_round_halves_away_from_zero():
+    """round(...) in grow_indexed_region.m:132 and generate_seeding_indexing_pos.m:17-37 takes
+    halves away from zero; numpy's round would take them to even."""
+    np.testing.assert_array_equal(G.mround([0.5, 1.5, 2.5, -0.5, -2.5, 2.4999, 3.0]), [1, 2, 3, -1, -3, 2, 3])
+    assert not np.array_equal(np.round([0.5, 2.5]), G.mround([0.5, 2.5]))
