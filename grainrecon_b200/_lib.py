@@ -31,7 +31,11 @@ EXPORTS = [
     "grc_fit_spot_count", "grc_fit_spot_fill", "grc_centroid_residual_adjoint", "grc_fit_grains_lm",
     "grc_fit_grains_nm", "grc_fit_grains_rms", "grc_fit_geometry_lm", "grc_fit_geometry_cost",
     "grc_fit_geometry_rms", "grc_score_trials_device", "grc_fit_orientation_nm", "grc_pair_spots",
+    "grc_walk_best_first", "grc_grow_best_first",
 ]
+
+# grc_walk_score_fn of the C header
+WALK_SCORE_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.POINTER(C.c_int32), C.c_int64, C.POINTER(C.c_double))
 
 # grc_spot_pair of the C header
 PAIR_DTYPE = np.dtype([("trial", "<i4"), ("iw", "<i4"), ("ih", "<i4"), ("spot", "<i4"), ("dety", "<f8"),
@@ -115,6 +119,10 @@ def load(path: str | None = None):
         "grc_score_trials_device": [vp, f, i64, f, i64, f, f, i64, f],
         "grc_fit_orientation_nm": [vp, f, f, i64, d, i, i, d, d, f, f, f, f, f],
         "grc_pair_spots": [vp, f, f, i64, f, i64, f, f, i64, C.POINTER(i64)],
+        "grc_walk_best_first": [WALK_SCORE_FN, vp, i64, i64, i64, f, f, f, f, f, d, d, d, d, f, f, f, f, f, i64,
+                                C.POINTER(i64), f, C.POINTER(i)],
+        "grc_grow_best_first": [vp, i64, i64, i64, f, f, f, f, f, d, d, d, d, f, f, f, f, f, f, f, f, f, f, f, f,
+                                f, f, i64, C.POINTER(i64), f, C.POINTER(i)],
     }
     for name, args in sig.items():
         fn = getattr(L, name)
@@ -143,6 +151,58 @@ def _ptr(a):
     if isinstance(a, int):
         return a
     raise TypeError(f"cannot take the address of {type(a)}")
+
+
+def _walk_arrays(I, Imask, DisMedian, Ninter):
+    """X x Y x Z maps (numpy index order) as MATLAB-order doubles, plus output buffers."""
+    I = np.asarray(I, np.float64)
+    X, Y, Z = I.shape
+    col = lambda a: np.ascontiguousarray(np.asarray(a, np.float64).reshape(X, Y, Z).transpose(2, 1, 0))
+    ins = [col(I), col(Imask), col(DisMedian), col(Ninter)]
+    outs = [np.empty((Z, Y, X)) for _ in range(3)] + [np.empty((Z, Y, X), np.uint8)]
+    cap = int((ins[1] > 0).sum()) + 1
+    return (X, Y, Z), ins, outs, np.empty(cap, np.int64), cap
+
+
+def _walk_result(dims, outs, idx, n, center, rc):
+    """(J, Completeness_out, DisMedian_out, Ninter_out, center, replace_center, indexed_indices)."""
+    X, Y, Z = dims
+    C_out, D_out, N_out, J = (a.transpose(2, 1, 0) for a in outs)
+    k = idx[:n] - 1
+    ind = np.stack([k % X + 1, (k // X) % Y + 1, k // (X * Y) + 1], 1)
+    return J.astype(bool), C_out, D_out, N_out, center, int(rc.value), ind
+
+
+def walk_best_first(score, I, Imask, DisMedian, Ninter, seed, drop_off, maxD, indexed_comp, maxDmedian):
+    """grow_indexed_region.m's region walk in the library with a Python scorer: ``score(vox)``
+    maps (k x 3) 1-based voxel indices to (k x 3) [Nr_simu, Nr_intersect, dis_median].  Maps are
+    X x Y x Z arrays in numpy index order.  Returns (J, Completeness_out, DisMedian_out,
+    Ninter_out, center, replace_center, indexed_indices) as grow_indexed_region.m does."""
+    L = load()
+    dims, ins, outs, idx, cap = _walk_arrays(I, Imask, DisMedian, Ninter)
+    err = []
+
+    def cb(user, vox, n, out):
+        try:
+            v = np.ctypeslib.as_array(vox, shape=(n * 3,)).reshape(n, 3).astype(np.int64)
+            r = np.asarray(score(v), np.float64).reshape(n, 3)
+            np.ctypeslib.as_array(out, shape=(n * 3,))[:] = r.reshape(-1)
+            return GRC_OK
+        except Exception as e:  # noqa: BLE001 -- re-raised after the walk returns
+            err.append(e)
+            return GRC_EINVAL
+
+    fn = WALK_SCORE_FN(cb)
+    sd = np.asarray(seed, np.int32).reshape(3)
+    n, center, rc = C.c_int64(), np.zeros(3), C.c_int()
+    code = L.grc_walk_best_first(fn, None, *dims, *[_ptr(a) for a in ins], _ptr(sd), float(drop_off), float(maxD),
+                                 float(indexed_comp), float(maxDmedian), *[_ptr(a) for a in outs], _ptr(idx), cap,
+                                 C.byref(n), _ptr(center), C.byref(rc))
+    if err:
+        raise err[0]
+    if code != GRC_OK:
+        raise GrcError(code, "walk_best_first")
+    return _walk_result(dims, outs, idx, n.value, center, rc)
 
 
 def f32(a) -> np.ndarray:
@@ -235,6 +295,21 @@ class Context:
         self._check(self.L.grc_forward_comp(self.h, p[0], p[1], n, p[2], p[3], p[4], p[5], p[6], p[7], p[8],
                                             _ptr(out)))
         return out
+
+    def grow_best_first(self, I, Imask, DisMedian, Ninter, seed, drop_off, maxD, indexed_comp, maxDmedian, U, S,
+                        B, hkl, proj_bin_bw, rot_angles, RotDet, param, param1):
+        """grow_indexed_region.m's region walk on the GPU scorer (grc_grow_best_first); returns
+        (J, Completeness_out, DisMedian_out, Ninter_out, center, replace_center, indexed_indices)."""
+        dims, ins, outs, idx, cap = _walk_arrays(I, Imask, DisMedian, Ninter)
+        sd = np.asarray(seed, np.int32).reshape(3)
+        pb = None if proj_bin_bw is None else f32(proj_bin_bw)
+        keep = [f32(U), f32(S), f32(B), f32(hkl), pb, f32(rot_angles), f32(RotDet), f32(param), f32(param1)]
+        n, center, rc = C.c_int64(), np.zeros(3), C.c_int()
+        self._check(self.L.grc_grow_best_first(self.h, *dims, *[_ptr(a) for a in ins], _ptr(sd), float(drop_off),
+                                               float(maxD), float(indexed_comp), float(maxDmedian),
+                                               *[_ptr(a) for a in keep], *[_ptr(a) for a in outs], _ptr(idx), cap,
+                                               C.byref(n), _ptr(center), C.byref(rc)))
+        return _walk_result(dims, outs, idx, n.value, center, rc)
 
     def grow_indexed_region(self, rows6, U, S, B, hkl, proj_bin_bw, rot_angles, RotDet, param, param1, out=None):
         """cuda_grow_indexed_region: returns 7*m floats [x y z Nr_simu Nr_intersect dis_median flag]."""

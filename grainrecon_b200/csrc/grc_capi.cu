@@ -626,6 +626,114 @@ int grc_grow_indexed_region(grc_ctx *ctx, const float *rows6, int64_t m, const f
     return GRC_OK;
 }
 
+namespace {
+
+// Per-voxel score cache of a best-first walk for one orientation.  A request with unscored
+// voxels scores, in one grc_grow_indexed_region call, every unscored in-mask voxel of the box
+// that reaches kWalkHalo voxels beyond the unscored ones (and those themselves): the walk then
+// makes one GPU call per few thousand voxels instead of one per step, with the same values.
+constexpr int64_t kWalkHalo = 6;
+
+struct WalkCache {
+    grc_ctx *ctx;
+    int64_t X, Y, Z;
+    const double *mask;
+    const float *U, *S, *B, *hkl, *map, *rot, *R, *param, *param1;
+    std::vector<uint8_t> have;  // 0 unscored, 1 scored, 2 queued for this call
+    std::vector<float> val;     // 3 per voxel: Nr_simu Nr_intersect dis_median
+    std::vector<int32_t> todo;
+    std::vector<float> rows, out;
+
+    int64_t lin(int64_t x, int64_t y, int64_t z) const { return (x - 1) + X * ((y - 1) + Y * (z - 1)); }
+
+    static int score(void *user, const int32_t *vox, int64_t n, double *res) {
+        WalkCache &c = *static_cast<WalkCache *>(user);
+        int64_t lo[3] = {INT64_MAX, INT64_MAX, INT64_MAX}, hi[3] = {0, 0, 0};
+        bool miss = false;
+        for (int64_t j = 0; j < n; ++j) {
+            if (c.have[c.lin(vox[3 * j], vox[3 * j + 1], vox[3 * j + 2])]) continue;
+            miss = true;
+            for (int d = 0; d < 3; ++d) {
+                lo[d] = std::min<int64_t>(lo[d], vox[3 * j + d]);
+                hi[d] = std::max<int64_t>(hi[d], vox[3 * j + d]);
+            }
+        }
+        if (miss) {
+            const int64_t dims[3] = {c.X, c.Y, c.Z};
+            for (int d = 0; d < 3; ++d) {
+                lo[d] = std::max<int64_t>(lo[d] - kWalkHalo, 1);
+                hi[d] = std::min<int64_t>(hi[d] + kWalkHalo, dims[d]);
+            }
+            c.todo.clear();
+            auto queue = [&](int64_t x, int64_t y, int64_t z) {
+                c.have[c.lin(x, y, z)] = 2;
+                c.todo.push_back((int32_t)x);
+                c.todo.push_back((int32_t)y);
+                c.todo.push_back((int32_t)z);
+            };
+            for (int64_t z = lo[2]; z <= hi[2]; ++z)
+                for (int64_t y = lo[1]; y <= hi[1]; ++y)
+                    for (int64_t x = lo[0]; x <= hi[0]; ++x) {
+                        const int64_t k = c.lin(x, y, z);
+                        if (!c.have[k] && c.mask[k] > 0) queue(x, y, z);
+                    }
+            for (int64_t j = 0; j < n; ++j)  // requested voxels outside the mask too
+                if (!c.have[c.lin(vox[3 * j], vox[3 * j + 1], vox[3 * j + 2])])
+                    queue(vox[3 * j], vox[3 * j + 1], vox[3 * j + 2]);
+            const int64_t m = (int64_t)c.todo.size() / 3;
+            c.rows.assign(6 * m, 0.f);
+            c.out.resize(7 * m);
+            for (int64_t i = 0; i < m; ++i)
+                for (int d = 0; d < 3; ++d) c.rows[6 * i + d] = (float)c.todo[3 * i + d];
+            const int rc = grc_grow_indexed_region(c.ctx, c.rows.data(), m, c.U, c.S, c.B, c.hkl, c.map, c.rot, c.R,
+                                                   c.param, c.param1, c.out.data());
+            if (rc != GRC_OK) return rc;
+            c.map = nullptr;  // resident after the first call
+            for (int64_t i = 0; i < m; ++i) {
+                const int64_t k = c.lin(c.todo[3 * i], c.todo[3 * i + 1], c.todo[3 * i + 2]);
+                for (int d = 0; d < 3; ++d) c.val[3 * k + d] = c.out[7 * i + 3 + d];
+                c.have[k] = 1;
+            }
+        }
+        for (int64_t j = 0; j < n; ++j) {
+            const int64_t k = c.lin(vox[3 * j], vox[3 * j + 1], vox[3 * j + 2]);
+            for (int d = 0; d < 3; ++d) res[3 * j + d] = (double)c.val[3 * k + d];
+        }
+        return GRC_OK;
+    }
+};
+
+int fail_locked(grc_ctx *ctx, int code, const char *what) {
+    Lock l(ctx);
+    return fail(ctx, code, "%s", what);
+}
+
+}  // namespace
+
+int grc_grow_best_first(grc_ctx *ctx, int64_t X, int64_t Y, int64_t Z, const double *I, const double *Imask,
+                        const double *DisMedian, const double *Ninter, const int32_t seed[3], double drop_off,
+                        double maxD, double indexed_comp, double maxDmedian, const float *U, const float *S,
+                        const float *B, const float *hkl, const float *map, const float *rot, const float *R,
+                        const float *param, const float *param1, double *C_out, double *D_out, double *N_out,
+                        uint8_t *J_out, int64_t *idx_out, int64_t idx_cap, int64_t *n_idx, double center[3],
+                        int *replace_center) {
+    if (!ctx) return GRC_EINVAL;
+    // no context lock here: every block of scores is one grc_grow_indexed_region call, which
+    // takes it
+    if (!Imask || !U || !param1) return fail_locked(ctx, GRC_EINVAL, "grow_best_first: NULL argument");
+    if (X < 1 || Y < 1 || Z < 1 || X > INT32_MAX || Y > INT32_MAX || Z > INT32_MAX || X * Y > INT64_MAX / Z)
+        return fail_locked(ctx, GRC_EINVAL, "grow_best_first: bad volume size");
+    WalkCache c{ctx, X, Y, Z, Imask, U, S, B, hkl, map, rot, R, param, param1};
+    c.have.assign((size_t)(X * Y * Z), 0);
+    c.val.assign((size_t)(3 * X * Y * Z), 0.f);
+    const int rc = grc_walk_best_first(&WalkCache::score, &c, X, Y, Z, I, Imask, DisMedian, Ninter, seed, drop_off,
+                                       maxD, indexed_comp, maxDmedian, C_out, D_out, N_out, J_out, idx_out, idx_cap,
+                                       n_idx, center, replace_center);
+    if (rc == GRC_EINVAL) return fail_locked(ctx, GRC_EINVAL, "grow_best_first: NULL map or seed outside the volume");
+    if (rc == GRC_ECAPACITY) return fail_locked(ctx, GRC_ECAPACITY, "grow_best_first: more grown voxels than idx_cap");
+    return rc;  // a scorer error was recorded by grc_grow_indexed_region
+}
+
 int grc_forward_comp_compete(grc_ctx *ctx, const float *rows5, int64_t m, const float *id_neigb, int64_t n_neigb,
                              const float *euler, int64_t n_grain, const float *S, const float *B, const float *hkl,
                              const float *map, const float *rot, const float *R, const float *param,

@@ -235,149 +235,23 @@ def grow_unindexed_compete_comp_cuda(DS_in, wait_revising_voxels, id_neigb_all, 
     return DS_out, out
 
 
-_NEIGB = np.array([[1, 1, 0], [1, -1, 0], [1, 0, 1], [1, 0, -1], [1, 0, 0], [0, 1, 0], [0, -1, 0], [0, 1, 1],
-                   [0, 0, 1], [0, -1, 1], [0, 1, -1], [0, 0, -1], [0, -1, -1], [-1, 1, 0], [-1, -1, 0], [-1, 0, 1],
-                   [-1, 0, -1], [-1, 0, 0]], np.int64)  # grow_indexed_region.m:26-29, 18 neighbours
-
-
-def best_first_growth(score, I, Imask, DisMedian, Ninter, pos_indices, drop_off, maxD, indexed_comp, maxDmedian):
-    """The region walk of grow_indexed_region.m:6-137 with a pluggable scorer.
-
-    ``score(vox)`` maps (k x 3) 1-based voxel indices to rows [Nr_simu, Nr_intersect, dis_median].
-    From the current voxel every unvisited in-mask neighbour is scored (one batch per step; the
-    scores do not depend on the region) and kept when it beats the map -- ``C > I`` with
-    ``dis_median <= min(DisMedian, maxDmedian)``, or ``|C - I| <= 0.01`` with more
-    intersections than ``Ninter`` (:50-52).  The walk then moves to the best kept voxel while its
-    completeness stays above ``seed_comp * (1 - drop_off)``.  Returns (J, Completeness_out,
-    DisMedian_out, Ninter_out, center, replace_center, indexed_indices)."""
-    I = np.array(I, dtype=np.float64, copy=True)
-    x, y, z = (int(p) for p in pos_indices)
-    I[x - 1, y - 1, z - 1] = indexed_comp
-    J = np.zeros(I.shape, np.int8)
-    C_out = I.copy()
-    D_out = np.array(DisMedian, dtype=np.float64, copy=True)
-    N_out = np.array(Ninter, dtype=np.float64, copy=True)
-    dims = np.array(I.shape)
-    seed_comp = I[x - 1, y - 1, z - 1]
-    csum = seed_comp
-    cpos = seed_comp * np.array([x, y, z], np.float64)
-    center0 = cpos / csum
-    n_mask = int((np.asarray(Imask) > 0).sum())
-    neg = np.empty((64, 6))  # kept voxels [x y z C dis_median Nr_intersect], first n rows live
-    n = 0
-    reg_size = 0
-    Imask = np.asarray(Imask)
-    D_in, N_in = np.asarray(DisMedian, np.float64), np.asarray(Ninter, np.float64)
-    while True:
-        nb = np.array([x, y, z]) + _NEIGB
-        ins = np.all((nb >= 1) & (nb <= dims), axis=1)
-        nb = nb[ins]
-        keep = (J[tuple((nb - 1).T)] == 0) & (Imask[tuple((nb - 1).T)] > 0)
-        nb = nb[keep]
-        if len(nb):
-            r = np.asarray(score(nb), np.float64).reshape(-1, 3)
-            with np.errstate(invalid="ignore", divide="ignore"):
-                c = r[:, 1] / r[:, 0]
-            ix = tuple((nb - 1).T)
-            i0, d0, n0 = I[ix], D_in[ix], N_in[ix]
-            ok = ((c > i0) & (r[:, 2] <= np.minimum(d0, maxDmedian))) | ((np.abs(c - i0) <= 0.01) & (r[:, 1] > n0))
-            k = np.nonzero(ok)[0]
-            if len(k):
-                if n + len(k) > len(neg):
-                    neg = np.concatenate([neg, np.empty((max(len(neg), len(k)), 6))])
-                neg[n:n + len(k), :3] = nb[k]
-                neg[n:n + len(k), 3] = c[k]
-                neg[n:n + len(k), 4] = r[k, 2]
-                neg[n:n + len(k), 5] = r[k, 1]
-                n += len(k)
-                J[tuple((nb[k] - 1).T)] = 1
-        J[x - 1, y - 1, z - 1] = 2
-        if n == 0:
-            break
-        dist = neg[:n, 3] / seed_comp
-        index = int(np.nanargmax(dist))
-        reg_size += 1
-        if dist[index] > 1 - drop_off and reg_size < n_mask - 1:
-            e = neg[index].copy()
-            csum += e[3]
-            cpos += e[3] * e[:3]
-            xi, yi, zi = (int(v) - 1 for v in e[:3])
-            C_out[xi, yi, zi], D_out[xi, yi, zi], N_out[xi, yi, zi] = e[3], e[4], e[5]
-            x, y, z = xi + 1, yi + 1, zi + 1
-            neg[index] = neg[n - 1]  # the last kept voxel takes the chosen one's place
-            n -= 1
-        else:
-            break
-    Jb = J > 1
-    idx = np.argwhere(Jb.transpose(2, 1, 0))[:, ::-1] + 1
-    center1 = cpos / csum
-    if np.sqrt(((center1 - center0) ** 2).sum()) > max(maxD, maxD / 10000 * len(idx)):
-        center, replace_center = G.mround(center1), 1
-    else:
-        center, replace_center = center0, 0
-    return Jb, C_out, D_out, N_out, center, replace_center, idx
-
-
 def grow_indexed_region(I, Imask, DisMedian, Ninter, pos_indices, drop_off, maxD, indexed_comp, UU, proj_bin_bw,
                         rot_angles, S, B, Ahkl, nrhkl, RotDet, thetamax, lambda_min, lambda_max, Lsam2sou, Lsam2det,
                         minEucDis, dety00, detz00, P0y, P0z, RotAxisOffset, pixelysize, pixelzsize, dety0, detz0,
                         detysize, detzsize, BeamStopY, BeamStopZ, RecVolumePixel, tomo_scale, VoxSize,
                         simap_data_flag, maxDmedian):
-    """grow_indexed_region.m:1-145: best-first growth from the seed voxel, each step's neighbours
-    scored on the GPU in one call.  ``minEucDis``, ``dety0`` and ``detz0`` must equal the scorer's
-    options (0.5 px threshold, detector centre)."""
+    """grow_indexed_region.m:1-145: best-first growth from the seed voxel in the library's native
+    walk (grc_grow_best_first), its voxels scored on the GPU a block at a time.  ``minEucDis``,
+    ``dety0`` and ``detz0`` must equal the scorer's options (0.5 px threshold, detector centre).
+    Returns (J, Completeness_out, DisMedian_out, Ninter_out, center, replace_center,
+    indexed_indices)."""
     hkl = _hkl(Ahkl, nrhkl)
     param = _param(hkl.shape[0], len(rot_angles), Lsam2sou, Lsam2det, P0y, P0z, dety00, detz00, pixelysize,
                    pixelzsize, detysize, detzsize, BeamStopY, BeamStopZ, thetamax, lambda_min, lambda_max,
                    RotAxisOffset)
     param1 = np.array([*np.asarray(RecVolumePixel)[:, 0], simap_data_flag, VoxSize, *tomo_scale["Center"],
                        *tomo_scale["Dimension"], 0, 0, maxDmedian], dtype=np.float32)
-    ctx = context()
-    args = (G.flat_rowmajor(UU), G.flat_rowmajor(S), G.flat_rowmajor(B), G.flat_hkl(hkl))
-    first = [_map_for_call(proj_bin_bw)]
-
-    def score_rows(vox):
-        rows = np.zeros((len(vox), 6), np.float32)
-        rows[:, :3] = vox
-        out = ctx.grow_indexed_region(rows, *args, first[0], np.asarray(rot_angles, np.float32),
-                                      G.flat_rowmajor(RotDet), param, param1).reshape(-1, 7)
-        first[0] = None  # the map stays resident after the first call
-        return out[:, 3:6]
-
-    return best_first_growth(BlockScorer(score_rows, Imask), I, Imask, DisMedian, Ninter, pos_indices, drop_off,
-                             maxD, indexed_comp, maxDmedian)
-
-
-class BlockScorer:
-    """Memoised voxel scorer for one orientation.
-
-    A voxel's [Nr_simu, Nr_intersect, dis_median] depends only on the voxel and U, not on the
-    region grown so far, so the walk may read it from a cache.  A request with unscored voxels
-    scores, in one GPU call, every unscored in-mask voxel of the box that reaches ``halo`` voxels
-    beyond the requested ones: the walk then makes one call per few thousand voxels instead of
-    one per step, with the same values."""
-
-    def __init__(self, score_rows, Imask, halo: int = 6):
-        self.score_rows = score_rows
-        self.mask = np.asarray(Imask) > 0
-        self.have = np.zeros(self.mask.shape, bool)
-        self.val = np.zeros(self.mask.shape + (3,), np.float64)
-        self.halo = halo
-        self.calls = 0
-
-    def __call__(self, vox):
-        vox = np.asarray(vox, np.int64).reshape(-1, 3)
-        ix = tuple((vox - 1).T)
-        miss = ~self.have[ix]
-        if miss.any():
-            m = vox[miss]
-            lo = np.maximum(m.min(axis=0) - self.halo, 1)
-            hi = np.minimum(m.max(axis=0) + self.halo, self.mask.shape)
-            box = tuple(slice(a - 1, b) for a, b in zip(lo, hi))
-            todo = self.mask[box] & ~self.have[box]
-            blk = np.argwhere(todo) + lo
-            blk = np.unique(np.concatenate([blk, m]), axis=0)  # requested voxels outside the mask too
-            self.val[tuple((blk - 1).T)] = np.asarray(self.score_rows(blk), np.float64).reshape(-1, 3)
-            self.have[tuple((blk - 1).T)] = True
-            self.calls += 1
-        return self.val[ix]
+    return context().grow_best_first(I, Imask, DisMedian, Ninter, pos_indices, drop_off, maxD, indexed_comp,
+                                     maxDmedian, G.flat_rowmajor(UU), G.flat_rowmajor(S), G.flat_rowmajor(B),
+                                     G.flat_hkl(hkl), _map_for_call(proj_bin_bw), np.asarray(rot_angles, np.float32),
+                                     G.flat_rowmajor(RotDet), param, param1)

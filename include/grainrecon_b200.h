@@ -110,6 +110,48 @@ int grc_grow_indexed_region(grc_ctx *ctx, const float *rows6, int64_t m, const f
                             const float *RotDet, const float *param, const float *param1, float *out);
 
 /*
+ * Scores of voxels for a best-first walk: vox holds 3*n 1-based (x, y, z); out receives 3*n
+ * doubles [Nr_simu Nr_intersect dis_median].  Returns GRC_OK or an error code that ends the
+ * walk.
+ */
+typedef int (*grc_walk_score_fn)(void *user, const int32_t *vox, int64_t n, double *out);
+
+/*
+ * Replaces the region walk of grow_indexed_region.m:32-137 (the CPU path's growth, which the
+ * GPU engine uses for spots of at most 2 pixels, GrainMapping_engine_gpu_comp.m), with the
+ * scores from `score`.  Maps are X x Y x Z doubles in MATLAB order (x fastest): I
+ * (completeness), Imask (> 0 = sample), DisMedian, Ninter; seed: 1-based (x, y, z).  From the
+ * current voxel every unvisited in-mask neighbour of the 18 of :50-52 is scored and kept when
+ * C > I with dis_median <= min(DisMedian, maxDmedian), or |C - I| <= 0.01 with more
+ * intersections than Ninter (:78-79); the walk moves to the first kept voxel of highest C while
+ * C / seed_comp > 1 - drop_off.  Out: C_out, D_out, N_out (the input maps with the seed's
+ * completeness set to indexed_comp and each grown voxel's values), J_out (1 = grown), idx_out
+ * the grown voxels' 1-based linear indices in find() order (*n_idx of them; GRC_ECAPACITY when
+ * more than idx_cap, with *n_idx the count needed), center and replace_center of :131-137.
+ */
+int grc_walk_best_first(grc_walk_score_fn score, void *user, int64_t X, int64_t Y, int64_t Z, const double *I,
+                        const double *Imask, const double *DisMedian, const double *Ninter, const int32_t seed[3],
+                        double drop_off, double maxD, double indexed_comp, double maxDmedian, double *C_out,
+                        double *D_out, double *N_out, uint8_t *J_out, int64_t *idx_out, int64_t idx_cap,
+                        int64_t *n_idx, double center[3], int *replace_center);
+
+/*
+ * grow_indexed_region.m:1-145 on the GPU scorer: grc_walk_best_first with the voxels scored by
+ * the grc_grow_indexed_region kernels for orientation U (9 floats row-major) and the geometry
+ * arguments of that entry (param1: its 14 floats; only the first 11, which place voxels, are
+ * used).  A voxel's score for one U does not depend on the region, so scores are cached: a
+ * request with unscored voxels scores every unscored in-mask voxel of the box reaching 6 voxels
+ * beyond them in one kernel call.  proj_bin_bw may be NULL when a map is resident.
+ */
+int grc_grow_best_first(grc_ctx *ctx, int64_t X, int64_t Y, int64_t Z, const double *I, const double *Imask,
+                        const double *DisMedian, const double *Ninter, const int32_t seed[3], double drop_off,
+                        double maxD, double indexed_comp, double maxDmedian, const float *U, const float *S,
+                        const float *B, const float *hkl, const float *proj_bin_bw, const float *rot_angles,
+                        const float *RotDet, const float *param, const float *param1, double *C_out, double *D_out,
+                        double *N_out, uint8_t *J_out, int64_t *idx_out, int64_t idx_cap, int64_t *n_idx,
+                        double center[3], int *replace_center);
+
+/*
  * Replaces cuda_forward_comp_compete(rows5, id_neigb_all, Euler, S, B, hkl,
  * proj_bin_bw, rot_angles, RotDet, param, param1) called at
  * grow_unindexed_compete_comp_cuda.m:39-41.  rows5: 5*m floats [x y z first

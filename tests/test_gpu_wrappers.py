@@ -7,7 +7,9 @@ import pytest
 from grainrecon_b200 import forward as FW
 from grainrecon_b200 import geometry as G
 from grainrecon_b200 import synth
+from grainrecon_b200._lib import GRC_EINVAL, GrcError
 from oracle import oracle as O
+from oracle import walk_oracle as WO
 
 pytestmark = pytest.mark.gpu
 
@@ -146,8 +148,9 @@ def test_compete(scene):
 
 
 def test_best_first_growth_matches_oracle_walk(scene):
-    """grow_indexed_region (the CPU-path growth) on the GPU scorer against the same walk scored by
-    the oracle: identical regions, maps and centre unless the oracle met an edge reflection."""
+    """grow_indexed_region (the CPU-path growth: the library's native walk on the GPU scorer)
+    against the oracle's numpy walk scored by the FP64 oracle: identical regions, maps and centre
+    unless the oracle met an edge reflection."""
     s, dmap, pbb = scene
     g = s.geom
     dims = s.grain_id.shape
@@ -177,7 +180,7 @@ def test_best_first_growth_matches_oracle_walk(scene):
         edges_seen[0] += int(edges.sum())
         return out.reshape(-1, 7)[:, 3:6]
 
-    ref = FW.best_first_growth(oracle_score, I, Imask, Dm, Ni, seed, 0.05, 3, 0.95, 10)
+    ref = WO.best_first_growth(oracle_score, I, Imask, Dm, Ni, seed, 0.05, 3, 0.95, 10)
     J, C, D, N, center, rc, grown = gpu
     assert J[tuple(seed - 1)] and len(grown) > 5
     if edges_seen[0] == 0:
@@ -193,3 +196,23 @@ def test_best_first_growth_matches_oracle_walk(scene):
         assert ref[0][tuple(seed - 1)]
         jac = (J & ref[0]).sum() / (J | ref[0]).sum()
         assert jac > 0.9, (jac, edges_seen[0])
+
+
+def test_native_walk_refuses_a_seed_outside_the_volume(scene):
+    s, dmap, pbb = scene
+    g = s.geom
+    dims = s.grain_id.shape
+    ts, rvp = _tomo(s)
+    S9, B9, hkl, rot, R9, p = s.mex_arrays()
+    Imask = (s.grain_id > 0).astype(np.float64)
+    p1 = s.vol.param14(0, 0, 10)
+    ctx = FW.context()
+    with pytest.raises(GrcError) as e:
+        ctx.grow_best_first(np.zeros(dims), Imask, np.zeros(dims) + 20, np.zeros(dims), (dims[0] + 1, 1, 1), 0.05,
+                            3, 0.95, 10, G.flat_rowmajor(np.eye(3)), S9, B9, hkl, None, rot, R9, p, p1)
+    assert e.value.code == GRC_EINVAL
+    seed = s.voxel_indices()[0]  # the context stays usable
+    out = ctx.grow_best_first(np.zeros(dims), Imask, np.zeros(dims) + 20, np.zeros(dims), seed, 0.05, 3, 0.95, 10,
+                              G.flat_rowmajor(G.quat_to_u(s.grain_q[s.grain_id[tuple(seed - 1)] - 1])), S9, B9, hkl,
+                              None, rot, R9, p, p1)
+    assert out[0][tuple(seed - 1)] and len(out[6]) >= 1
