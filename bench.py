@@ -506,6 +506,80 @@ def run_seed(args):
     return 0
 
 
+def run_walk(args):
+    """Best-first region growth (grow_indexed_region.m:32-137) of the three largest grains of the FCC
+    Al sample, through grc_grow_best_first with host arrays: the native walk, its voxels scored
+    on the GPU a block at a time."""
+    import torch
+    from grainrecon_b200 import geometry as G
+    from grainrecon_b200 import synth
+    from grainrecon_b200._lib import Context
+
+    rank, world, local = env_rank()
+    torch.cuda.set_device(local)
+    s = synth.make_sample("al400", seed=args.seed)
+    ctx = Context(local)
+    host = synth.device_maps(s, ctx, keep_host_map=not args.no_cpu_baseline)
+    S9, B9, hkl, rot, R9, p = s.mex_arrays()
+    dims = s.grain_id.shape
+    Imask = (s.grain_id > 0).astype(np.float64)
+    idx = s.voxel_indices()
+    gid = s.grain_id[tuple((idx - 1).T)]
+    sizes = np.bincount(gid)
+    grains = np.argsort(sizes)[::-1][:3]
+    p1 = s.vol.param14(0, 0, 10)
+    zeros, twenty = np.zeros(dims), np.zeros(dims) + 20
+    cases = []
+    for g in grains:
+        members = idx[gid == g]
+        cases.append((members[len(members) // 2], G.flat_rowmajor(G.quat_to_u(s.grain_q[g - 1]))))
+    walk = lambda seed, U: ctx.grow_best_first(zeros, Imask, twenty, zeros, seed, 0.05, 3, 0.95, 10, U, S9, B9,
+                                               hkl, None, rot, R9, p, p1)
+    walk(*cases[0])  # warm-up
+    with ClockSampler(local) as clk:
+        t0 = time.perf_counter()
+        grown = [len(walk(*c)[6]) for c in cases]
+        dt = time.perf_counter() - t0
+    line = {"metric": "best-first grown voxels/s", "value": sum(grown) / dt, "unit": "voxels/s", "n_gpus": 1,
+            "higher_is_better": True, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": (f"grow_indexed_region walk from the centre voxel of the 3 largest grains "
+                                    f"({', '.join(str(int(sizes[g])) for g in grains)} voxels) of FCC Al 400 grains, "
+                                    f"{int(Imask.sum())} voxels, 2048x2048 detector, 361 projections, drop_off 0.05")},
+            "clocks": clk.summary(), "grown": grown, "seconds": dt}
+    if rank == 0 and not args.no_cpu_baseline:
+        # the oracle walk with the FP64 oracle scorer, the first 300 steps of the first case
+        from oracle import oracle as O
+        from oracle import walk_oracle as WO
+        seed, U = cases[0]
+        steps = [0]
+
+        class Enough(Exception):
+            pass
+
+        def score(vox):
+            if steps[0] == 300:
+                raise Enough
+            steps[0] += 1
+            rows6 = np.zeros((len(vox), 6), np.float32)
+            rows6[:, :3] = vox
+            out, _ = O.grow(rows6, U, S9, B9, hkl, host, rot, R9, p, p1)
+            return out.reshape(-1, 7)[:, 3:6]
+
+        t0 = time.perf_counter()
+        try:
+            WO.best_first_growth(score, zeros, Imask, twenty, zeros, seed, 0.05, 3, 0.95, 10)
+        except Enough:
+            pass
+        per_step = (time.perf_counter() - t0) / steps[0]
+        line["cpu_baseline"] = {"value": 1.0 / per_step, "unit": "voxels/s", "cores": O.max_threads(),
+                                "kind": "port", "sample": (f"oracle walk + FP64 oracle scorer, first {steps[0]} steps "
+                                                           f"of the first grain (one voxel grown per step)")}
+    ctx.close()
+    if rank == 0:
+        print(json.dumps(line, default=float), flush=True)
+    return 0
+
+
 def run_map(args):
     """Whole mapping run of the BCC Fe sample (6 grains, 6,320 voxels, 1024x1024 detector, 181
     projections): GrainMapping_fun's iteration on the GPU engine from the masks alone."""
@@ -658,7 +732,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="al400", choices=["al400", "fe6", "al400-grow", "fe-fit", "al-geofit",
-                                                                "al400-seed", "fe6-map"])
+                                                                "al400-seed", "fe6-map", "al400-walk"])
     ap.add_argument("--map-iters", type=int, default=4, help="fe6-map: mapping iterations at most")
     ap.add_argument("--nr-seed", type=int, default=400, help="al400-seed: candidates refined per seed")
     ap.add_argument("--seed-batch", type=int, default=16, help="al400-seed: seeds per step")
@@ -685,6 +759,8 @@ def main():
         return run_seed(args)
     if args.config == "fe6-map":
         return run_map(args)
+    if args.config == "al400-walk":
+        return run_walk(args)
     return run_ours(args)
 
 
