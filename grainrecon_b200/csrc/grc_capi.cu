@@ -720,18 +720,21 @@ int grc_grow_best_first(grc_ctx *ctx, int64_t X, int64_t Y, int64_t Z, const dou
     if (!ctx) return GRC_EINVAL;
     // no context lock here: every block of scores is one grc_grow_indexed_region call, which
     // takes it
-    if (!Imask || !U || !param1) return fail_locked(ctx, GRC_EINVAL, "grow_best_first: NULL argument");
+    if (!I || !Imask || !DisMedian || !Ninter || !seed || !U || !param1 || !C_out || !D_out || !N_out || !J_out ||
+        !n_idx || !center || !replace_center || (idx_cap > 0 && !idx_out))
+        return fail_locked(ctx, GRC_EINVAL, "grow_best_first: NULL argument");
     if (X < 1 || Y < 1 || Z < 1 || X > INT32_MAX || Y > INT32_MAX || Z > INT32_MAX || X * Y > INT64_MAX / Z)
         return fail_locked(ctx, GRC_EINVAL, "grow_best_first: bad volume size");
+    if (seed[0] < 1 || seed[1] < 1 || seed[2] < 1 || seed[0] > X || seed[1] > Y || seed[2] > Z)
+        return fail_locked(ctx, GRC_EINVAL, "grow_best_first: seed outside the volume");
     WalkCache c{ctx, X, Y, Z, Imask, U, S, B, hkl, map, rot, R, param, param1};
     c.have.assign((size_t)(X * Y * Z), 0);
     c.val.assign((size_t)(3 * X * Y * Z), 0.f);
     const int rc = grc_walk_best_first(&WalkCache::score, &c, X, Y, Z, I, Imask, DisMedian, Ninter, seed, drop_off,
                                        maxD, indexed_comp, maxDmedian, C_out, D_out, N_out, J_out, idx_out, idx_cap,
                                        n_idx, center, replace_center);
-    if (rc == GRC_EINVAL) return fail_locked(ctx, GRC_EINVAL, "grow_best_first: NULL map or seed outside the volume");
     if (rc == GRC_ECAPACITY) return fail_locked(ctx, GRC_ECAPACITY, "grow_best_first: more grown voxels than idx_cap");
-    return rc;  // a scorer error was recorded by grc_grow_indexed_region
+    return rc;  // arguments were checked above: any other error is the scorer's, recorded by grc_grow_indexed_region
 }
 
 int grc_forward_comp_compete(grc_ctx *ctx, const float *rows5, int64_t m, const float *id_neigb, int64_t n_neigb,
