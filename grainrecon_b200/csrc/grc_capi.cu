@@ -101,6 +101,13 @@ bool is_device_ptr(const void *p) {
 
 bool is_int(float v) { return std::isfinite(v) && std::floor(v) == v; }
 
+// A *_device entry hands its buffers straight to kernels: a host pointer there would fault on
+// the GPU, so it is refused here.  NULL passes (the callers check NULL with their own message).
+int need_device(grc_ctx *ctx, const void *p, const char *what) {
+    if (p && !is_device_ptr(p)) return fail(ctx, GRC_EINVAL, "%s is not device memory", what);
+    return GRC_OK;
+}
+
 void refresh_hit(grc_ctx *ctx) {
     if (!ctx->has_masks) return;
     const double thr = ctx->opt_thr;
@@ -600,11 +607,12 @@ int grc_forward_comp(grc_ctx *ctx, const float *pos, const float *q, int64_t n_q
     return GRC_OK;
 }
 
-int grc_grow_indexed_region(grc_ctx *ctx, const float *rows6, int64_t m, const float *U, const float *S,
-                            const float *B, const float *hkl, const float *map, const float *rot, const float *R,
-                            const float *param, const float *param1, float *out) {
-    if (!ctx) return GRC_EINVAL;
-    Lock l(ctx);
+namespace {
+
+// grc_grow_indexed_region with the context lock already held by the caller.
+int grow_indexed_region_held(grc_ctx *ctx, const float *rows6, int64_t m, const float *U, const float *S,
+                             const float *B, const float *hkl, const float *map, const float *rot, const float *R,
+                             const float *param, const float *param1, float *out) {
     if (!U || !param1 || !out || (m > 0 && !rows6)) return fail(ctx, GRC_EINVAL, "grow: NULL argument");
     if (m < 0) return fail(ctx, GRC_EINVAL, "grow: negative row count");
     TRY(set_geometry(ctx, S, B, hkl, rot, R, param));
@@ -624,6 +632,16 @@ int grc_grow_indexed_region(grc_ctx *ctx, const float *rows6, int64_t m, const f
     CU(cudaStreamSynchronize(ctx->stream));
     CU(cudaGetLastError());
     return GRC_OK;
+}
+
+}  // namespace
+
+int grc_grow_indexed_region(grc_ctx *ctx, const float *rows6, int64_t m, const float *U, const float *S,
+                            const float *B, const float *hkl, const float *map, const float *rot, const float *R,
+                            const float *param, const float *param1, float *out) {
+    if (!ctx) return GRC_EINVAL;
+    Lock l(ctx);
+    return grow_indexed_region_held(ctx, rows6, m, U, S, B, hkl, map, rot, R, param, param1, out);
 }
 
 namespace {
@@ -685,8 +703,8 @@ struct WalkCache {
             c.out.resize(7 * m);
             for (int64_t i = 0; i < m; ++i)
                 for (int d = 0; d < 3; ++d) c.rows[6 * i + d] = (float)c.todo[3 * i + d];
-            const int rc = grc_grow_indexed_region(c.ctx, c.rows.data(), m, c.U, c.S, c.B, c.hkl, c.map, c.rot, c.R,
-                                                   c.param, c.param1, c.out.data());
+            const int rc = grow_indexed_region_held(c.ctx, c.rows.data(), m, c.U, c.S, c.B, c.hkl, c.map, c.rot,
+                                                    c.R, c.param, c.param1, c.out.data());
             if (rc != GRC_OK) return rc;
             c.map = nullptr;  // resident after the first call
             for (int64_t i = 0; i < m; ++i) {
@@ -703,11 +721,6 @@ struct WalkCache {
     }
 };
 
-int fail_locked(grc_ctx *ctx, int code, const char *what) {
-    Lock l(ctx);
-    return fail(ctx, code, "%s", what);
-}
-
 }  // namespace
 
 int grc_grow_best_first(grc_ctx *ctx, int64_t X, int64_t Y, int64_t Z, const double *I, const double *Imask,
@@ -718,23 +731,28 @@ int grc_grow_best_first(grc_ctx *ctx, int64_t X, int64_t Y, int64_t Z, const dou
                         uint8_t *J_out, int64_t *idx_out, int64_t idx_cap, int64_t *n_idx, double center[3],
                         int *replace_center) {
     if (!ctx) return GRC_EINVAL;
-    // no context lock here: every block of scores is one grc_grow_indexed_region call, which
-    // takes it
+    // the lock is held for the whole walk, so the geometry and map its cached scores come from
+    // cannot change between two blocks of scores
+    Lock l(ctx);
     if (!I || !Imask || !DisMedian || !Ninter || !seed || !U || !param1 || !C_out || !D_out || !N_out || !J_out ||
         !n_idx || !center || !replace_center || (idx_cap > 0 && !idx_out))
-        return fail_locked(ctx, GRC_EINVAL, "grow_best_first: NULL argument");
+        return fail(ctx, GRC_EINVAL, "grow_best_first: NULL argument");
     if (X < 1 || Y < 1 || Z < 1 || X > INT32_MAX || Y > INT32_MAX || Z > INT32_MAX || X * Y > INT64_MAX / Z)
-        return fail_locked(ctx, GRC_EINVAL, "grow_best_first: bad volume size");
+        return fail(ctx, GRC_EINVAL, "grow_best_first: bad volume size");
     if (seed[0] < 1 || seed[1] < 1 || seed[2] < 1 || seed[0] > X || seed[1] > Y || seed[2] > Z)
-        return fail_locked(ctx, GRC_EINVAL, "grow_best_first: seed outside the volume");
-    WalkCache c{ctx, X, Y, Z, Imask, U, S, B, hkl, map, rot, R, param, param1};
+        return fail(ctx, GRC_EINVAL, "grow_best_first: seed outside the volume");
+    // only the first 11 floats of param1 place voxels; the grow kernel's own thresholds
+    // (seed_comp, drop_off, maxDmedian) are not used by the walk and may hold anything
+    float p1[14];
+    for (int i = 0; i < 14; ++i) p1[i] = i < 11 ? param1[i] : 0.f;
+    WalkCache c{ctx, X, Y, Z, Imask, U, S, B, hkl, map, rot, R, param, p1};
     c.have.assign((size_t)(X * Y * Z), 0);
     c.val.assign((size_t)(3 * X * Y * Z), 0.f);
     const int rc = grc_walk_best_first(&WalkCache::score, &c, X, Y, Z, I, Imask, DisMedian, Ninter, seed, drop_off,
                                        maxD, indexed_comp, maxDmedian, C_out, D_out, N_out, J_out, idx_out, idx_cap,
                                        n_idx, center, replace_center);
-    if (rc == GRC_ECAPACITY) return fail_locked(ctx, GRC_ECAPACITY, "grow_best_first: more grown voxels than idx_cap");
-    return rc;  // arguments were checked above: any other error is the scorer's, recorded by grc_grow_indexed_region
+    if (rc == GRC_ECAPACITY) return fail(ctx, GRC_ECAPACITY, "grow_best_first: more grown voxels than idx_cap");
+    return rc;  // arguments were checked above: any other error is the scorer's, recorded by the grow scorer
 }
 
 int grc_forward_comp_compete(grc_ctx *ctx, const float *rows5, int64_t m, const float *id_neigb, int64_t n_neigb,
@@ -772,6 +790,11 @@ int grc_forward_comp_device(grc_ctx *ctx, const float *d_pos, int64_t n_vox, con
     Lock l(ctx);
     if (n_vox < 0 || n_q < 0) return fail(ctx, GRC_EINVAL, "negative size");
     if (n_vox > 0 && n_q > 0 && (!d_pos || !d_q || !d_out)) return fail(ctx, GRC_EINVAL, "NULL device buffer");
+    if (n_vox > 0 && n_q > 0) {
+        TRY(need_device(ctx, d_pos, "d_pos"));
+        TRY(need_device(ctx, d_q, "d_q"));
+        TRY(need_device(ctx, d_out, "d_out"));
+    }
     return forward_device(ctx, d_pos, n_vox, d_q, n_q, d_out);
 }
 
@@ -781,6 +804,10 @@ int grc_grow_device(grc_ctx *ctx, const float *d_rows6, int64_t m, const float *
     Lock l(ctx);
     if (m < 0) return fail(ctx, GRC_EINVAL, "negative size");
     if (m > 0 && (!d_rows6 || !d_out)) return fail(ctx, GRC_EINVAL, "NULL device buffer");
+    if (m > 0) {
+        TRY(need_device(ctx, d_rows6, "d_rows6"));
+        TRY(need_device(ctx, d_out, "d_out"));
+    }
     return grow_device(ctx, d_rows6, m, U, param1, d_out);
 }
 
@@ -791,6 +818,13 @@ int grc_compete_device(grc_ctx *ctx, const float *d_rows5, int64_t m, const floa
     Lock l(ctx);
     if (m < 0 || n_neigb < 0 || n_grain < 0) return fail(ctx, GRC_EINVAL, "negative size");
     if (m > 0 && (!d_rows5 || !d_out || !d_euler)) return fail(ctx, GRC_EINVAL, "NULL device buffer");
+    if (m > 0) {
+        TRY(need_device(ctx, d_rows5, "d_rows5"));
+        TRY(need_device(ctx, d_id, "d_id_neigb"));
+        TRY(need_device(ctx, d_euler, "d_euler"));
+        TRY(need_device(ctx, d_out, "d_out"));
+        TRY(need_device(ctx, d_trial_out, "d_trial_out"));
+    }
     return compete_device(ctx, d_rows5, m, d_id, n_neigb, d_euler, n_grain, param1, d_out, d_trial_out);
 }
 
@@ -803,6 +837,11 @@ int grc_score_trials_device(grc_ctx *ctx, const double *d_pos, int64_t n_vox, co
     if (n_trials < 0 || n_vox < 0 || n_q < 0) return fail(ctx, GRC_EINVAL, "negative size");
     if (n_trials == 0) return GRC_OK;
     if (!d_pos || !d_q || !d_out || n_vox < 1 || n_q < 1) return fail(ctx, GRC_EINVAL, "trials: NULL buffer or no rows");
+    TRY(need_device(ctx, d_pos, "trials: d_pos"));
+    TRY(need_device(ctx, d_q, "trials: d_q"));
+    TRY(need_device(ctx, d_out, "trials: d_out"));
+    TRY(need_device(ctx, d_tv, "trials: d_trial_voxel"));
+    TRY(need_device(ctx, d_to, "trials: d_trial_orient"));
     if ((d_tv == nullptr) != (d_to == nullptr))
         return fail(ctx, GRC_EINVAL, "trials: give both index arrays or neither");
     if (!d_tv && (n_vox != n_trials || n_q != n_trials))
@@ -1154,6 +1193,10 @@ extern "C" int grc_forward_comp_noalloc(grc_ctx *ctx, const float *pos, const fl
     Lock l(ctx);
     if (!pos || (n_q > 0 && (!d_q || !d_out))) return fail(ctx, GRC_EINVAL, "noalloc: NULL argument");
     if (n_q < 0) return fail(ctx, GRC_EINVAL, "noalloc: negative orientation count");
+    if (n_q > 0) {
+        TRY(need_device(ctx, d_q, "noalloc: d_q"));
+        TRY(need_device(ctx, d_out, "noalloc: d_out"));
+    }
     if (n_q > kNoAllocMaxQ)
         return fail(ctx, GRC_ECAPACITY,
                     "noalloc: %lld orientations exceed the fixed scratch of %lld (GRC_NOALLOC_MAX_ORIENTATIONS); "

@@ -53,18 +53,11 @@ class Sample:
                 self.geom.param20(self.nhkl))
 
 
-def voronoi_cylinder(dim: int, n_grains: int, seed: int, lognormal_sigma: float = 0.0) -> np.ndarray:
-    """Grain-id volume (dim^3, int32) of a cylinder along z split by a seeded Voronoi.
-
-    With ``lognormal_sigma > 0`` each site gets a log-normal weight and voxels go to
-    the site minimising |x-c|^2 - w^2 (a power diagram), which spreads grain sizes.
-    """
+def voronoi_sites(dim: int, n_grains: int, seed: int, lognormal_sigma: float = 0.0):
+    """Seeded sites (n x 3, inside the cylinder) and squared weights (n) of the power diagram
+    that ``voronoi_cylinder`` and ``voronoi_cylinder_torch`` partition the volume with."""
     rng = np.random.default_rng(seed)
     r = dim / 2.0
-    ax = np.arange(dim) + 0.5
-    X, Y, Z = np.meshgrid(ax, ax, ax, indexing="ij")
-    inside = (X - r) ** 2 + (Y - r) ** 2 <= r * r
-    # sites inside the cylinder
     sites = []
     while len(sites) < n_grains:
         p = rng.random(3) * dim
@@ -76,9 +69,22 @@ def voronoi_cylinder(dim: int, n_grains: int, seed: int, lognormal_sigma: float 
     if lognormal_sigma > 0:
         w = rng.lognormal(mean=0.0, sigma=lognormal_sigma, size=n_grains) * mean_d * 0.5
         w2 = w * w
+    return sites, w2
+
+
+def voronoi_cylinder(dim: int, n_grains: int, seed: int, lognormal_sigma: float = 0.0) -> np.ndarray:
+    """Grain-id volume (dim^3, int32) of a cylinder along z split by a seeded Voronoi.
+
+    With ``lognormal_sigma > 0`` each site gets a log-normal weight and voxels go to
+    the site minimising |x-c|^2 - w^2 (a power diagram), which spreads grain sizes.
+    """
+    r = dim / 2.0
+    ax = np.arange(dim) + 0.5
+    X, Y, Z = np.meshgrid(ax, ax, ax, indexing="ij")
+    inside = (X - r) ** 2 + (Y - r) ** 2 <= r * r
+    sites, w2 = voronoi_sites(dim, n_grains, seed, lognormal_sigma)
     pts = np.stack([X[inside], Y[inside], Z[inside]], axis=1)
     best = np.zeros(len(pts), np.int32)
-    bestd = np.full(len(pts), np.inf)
     chunk = 1 << 16
     for s in range(0, len(pts), chunk):
         p = pts[s:s + chunk]
@@ -122,7 +128,7 @@ def named_setup(kind: str, seed: int = 1, **over):
     return geom, cell, sg, G.gen_hkl(sg, 6), dim, ng, vox, sigma
 
 
-def make_sample(kind: str = "fe_small", seed: int = 1, **over) -> Sample:
+def make_sample(kind: str = "fe_small", seed: int = 1, voronoi=None, **over) -> Sample:
     """Named synthetic samples.
 
     ``fe6``   : BCC Fe a=2.8665, 6 grains, 100 um cylinder at 5 um (20^3 grid, ~6.3k voxels),
@@ -133,11 +139,16 @@ def make_sample(kind: str = "fe_small", seed: int = 1, **over) -> Sample:
                 0.0336 mm, 361 projections 0:1:360.
     ``fe_small``: the fe6 set-up shrunk for fast CPU tests (12^3 grid, 256^2 detector at
                 0.2688 mm, 37 projections 0:10:360).
+
+    ``voronoi(dim, n_grains, seed, sigma)`` replaces the grain-id generator (by default numpy,
+    or torch on a GPU for grids of 64^3 and more; all take the sites of ``voronoi_sites``).
     """
     geom, cell, sg, hkl, dim, ng, vox, sigma = named_setup(kind, seed, **over)
     vol = G.Volume(rec_volume_pixel=(1, 1, 1), simap=1, vox_size=vox, center=(0.0, 0.0, 0.0),
                    dimension=(dim, dim, dim))
-    if dim >= 64:
+    if voronoi is not None:
+        use_torch = False
+    elif dim >= 64:
         try:
             import torch
             use_torch = torch.cuda.is_available()
@@ -145,7 +156,9 @@ def make_sample(kind: str = "fe_small", seed: int = 1, **over) -> Sample:
             use_torch = False
     else:
         use_torch = False
-    if use_torch:
+    if voronoi is not None:
+        gid = np.asarray(voronoi(dim, ng, seed, sigma), np.int32)
+    elif use_torch:
         gid = voronoi_cylinder_torch(dim, ng, seed, sigma).cpu().numpy()
     else:
         gid = voronoi_cylinder(dim, ng, seed, sigma)
@@ -262,19 +275,10 @@ def voronoi_cylinder_torch(dim: int, n_grains: int, seed: int, lognormal_sigma: 
     """``voronoi_cylinder`` evaluated with torch on ``device`` (same sites and weights)."""
     import torch
 
-    rng = np.random.default_rng(seed)
     r = dim / 2.0
-    sites = []
-    while len(sites) < n_grains:
-        p = rng.random(3) * dim
-        if (p[0] - r) ** 2 + (p[1] - r) ** 2 <= r * r:
-            sites.append(p)
-    sites = torch.tensor(np.array(sites), dtype=torch.float64, device=device)
-    mean_d = dim / max(n_grains, 1) ** (1 / 3)
-    w2 = torch.zeros(n_grains, dtype=torch.float64, device=device)
-    if lognormal_sigma > 0:
-        w = rng.lognormal(mean=0.0, sigma=lognormal_sigma, size=n_grains) * mean_d * 0.5
-        w2 = torch.tensor(w * w, dtype=torch.float64, device=device)
+    s_np, w_np = voronoi_sites(dim, n_grains, seed, lognormal_sigma)
+    sites = torch.tensor(s_np, dtype=torch.float64, device=device)
+    w2 = torch.tensor(w_np, dtype=torch.float64, device=device)
     ax = torch.arange(dim, dtype=torch.float64, device=device) + 0.5
     gid = torch.zeros((dim, dim, dim), dtype=torch.int32, device=device)
     for ix in range(dim):

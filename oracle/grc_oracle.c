@@ -25,9 +25,12 @@
  *
  * Edge listing: a reflection is an "edge" when its FP64 landing coordinate lies
  * within EDGE_PX of a pixel-rounding boundary, or its wavelength / Bragg angle
- * lies within a relative 1e-9 of a selection threshold.  Those reflections can
- * legitimately flip between two correct implementations; every trial reports
- * how many it has.
+ * lies within a relative 1e-9 of a selection threshold.  Every trial reports how
+ * many it has.  A "tight edge" uses the bands EDGE_PX_TIGHT (1e-9 px) and
+ * EDGE_REL_TIGHT (1e-12): only there can two correct FP64 evaluations of the
+ * chain (this acos form and an algebraic form) round differently, so counts of a
+ * trial without a tight edge must agree exactly.  The tight count is reported
+ * separately (out[4] of oracle_trial, the optional ``tight`` arrays).
  */
 #include <math.h>
 #include <stdint.h>
@@ -39,6 +42,8 @@
 
 #define EDGE_PX 1e-4
 #define EDGE_REL 1e-9
+#define EDGE_PX_TIGHT 1e-9
+#define EDGE_REL_TIGHT 1e-12
 
 typedef struct {
     int nhkl, nrot, detysize, detzsize;
@@ -92,14 +97,15 @@ typedef struct {
 
 /*
  * One (U, pos) trial: forward_comp.m:8-90.  ``dis`` is caller scratch of nrot*nhkl
- * doubles.  Returns Nr_simu, Nr_intersect, dis_median and the edge count; when
- * ``rec`` is non-NULL every reflection's landing record is written there.
+ * doubles.  Returns out[0..4] = Nr_simu, Nr_intersect, dis_median, the edge count and
+ * the tight-edge count; when ``rec`` is non-NULL every reflection's landing record is
+ * written there.
  */
 static void oracle_trial(const ogeo *g, const double U[3][3], const double pos_in[3], double *dis,
                          double out[4], olanding *rec) {
     const double L = g->lss + g->lsd;
     const double pi = 3.14159265358979323846;
-    int nsimu = 0, ninter = 0, nedge = 0;
+    int nsimu = 0, ninter = 0, nedge = 0, ntight = 0;
     /* Gw = S*U*B*hkl (forward_comp.m:15-16) */
     double SU[3][3], SUB[3][3];
     for (int i = 0; i < 3; ++i)
@@ -147,6 +153,9 @@ static void oracle_trial(const ogeo *g, const double U[3][3], const double pos_i
             int edge = fabs(lambda - g->lmin) <= EDGE_REL * g->lmin ||
                        fabs(lambda - g->lmax) <= EDGE_REL * g->lmax ||
                        fabs(beta - pi / 2) <= EDGE_REL || fabs(beta - beta_max) <= EDGE_REL;
+            int tight = fabs(lambda - g->lmin) <= EDGE_REL_TIGHT * g->lmin ||
+                        fabs(lambda - g->lmax) <= EDGE_REL_TIGHT * g->lmax ||
+                        fabs(beta - pi / 2) <= EDGE_REL_TIGHT || fabs(beta - beta_max) <= EDGE_REL_TIGHT;
             if (!pass_bl && !edge && !rec) continue; /* select3 is a conjunction: skip the rest */
             double konst = sqrt(Gt[1] * Gt[1] + Gt[2] * Gt[2]);                        /* :44 */
             double nv1 = sqrt(0.0 + Gt[1] * Gt[1] + Gt[2] * Gt[2]);
@@ -173,6 +182,7 @@ static void oracle_trial(const ogeo *g, const double U[3][3], const double pos_i
                 u < g->detysize + 3 && v < g->detzsize + 3) {
                 double fu = u - floor(u), fv = v - floor(v);
                 if (fabs(fu - 0.5) < EDGE_PX || fabs(fv - 0.5) < EDGE_PX) edge = 1;
+                if (fabs(fu - 0.5) < EDGE_PX_TIGHT || fabs(fv - 0.5) < EDGE_PX_TIGHT) tight = 1;
             }
             double disv = NAN;
             if (sel) {
@@ -183,6 +193,7 @@ static void oracle_trial(const ogeo *g, const double U[3][3], const double pos_i
                 if (disv <= thr) ++ninter; /* :71-72 */
             }
             if (edge) ++nedge;
+            if (tight) ++ntight;
             if (rec) {
                 olanding *r = &rec[(size_t)iw * g->nhkl + ih];
                 r->iw = iw; r->ih = ih; r->sel = sel; r->edge = edge;
@@ -194,6 +205,7 @@ static void oracle_trial(const ogeo *g, const double U[3][3], const double pos_i
     out[1] = ninter;
     out[2] = matlab_median(dis, nsimu); /* :86-90 */
     out[3] = nedge;
+    out[4] = ntight;
 }
 
 static void quat_u(const float *q, double U[3][3]) {
@@ -222,9 +234,13 @@ static void pos_from_index(const float *row, const float *p1, double pos[3]) {
     if (p1[3] == 1.0f) { pos[0] = -pos[0]; pos[1] = -pos[1]; }
 }
 
+/* nthreads > 0: use that many threads; otherwise the default the process started with (an earlier
+ * call's explicit count does not stick). */
+static int default_threads = 0;
 static int nthreads_set(int nthreads) {
 #ifdef _OPENMP
-    if (nthreads > 0) omp_set_num_threads(nthreads);
+    if (default_threads == 0) default_threads = omp_get_max_threads();
+    omp_set_num_threads(nthreads > 0 ? nthreads : default_threads);
     return omp_get_max_threads();
 #else
     (void)nthreads;
@@ -232,17 +248,17 @@ static int nthreads_set(int nthreads) {
 #endif
 }
 
-/* One trial through the public surface: U row-major (double), pos [mm]. */
+/* One trial through the public surface: U row-major (double), pos [mm]; out5 as oracle_trial. */
 int oracle_forward_comp(const double *U9, const double *pos, const float *S, const float *B, const float *hkl,
                         const float *map, const float *rot, const float *R, const float *param, double dety0,
-                        double detz0, double thr, double *out4) {
+                        double detz0, double thr, double *out5) {
     ogeo g;
     geo_init(&g, S, B, hkl, map, rot, R, param, dety0, detz0, thr);
     double U[3][3];
     for (int i = 0; i < 9; ++i) U[i / 3][i % 3] = U9[i];
     double *dis = (double *)malloc(sizeof(double) * (size_t)g.nrot * g.nhkl + 8);
     if (!dis) return -1;
-    oracle_trial(&g, U, pos, dis, out4, NULL);
+    oracle_trial(&g, U, pos, dis, out5, NULL);
     free(dis);
     return 0;
 }
@@ -250,14 +266,14 @@ int oracle_forward_comp(const double *U9, const double *pos, const float *S, con
 /* Every reflection's landing record for one trial (tests and known-answer cases). */
 int oracle_landings(const double *U9, const double *pos, const float *S, const float *B, const float *hkl,
                     const float *map, const float *rot, const float *R, const float *param, double dety0,
-                    double detz0, double thr, olanding *rec, double *out4) {
+                    double detz0, double thr, olanding *rec, double *out5) {
     ogeo g;
     geo_init(&g, S, B, hkl, map, rot, R, param, dety0, detz0, thr);
     double U[3][3];
     for (int i = 0; i < 9; ++i) U[i / 3][i % 3] = U9[i];
     double *dis = (double *)malloc(sizeof(double) * (size_t)g.nrot * g.nhkl + 8);
     if (!dis) return -1;
-    oracle_trial(&g, U, pos, dis, out4, rec);
+    oracle_trial(&g, U, pos, dis, out5, rec);
     free(dis);
     return 0;
 }
@@ -265,12 +281,13 @@ int oracle_landings(const double *U9, const double *pos, const float *S, const f
 /*
  * ForwardCalc_OR_space_comp.m:22-56 on the cuda_forward_comp argument list:
  * out[4i..4i+3] = [Nr_simu, Nr_intersect, completeness, dis_median] (float),
- * edges[i] = edge-reflection count of orientation i.
+ * edges[i] = edge-reflection count of orientation i, tight[i] its tight-edge count
+ * (either may be NULL).
  */
 int oracle_orientation_scan(const float *pos3, const float *q, int64_t n, const float *S, const float *B,
                             const float *hkl, const float *map, const float *rot, const float *R,
                             const float *param, double dety0, double detz0, double thr, int nthreads,
-                            float *out, int32_t *edges) {
+                            float *out, int32_t *edges, int32_t *tight) {
     ogeo g;
     geo_init(&g, S, B, hkl, map, rot, R, param, dety0, detz0, thr);
     double pos[3] = {pos3[0], pos3[1], pos3[2]};
@@ -285,7 +302,7 @@ int oracle_orientation_scan(const float *pos3, const float *q, int64_t n, const 
         } else {
 #pragma omp for schedule(dynamic, 4)
             for (int64_t i = 0; i < n; ++i) {
-                double U[3][3], o[4];
+                double U[3][3], o[5];
                 quat_u(q + 4 * i, U);
                 oracle_trial(&g, U, pos, dis, o, NULL);
                 out[4 * i] = (float)o[0];
@@ -293,6 +310,7 @@ int oracle_orientation_scan(const float *pos3, const float *q, int64_t n, const 
                 out[4 * i + 2] = (float)(o[1] / o[0]);
                 out[4 * i + 3] = (float)o[2];
                 if (edges) edges[i] = (int32_t)o[3];
+                if (tight) tight[i] = (int32_t)o[4];
             }
             free(dis);
         }
@@ -310,7 +328,7 @@ int oracle_orientation_scan(const float *pos3, const float *q, int64_t n, const 
 int oracle_grow(const float *rows6, int64_t m, const float *U9f, const float *S, const float *B,
                 const float *hkl, const float *map, const float *rot, const float *R, const float *param,
                 const float *param1, double dety0, double detz0, double thr, int rule, const float *ninter,
-                int nthreads, float *out7, int32_t *edges) {
+                int nthreads, float *out7, int32_t *edges, int32_t *tight) {
     ogeo g;
     geo_init(&g, S, B, hkl, map, rot, R, param, dety0, detz0, thr);
     double U[3][3];
@@ -328,7 +346,7 @@ int oracle_grow(const float *rows6, int64_t m, const float *U9f, const float *S,
 #pragma omp for schedule(dynamic, 4)
             for (int64_t i = 0; i < m; ++i) {
                 const float *row = rows6 + 6 * i;
-                double pos[3], o[4];
+                double pos[3], o[5];
                 pos_from_index(row, param1, pos);
                 oracle_trial(&g, U, pos, dis, o, NULL);
                 double C = o[1] / o[0];
@@ -342,6 +360,7 @@ int oracle_grow(const float *rows6, int64_t m, const float *U9f, const float *S,
                 w[0] = row[0]; w[1] = row[1]; w[2] = row[2];
                 w[3] = (float)o[0]; w[4] = (float)o[1]; w[5] = (float)o[2]; w[6] = (float)flag;
                 if (edges) edges[i] = (int32_t)o[3];
+                if (tight) tight[i] = (int32_t)o[4];
             }
             free(dis);
         }
@@ -359,7 +378,7 @@ int oracle_grow(const float *rows6, int64_t m, const float *U9f, const float *S,
 int oracle_compete(const float *rows5, int64_t m, const float *id_neigb, const float *euler, const float *S,
                    const float *B, const float *hkl, const float *map, const float *rot, const float *R,
                    const float *param, const float *param1, double dety0, double detz0, double thr,
-                   int nthreads, float *out8, int32_t *edges) {
+                   int nthreads, float *out8, int32_t *edges, int32_t *tight) {
     ogeo g;
     geo_init(&g, S, B, hkl, map, rot, R, param, dety0, detz0, thr);
     const double pi = 3.14159265358979323846;
@@ -384,15 +403,16 @@ int oracle_compete(const float *rows5, int64_t m, const float *id_neigb, const f
                 w[7] = 2000.0f;
                 double bestC = NAN, bestI = 0, bestM = 2000;
                 int64_t bestG = -1;
-                int ne = 0;
+                int ne = 0, nt = 0;
                 for (int64_t j = first; j <= last; ++j) {
                     int64_t gid = (int64_t)id_neigb[j - 1];
                     const float *e = euler + 3 * (gid - 1);
-                    double U[3][3], o[4];
+                    double U[3][3], o[5];
                     euler_u((double)e[0] * pi / 180, (double)e[1] * pi / 180, (double)e[2] * pi / 180, U);
                     oracle_trial(&g, U, pos, dis, o, NULL);
                     double C = o[1] / o[0];
                     ne += (int)o[3];
+                    nt += (int)o[4];
                     if (bestG < 0 || (!isnan(C) && (isnan(bestC) || C > bestC))) {
                         bestC = C; bestI = o[1]; bestM = o[2]; bestG = gid;
                     }
@@ -403,6 +423,7 @@ int oracle_compete(const float *rows5, int64_t m, const float *id_neigb, const f
                     w[4] = (float)bestG; w[5] = (float)bestC; w[6] = (float)bestI; w[7] = (float)bestM;
                 }
                 if (edges) edges[i] = ne;
+                if (tight) tight[i] = nt;
             }
             free(dis);
         }
@@ -412,7 +433,8 @@ int oracle_compete(const float *rows5, int64_t m, const float *id_neigb, const f
 
 int oracle_max_threads(void) {
 #ifdef _OPENMP
-    return omp_get_max_threads();
+    if (default_threads == 0) default_threads = omp_get_max_threads();
+    return default_threads;
 #else
     return 1;
 #endif

@@ -49,11 +49,11 @@ def lib():
         L.oracle_landings.argtypes = [_f64p, _f64p, _f32p, _f32p, _f32p, _f32p, _f32p, _f32p, _f32p,
                                       d, d, d, C.POINTER(Landing), _f64p]
         L.oracle_orientation_scan.argtypes = [_f32p, _f32p, i64, _f32p, _f32p, _f32p, _f32p, _f32p, _f32p,
-                                              _f32p, d, d, d, i, _f32p, _i32p]
+                                              _f32p, d, d, d, i, _f32p, _i32p, _i32p]
         L.oracle_grow.argtypes = [_f32p, i64, _f32p, _f32p, _f32p, _f32p, _f32p, _f32p, _f32p, _f32p,
-                                  _f32p, d, d, d, i, C.c_void_p, i, _f32p, _i32p]
+                                  _f32p, d, d, d, i, C.c_void_p, i, _f32p, _i32p, _i32p]
         L.oracle_compete.argtypes = [_f32p, i64, _f32p, _f32p, _f32p, _f32p, _f32p, _f32p, _f32p, _f32p,
-                                     _f32p, _f32p, d, d, d, i, _f32p, _i32p]
+                                     _f32p, _f32p, d, d, d, i, _f32p, _i32p, _i32p]
         L.oracle_max_threads.restype = i
         L.oracle_fit_uv_jac.argtypes = [i, _f64p, _f64p, _f64p, _f64p, _f64p, d, d, d, d, d, _f64p, _f64p, _f64p]
         _lib = L
@@ -74,9 +74,9 @@ def _defaults(param, dety0, detz0):
 
 
 def forward_comp(U, pos, S, B, hkl, proj_bin_bw, rot_angles, RotDet, param, dety0=None, detz0=None, thr=0.5):
-    """One trial: (Nr_simu, Nr_intersect, dis_median, n_edge) in FP64."""
+    """One trial: (Nr_simu, Nr_intersect, dis_median, n_edge, n_tight_edge) in FP64."""
     p, dety0, detz0 = _defaults(param, dety0, detz0)
-    out = np.zeros(4)
+    out = np.zeros(5)
     lib().oracle_forward_comp(np.ascontiguousarray(U, np.float64).reshape(9), np.ascontiguousarray(pos, np.float64),
                               _f32(S), _f32(B), _f32(hkl), _f32(proj_bin_bw), _f32(rot_angles), _f32(RotDet), p,
                               dety0, detz0, thr, out)
@@ -88,7 +88,7 @@ def landings(U, pos, S, B, hkl, proj_bin_bw, rot_angles, RotDet, param, dety0=No
     p, dety0, detz0 = _defaults(param, dety0, detz0)
     n = int(p[0]) * int(p[1])
     rec = (Landing * n)()
-    out = np.zeros(4)
+    out = np.zeros(5)
     lib().oracle_landings(np.ascontiguousarray(U, np.float64).reshape(9), np.ascontiguousarray(pos, np.float64),
                           _f32(S), _f32(B), _f32(hkl), _f32(proj_bin_bw), _f32(rot_angles), _f32(RotDet), p,
                           dety0, detz0, thr, rec, out)
@@ -97,50 +97,58 @@ def landings(U, pos, S, B, hkl, proj_bin_bw, rot_angles, RotDet, param, dety0=No
 
 
 def orientation_scan(pos, q, S, B, hkl, proj_bin_bw, rot_angles, RotDet, param, dety0=None, detz0=None,
-                     thr=0.5, nthreads=0):
-    """cuda_forward_comp semantics on the CPU: (out[4N] float32, edges[N])."""
+                     thr=0.5, nthreads=0, tight=False):
+    """cuda_forward_comp semantics on the CPU: (out[4N] float32, edges[N]), plus the tight-edge
+    counts (reflections within 1e-9 px of a rounding boundary or 1e-12 of a window bound) as a
+    third value when ``tight``."""
     p, dety0, detz0 = _defaults(param, dety0, detz0)
     q = _f32(q)
     n = q.size // 4
     out = np.zeros(4 * n, np.float32)
     edges = np.zeros(n, np.int32)
+    te = np.zeros(n, np.int32)
     rc = lib().oracle_orientation_scan(_f32(pos), q, n, _f32(S), _f32(B), _f32(hkl), _f32(proj_bin_bw),
-                                       _f32(rot_angles), _f32(RotDet), p, dety0, detz0, thr, nthreads, out, edges)
+                                       _f32(rot_angles), _f32(RotDet), p, dety0, detz0, thr, nthreads, out, edges,
+                                       te)
     assert rc == 0
-    return out, edges
+    return (out, edges, te) if tight else (out, edges)
 
 
 def grow(rows6, U, S, B, hkl, proj_bin_bw, rot_angles, RotDet, param, param1, dety0=None, detz0=None,
-         thr=0.5, rule=0, ninter=None, nthreads=0):
-    """cuda_grow_indexed_region semantics on the CPU: (out[7M] float32, edges[M])."""
+         thr=0.5, rule=0, ninter=None, nthreads=0, tight=False):
+    """cuda_grow_indexed_region semantics on the CPU: (out[7M] float32, edges[M]) (+ tight-edge
+    counts when ``tight``)."""
     p, dety0, detz0 = _defaults(param, dety0, detz0)
     rows6 = _f32(rows6)
     m = rows6.size // 6
     out = np.zeros(7 * m, np.float32)
     edges = np.zeros(m, np.int32)
+    te = np.zeros(m, np.int32)
     nin = None
     if ninter is not None:
         nin = _f32(ninter)
     rc = lib().oracle_grow(rows6, m, _f32(U), _f32(S), _f32(B), _f32(hkl), _f32(proj_bin_bw), _f32(rot_angles),
                            _f32(RotDet), p, _f32(param1), dety0, detz0, thr, rule,
-                           None if nin is None else nin.ctypes.data, nthreads, out, edges)
+                           None if nin is None else nin.ctypes.data, nthreads, out, edges, te)
     assert rc == 0
-    return out, edges
+    return (out, edges, te) if tight else (out, edges)
 
 
 def compete(rows5, id_neigb, euler, S, B, hkl, proj_bin_bw, rot_angles, RotDet, param, param1, dety0=None,
-            detz0=None, thr=0.5, nthreads=0):
-    """cuda_forward_comp_compete semantics on the CPU: (out[8M] float32, edges[M])."""
+            detz0=None, thr=0.5, nthreads=0, tight=False):
+    """cuda_forward_comp_compete semantics on the CPU: (out[8M] float32, edges[M]) (+ tight-edge
+    counts when ``tight``)."""
     p, dety0, detz0 = _defaults(param, dety0, detz0)
     rows5 = _f32(rows5)
     m = rows5.size // 5
     out = np.zeros(8 * m, np.float32)
     edges = np.zeros(m, np.int32)
+    te = np.zeros(m, np.int32)
     rc = lib().oracle_compete(rows5, m, _f32(id_neigb), _f32(euler), _f32(S), _f32(B), _f32(hkl),
                               _f32(proj_bin_bw), _f32(rot_angles), _f32(RotDet), p, _f32(param1), dety0, detz0,
-                              thr, nthreads, out, edges)
+                              thr, nthreads, out, edges, te)
     assert rc == 0
-    return out, edges
+    return (out, edges, te) if tight else (out, edges)
 
 
 def max_threads() -> int:

@@ -95,7 +95,7 @@ def test_batch_vs_oracle_small(setup):
     s, dmap, rows5, ids, eul, ctx, ref, dev, param1 = setup
     S9, B9, hkl, rot, R9, p = s.mex_arrays()
     sub = rows5[:40].copy()
-    want, edges = O.compete(sub, ids, eul, S9, B9, hkl, dmap, rot, R9, p, param1)
+    want, _, edges = O.compete(sub, ids, eul, S9, B9, hkl, dmap, rot, R9, p, param1, tight=True)
     want = want.reshape(-1, 8)
     clean = edges == 0
     np.testing.assert_array_equal(ref[:40][clean][:, :7], want[clean][:, :7])

@@ -175,7 +175,7 @@ def test_completeness_with_fitted_geometry_matches_oracle(env):
     for v in idx[rng.choice(len(idx), 3, replace=False)]:
         pos = s.vol.pos_of_index(v).astype(np.float32)
         gpu = ctx.forward_comp(pos, q, S9, B9, hkl, dmap, rot, R9, p).reshape(-1, 4)
-        ref, edges = O.orientation_scan(pos, q, S9, B9, hkl, dmap, rot, R9, p)
+        ref, _, edges = O.orientation_scan(pos, q, S9, B9, hkl, dmap, rot, R9, p, tight=True)
         ref = ref.reshape(-1, 4)
         clean = edges == 0
         assert clean.sum() > len(q) // 2

@@ -1,9 +1,14 @@
 """Parity on the full benchmark geometries and the grid-argmax known-answer case.
 
 * BCC Fe, 1024^2 detector, 181 projections, 86 reflections (the CPU-runnable configuration) and
-  FCC Al, 2048^2 detector, 361 projections, 64 reflections (the seeding configuration): counts,
-  completeness and medians bit-exact against the oracle for every trial without an edge
-  reflection, on seed subsets of the orientation grid.
+  FCC Al, 2048^2 detector, 361 projections, 64 reflections (the seeding configuration), on both
+  scoring kernels: Nr_simu, Nr_intersect, completeness, dis_median and the per-voxel argmax over
+  orientations equal the oracle's on every trial.  The one allowance is a trial holding a
+  reflection whose oracle landing lies within 1e-9 px of a rounding boundary (or whose
+  wavelength or Bragg angle lies within a relative 1e-12 of a window bound): there two correct
+  FP64 evaluations may round apart, so its counts may differ by at most that number.  Such
+  trials are counted and reported, as are the trials with a reflection within 1e-4 px of a
+  boundary (the listing band), which must match like every other trial.
 * The best orientation of a grid that does not contain the ground truth is the grid point nearest
   to it, or ties with it in completeness (the scan's argmax is a first maximum)."""
 import numpy as np
@@ -39,31 +44,51 @@ def fe6():
     ctx.close()
 
 
+def _first_max(c):
+    """MATLAB max over completeness: first maximum, NaN ignored (-1 when every value is NaN)."""
+    c = np.where(np.isnan(c), -np.inf, c)
+    return int(np.argmax(c)) if np.isfinite(c).any() else -1
+
+
 def _parity(s, ctx, host, n_vox, n_q, seed):
+    """Both kernels against the oracle on n_vox random voxels x (grain orientations + n_q grid
+    orientations).  Returns (trials, trials with a listed 1e-4 px edge, trials with a tight edge)."""
     S9, B9, hkl, rot, R9, p = s.mex_arrays()
     idx = s.voxel_indices()
     rng = np.random.default_rng(seed)
     q = np.concatenate([s.grain_q, G.cubic_fz_orientations(n_q, seed)]).astype(np.float32)
-    n_clean = 0
+    n_all = n_listed = n_tight = 0
     for v in idx[rng.choice(len(idx), n_vox, replace=False)]:
         pos = s.vol.pos_of_index(v).astype(np.float32)
-        gpu = ctx.forward_comp(pos, q, S9, B9, hkl, None, rot, R9, p).reshape(-1, 4)
-        ref, edges = O.orientation_scan(pos, q, S9, B9, hkl, host, rot, R9, p)
+        ref, edges, tight = O.orientation_scan(pos, q, S9, B9, hkl, host, rot, R9, p, tight=True)
         ref = ref.reshape(-1, 4)
-        clean = edges == 0
-        n_clean += int(clean.sum())
-        np.testing.assert_array_equal(gpu[clean, :3], ref[clean, :3])
-        np.testing.assert_allclose(gpu[clean, 3], ref[clean, 3], rtol=1e-6)
-        d = np.abs(gpu[~clean, :2] - ref[~clean, :2]).max(axis=1) if (~clean).any() else np.zeros(0)
-        assert np.all(d <= edges[~clean])
+        exact = tight == 0
+        for path in (1, 2):
+            ctx.set_path(path)
+            gpu = ctx.forward_comp(pos, q, S9, B9, hkl, None, rot, R9, p).reshape(-1, 4)
+            assert ctx.last_stats()["path"] == path
+            np.testing.assert_array_equal(gpu[exact], ref[exact], err_msg=f"kernel path {path}")
+            d = np.abs(gpu[~exact, :2] - ref[~exact, :2]).max(axis=1) if (~exact).any() else np.zeros(0)
+            assert np.all(d <= tight[~exact])
+            if exact.all():
+                assert _first_max(gpu[:, 2]) == _first_max(ref[:, 2])
+        ctx.set_path(0)
+        n_all += len(q)
+        n_listed += int((edges > 0).sum())
+        n_tight += int((~exact).sum())
         g = s.grain_id[tuple(v - 1)]
-        assert gpu[g - 1, 2] >= 0.9  # the voxel's own grain orientation is (almost) complete
-    return n_clean
+        assert ref[g - 1, 2] >= 0.9  # the voxel's own grain orientation is (almost) complete
+    print(f"{n_all} trials: {n_listed} with a reflection within 1e-4 px of a boundary (all matched), "
+          f"{n_tight} with one within 1e-9 px")
+    return n_all, n_listed, n_tight
 
 
 def test_fe6_full_geometry_parity(fe6):
+    """16 voxels x 9,224 orientations (the 6 grains + a 9,218-orientation grid, the size of the
+    Oh 3-degree grid of the CPU configuration) on both kernels."""
     s, ctx, host = fe6
-    assert _parity(s, ctx, host, 3, 1500, 4) > 1000
+    n_all, n_listed, n_tight = _parity(s, ctx, host, 16, 9218, 4)
+    assert n_all == 16 * 9224 and n_tight <= n_all // 1000
 
 
 def test_grid_argmax_is_the_nearest_point_or_ties(fe6):
@@ -96,10 +121,13 @@ def test_grid_argmax_is_the_nearest_point_or_ties(fe6):
 
 
 def test_al400_full_geometry_parity():
+    """16 seed voxels x 4,496 orientations (400 grains + a 4,096-orientation grid) on both kernels.
+    About 80% of these trials hold a reflection within 1e-4 px of a boundary; all must match."""
     s = synth.make_sample("al400", seed=1)
     ctx = Context(0)
     try:
         host = synth.device_maps(s, ctx, keep_host_map=True)
-        assert _parity(s, ctx, host, 2, 400, 7) > 200  # ~20% of al400 trials carry no edge reflection
+        n_all, n_listed, n_tight = _parity(s, ctx, host, 16, 4096, 7)
+        assert n_all == 16 * 4496 and n_listed > n_all // 2 and n_tight <= n_all // 1000
     finally:
         ctx.close()

@@ -75,8 +75,8 @@ def test_landing_pixel_matches_closed_form(ctx):
     q = _random_quats(4096, 11)
     out = ctx.forward_comp(np.zeros(3, np.float32), q, S9, B9, hk, dmap.reshape(-1), np.zeros(1, np.float32),
                            G.flat_rowmajor(np.eye(3)), p).reshape(-1, 4)
-    ref, edges = O.orientation_scan(np.zeros(3, np.float32), q, S9, B9, hk, dmap, np.zeros(1, np.float32),
-                                    G.flat_rowmajor(np.eye(3)), p)
+    ref, _, edges = O.orientation_scan(np.zeros(3, np.float32), q, S9, B9, hk, dmap, np.zeros(1, np.float32),
+                                       G.flat_rowmajor(np.eye(3)), p, tight=True)
     ref = ref.reshape(-1, 4)
     sel, u, v = _closed_form(q, B9, hkl[0])
     on = sel & (np.round(u) >= 1) & (np.round(u) <= N) & (np.round(v) >= 1) & (np.round(v) <= N)

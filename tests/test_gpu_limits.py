@@ -52,7 +52,7 @@ def _parity(path, nrot, nhkl, n_or):
             pos = s.vol.pos_of_index(v).astype(np.float32)
             gpu = ctx.forward_comp(pos, q, S9, B9, hkl, None, rot, R9, p).reshape(-1, 4)
             used = ctx.last_stats()["path"]
-            ref, edges = O.orientation_scan(pos, q, S9, B9, hkl, host, rot, R9, p)
+            ref, _, edges = O.orientation_scan(pos, q, S9, B9, hkl, host, rot, R9, p, tight=True)
             ref = ref.reshape(-1, 4)
             clean = edges == 0
             n_clean += int(clean.sum())

@@ -1,4 +1,4 @@
-"""The allocation-free seeding scan against the regular drop-in entry.
+"""The allocation-free seeding scan against the regular drop-in entry and the oracle.
 
 grc_forward_comp_noalloc exists for callers that cannot allocate GPU memory while
 they score (a MEX shim inside MATLAB's gpuArray memory manager, a framework whose
@@ -13,7 +13,8 @@ import pytest
 
 from grainrecon_b200 import geometry as G
 from grainrecon_b200 import synth
-from grainrecon_b200._lib import NOALLOC_MAX_ORIENTATIONS, Context, GrcError, GRC_ECAPACITY
+from grainrecon_b200._lib import NOALLOC_MAX_ORIENTATIONS, Context, GrcError, GRC_ECAPACITY, GRC_EINVAL
+from oracle import oracle as O
 
 pytestmark = pytest.mark.gpu
 MED_RTOL = 1e-6  # dis_median tolerance used by the other parity tests
@@ -32,9 +33,10 @@ def test_noalloc_matches_drop_in_entry_twice():
             pos = s.vol.pos_of_index(v).astype(np.float32)
             q = np.concatenate([s.grain_q, G.cubic_fz_orientations(700 + 300 * k, 40 + k)]).astype(np.float32)
             ref = ctx.forward_comp(pos, q, S9, B9, hkl, dmap if k == 0 else None, rot, R9, p).reshape(-1, 4)
-            cases.append((pos, q, ref))
+            orc, _, tight = O.orientation_scan(pos, q, S9, B9, hkl, dmap, rot, R9, p, tight=True)
+            cases.append((pos, q, ref, orc.reshape(-1, 4), tight == 0))
         # two calls in a row, different sizes: the second must not see the first's leftovers
-        for pos, q, ref in cases:
+        for pos, q, ref, orc, exact in cases:
             d_q = torch.from_numpy(q.reshape(-1)).cuda()
             d_out = torch.full((q.shape[0] * 4,), -7.0, dtype=torch.float32, device="cuda")
             torch.cuda.synchronize()
@@ -42,6 +44,15 @@ def test_noalloc_matches_drop_in_entry_twice():
             got = d_out.cpu().numpy().reshape(-1, 4)
             np.testing.assert_array_equal(got[:, :3], ref[:, :3])
             np.testing.assert_allclose(got[:, 3], ref[:, 3], rtol=MED_RTOL)
+            # and the FP64 oracle, on every trial without a reflection within 1e-9 px of a boundary
+            assert exact.sum() >= len(q) - 2
+            np.testing.assert_array_equal(got[exact, :3], orc[exact, :3])
+            np.testing.assert_allclose(got[exact, 3], orc[exact, 3], rtol=MED_RTOL)
         with pytest.raises(GrcError) as e:
             ctx.forward_comp_noalloc(cases[0][0], d_q, NOALLOC_MAX_ORIENTATIONS + 1, d_out)
         assert e.value.code == GRC_ECAPACITY
+        # host buffers are refused before any kernel sees them
+        host_q = torch.from_numpy(cases[0][1].reshape(-1).copy())
+        with pytest.raises(GrcError) as e:
+            ctx.forward_comp_noalloc(cases[0][0], host_q, cases[0][1].shape[0], d_out)
+        assert e.value.code == GRC_EINVAL
