@@ -193,6 +193,9 @@ def run_reference(args):
     return 0
 
 
+SCORER_DTYPE = "f32+f64"  # FP32 landing chain, FP64 for every landing within 0.006 px of a pixel edge
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -212,6 +215,8 @@ def run_ours(args):
     setup_s = time.perf_counter() - t0
     S9, B9, hkl, rot, R9, p = s.mex_arrays()
     ctx.set_geometry(S9, B9, hkl, rot, R9, p)
+    comp = args.output == "completeness"
+    ctx.set_median(not comp)
     S = args.seeds
     K, W = args.steps, args.warmup
     need = (K + W) * S * world
@@ -219,16 +224,21 @@ def run_ours(args):
     d_pos = torch.from_numpy(seeds.reshape(-1).copy()).cuda()
     d_q = torch.from_numpy(q.reshape(-1)).cuda()
     d_out = torch.empty((K, S * N_ORIENT * 4), dtype=torch.float32, device="cuda")
+    d_best = torch.empty((K, S), dtype=torch.int32, device="cuda")
+    d_best_c = torch.empty((K, S), dtype=torch.float32, device="cuda")
     d_tmp = torch.empty(S * N_ORIENT * 4, dtype=torch.float32, device="cuda")
+    d_tb = torch.empty(S, dtype=torch.int32, device="cuda")
+    d_tc = torch.empty(S, dtype=torch.float32, device="cuda")
     stream = torch.cuda.ExternalStream(ctx.stream)
 
     def seed_slice(step):
         a, z = seed_range(step, rank, world, S)
         return d_pos[3 * a: 3 * z]
 
+    # one step: the seeding scan of S seeds x N_ORIENT orientations and each seed's first maximum
     ctx.set_timing(True)
     for i in range(W):
-        ctx.forward_comp_device(seed_slice(i), S, d_q, N_ORIENT, d_tmp)
+        ctx.forward_comp_argmax_device(seed_slice(i), S, d_q, N_ORIENT, d_tmp, d_tb, d_tc)
         ctx.last_stats()
     torch.cuda.synchronize()
     if world > 1:
@@ -241,7 +251,7 @@ def run_ours(args):
         torch.cuda.synchronize()
         ev0.record(stream)
         for i in range(K):
-            ctx.forward_comp_device(seed_slice(W + i), S, d_q, N_ORIENT, d_out[i])
+            ctx.forward_comp_argmax_device(seed_slice(W + i), S, d_q, N_ORIENT, d_out[i], d_best[i], d_best_c[i])
             st = ctx.last_stats()  # reads the scoring kernels' CUDA events of this step
             score_ms.append(st["score_ms"])
             launches += st["kernel_launches"]
@@ -253,7 +263,7 @@ def run_ours(args):
         # selected reflections (map lookups) per trial of the profiled steps: turns an ncu
         # capture's DRAM bytes per launch into bytes per lookup
         simu = d_out.view(K, -1, 4)[:, :, 0].double()
-        print(json.dumps({"profile": args.config, "lookups_per_trial": float(simu.mean()),
+        print(json.dumps({"profile": args.config, "output": args.output, "lookups_per_trial": float(simu.mean()),
                           "trials_per_step": S * N_ORIENT, "kernel_launches": launches}), flush=True)
         ctx.close()
         return 0
@@ -262,6 +272,24 @@ def run_ours(args):
     value = trials / (max_ms / 1e3)
     lookups = d_out.view(K, -1, 4)[:, :, 0].double().sum(dim=1).cpu().numpy()  # selected reflections per launch
     achieved = float(np.mean(lookups * 32.0 / (np.array(score_ms) / 1e3))) / 1e9
+    # the first maximum of each seed against the step's own completeness column
+    c = d_out.view(K, S, N_ORIENT, 4)[..., 2].cpu().numpy()
+    cm = np.where(np.isnan(c), -np.inf, c)
+    argmax_ok = bool(np.array_equal(cm.argmax(axis=2), d_best.cpu().numpy()))
+
+    # the other output mode on the same steps (device-resident), for comparison
+    ctx.set_median(comp)
+    for i in range(2):
+        ctx.forward_comp_argmax_device(seed_slice(i), S, d_q, N_ORIENT, d_tmp, d_tb, d_tc)
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    n_other = max(1, min(K, 5))
+    for i in range(n_other):
+        ctx.forward_comp_argmax_device(seed_slice(W + i), S, d_q, N_ORIENT, d_tmp, d_tb, d_tc)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    other_val = n_other * S * N_ORIENT * world / (max_over_ranks(ev0.elapsed_time(ev1), device="cuda") / 1e3)
+    ctx.set_median(not comp)
 
     # end to end through the drop-in entry, one call per seed voxel, pinned host buffers
     q_host = torch.from_numpy(q.reshape(-1)).pin_memory().numpy()
@@ -289,14 +317,15 @@ def run_ours(args):
     peak = peaks.get("hbm_gbs")
     peak_note = "measured hbm_gbs (MEASURED_PEAKS.json)" if peak else "fallback 6650 GB/s"
     peak = peak or 6650.0
-    kernel = "sweep_kernel" if path == 2 else "score_kernel"
+    kernel = "sweep_kernel" if path == 2 else ("scan_kernel" if path == 3 else "score_kernel")
     traffic = None
     issue = None
     clocks = clk.summary()
     try:
         # DRAM bytes per selected reflection and warp instructions per trial measured by ncu on
-        # the same kernel and workload (profiles/); absent for a workload that was not captured
-        prof = json.load(open(os.path.join(ROOT, "profiles", f"{kernel}_dram.json")))["workloads"][args.config]
+        # the same kernel, workload and output mode (profiles/); absent for one not captured
+        prof = json.load(open(os.path.join(ROOT, "profiles", f"{kernel}_dram.json")))["workloads"][
+            f"{args.config}-{args.output}"]
         traffic = float(np.mean(lookups)) * prof["dram_bytes_per_lookup"]
         if "warp_instructions_per_trial" in prof:
             # issue roofline: one warp instruction per scheduler per clock, 4 schedulers per SM
@@ -306,7 +335,8 @@ def run_ours(args):
             ach_issue = value / world * prof["warp_instructions_per_trial"]
             issue = {"achieved": ach_issue, "peak": peak_issue, "unit": "warp instructions/s",
                      "frac": ach_issue / peak_issue, "instructions_per_trial": prof["warp_instructions_per_trial"],
-                     "peak_source": f"{nsm} SMs x 4 schedulers x {sm_mhz:.0f} MHz (sampled under load)"}
+                     "peak_source": f"{nsm} SMs x 4 schedulers x {sm_mhz:.0f} MHz (sampled under load)",
+                     "instructions_source": f"stored ncu capture profiles/{kernel}_dram.json"}
     except (OSError, KeyError, ValueError):
         pass
     cpu = None
@@ -314,16 +344,28 @@ def run_ours(args):
         torch.cuda.synchronize()
         cpu = cpu_baseline(s, host_map, seeds, q, args.cpu_trials)
     if rank == 0:
+        cfg = workload_desc(s, S)
+        cfg["output"] = (("completeness only: Nr_simu, Nr_intersect and completeness from the bit-packed hit "
+                          "mask (column 4 NaN), and each seed's first maximum over its orientations; the "
+                          "seeding engine reads column 3 only (GrainMapping_engine_gpu_comp.m:103)") if comp else
+                         "the reference's four columns (exact dis_median from the 8-bit rank codes) and each "
+                         "seed's first maximum over its orientations")
         line = {"metric": METRIC, "value": value, "unit": "trials/s", "n_gpus": world, "steps": K, "warmup": W,
                 "ms_per_step": max_ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-                "dtype": "f64", "data": "synthetic", "config": workload_desc(s, S),
+                "dtype": SCORER_DTYPE, "data": "synthetic", "config": cfg,
                 "clocks": clocks,
                 "e2e": {"value": e2e_val, "unit": "trials/s",
                         "h2d_bytes_per_step": S * (12 + N_ORIENT * 16), "d2h_bytes_per_step": S * N_ORIENT * 16,
-                        "note": f"{e2e_steps} steps of {S} grc_forward_comp calls (one per seed voxel)"},
+                        "note": (f"{e2e_steps} steps of {S} grc_forward_comp calls (one per seed voxel), "
+                                 f"median {'off (grc_set_median(ctx, 0))' if comp else 'on'}")},
                 "gpu_launches": launches,
+                "argmax_matches_output": argmax_ok,
+                ("full_output" if comp else "completeness_only"): {
+                    "value": other_val, "unit": "trials/s", "steps": n_other,
+                    "note": "the same steps in the other output mode, device-resident"},
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                              "frac": achieved / peak, "traffic": traffic,
+                             "traffic_source": "stored ncu capture (profiles/), DRAM bytes per lookup x lookups",
                              "kernel": kernel, "peak_source": peak_note,
                              "algorithmic_bytes": "32 B (one sector) per selected reflection's map lookup",
                              "lookups_per_launch": float(np.mean(lookups)),
@@ -386,7 +428,26 @@ def run_grow(args):
         ctx.sync()
     graph_ms = ev0.elapsed_time(ev1) / args.steps
     batched = T / (graph_ms / 1e3)
-    # one scorer call per voxel, reference style (grow_indexed_region_cuda.m:105)
+    # the reference's own batching of this work: one compete call per 30,000 waiting voxels
+    # (revise_all_unindexed_voxel_cuda.m:77), each call planning its CSR list and copying nothing
+    # else (the device-buffer entry grc_compete_device, timed with CUDA events)
+    chunk = 30000
+    for _ in range(max(1, args.warmup)):
+        for c0 in range(0, m, chunk):
+            c1 = min(m, c0 + chunk)
+            ctx.compete_device(d_rows5[5 * c0:5 * c1], c1 - c0, d_ids, ids.size, d_eul, len(eul), param1,
+                               out[8 * c0:8 * c1])
+    ctx.sync()
+    ev0.record(stream)
+    for _ in range(args.steps):
+        for c0 in range(0, m, chunk):
+            c1 = min(m, c0 + chunk)
+            ctx.compete_device(d_rows5[5 * c0:5 * c1], c1 - c0, d_ids, ids.size, d_eul, len(eul), param1,
+                               out[8 * c0:8 * c1])
+    ev1.record(stream)
+    ctx.sync()
+    chunked_ms = ev0.elapsed_time(ev1) / args.steps
+    # one scorer call per voxel (the launch-bound extreme)
     nb = min(args.plain_voxels, m)
     one = torch.empty(8, dtype=torch.float32, device="cuda")
     for i in range(min(20, nb)):
@@ -400,7 +461,7 @@ def run_grow(args):
     plain = float(rows5[:nb, 4].max() - rows5[0, 3] + 1) / plain_s
     line = {"metric": METRIC, "value": batched, "unit": "trials/s", "n_gpus": 1, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": graph_ms, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "vs_baseline": None, "dtype": SCORER_DTYPE, "data": "synthetic",
             "config": {"workload": (f"batched grow: FCC Al 400 grains, {m} voxels with 1-64 candidates "
                                     f"(Geometric p=0.15, neighbour grains + 0.5 deg perturbations), {T} trials "
                                     f"per iteration"),
@@ -408,6 +469,11 @@ def run_grow(args):
             "clocks": clk.summary(),
             "batched_graph": {"trials_per_s": batched, "ms_per_iteration": graph_ms},
             "batched_direct": {"trials_per_s": T / (direct_ms / 1e3), "ms_per_iteration": direct_ms},
+            "graph_gain": direct_ms / graph_ms,
+            "reference_chunks": {"trials_per_s": T / (chunked_ms / 1e3), "ms_per_iteration": chunked_ms,
+                                 "note": (f"one grc_compete_device call per {chunk} voxels "
+                                          "(revise_all_unindexed_voxel_cuda.m:77), CSR planned per call")},
+            "speedup_vs_reference_chunks": chunked_ms / graph_ms,
             "plain_per_voxel": {"trials_per_s": plain, "voxels_sampled": nb,
                                 "note": "one grc_compete_device call (one scoring launch set) per voxel"},
             "speedup_vs_plain": batched / plain, "autotune": tune}
@@ -472,14 +538,11 @@ def run_seed(args):
     ids, p = batch(args.warmup)
     ph = {}
     t0 = time.perf_counter()
-    out = ix.scan(p)
-    cand = ix.top(out, ix.q)
+    cand = ix.candidates(p)
     torch.cuda.synchronize()
     ph["scan_top_s"] = time.perf_counter() - t0
     t0 = time.perf_counter()
-    best_q, best_c = ix.local_best(p, cand)
-    order = SD.sort_desc_nan_first(best_c, dim=1)[:, :1]
-    x0 = torch.gather(best_q, 1, order[:, :, None].expand(-1, -1, 4))[:, :, 1:].contiguous()
+    _, _, _, x0 = ix.refine(p, cand, 1)
     torch.cuda.synchronize()
     ph["local_refine_s"] = time.perf_counter() - t0
     t0 = time.perf_counter()
@@ -503,7 +566,7 @@ def run_seed(args):
     seeds = n * args.steps * world
     line = {"metric": "seeds indexed/s", "value": seeds / dt, "unit": "seeds/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": SCORER_DTYPE, "data": "synthetic",
             "config": {"workload": (f"seeding stage: FCC Al 400 grains, 2048x2048 detector, 361 projections; "
                                     f"{n} seeds per step x ({N_ORIENT} scan + {args.nr_seed} x 730 local-refine "
                                     f"trials + fminsearchbnd (<= 2000 evaluations) + 1 final)"),
@@ -559,7 +622,7 @@ def run_walk(args):
         grown = [len(walk(*c)[6]) for c in cases]
         dt = time.perf_counter() - t0
     line = {"metric": "best-first grown voxels/s", "value": sum(grown) / dt, "unit": "voxels/s", "n_gpus": 1,
-            "higher_is_better": True, "dtype": "f64", "data": "synthetic",
+            "higher_is_better": True, "dtype": SCORER_DTYPE, "data": "synthetic",
             "config": {"workload": (f"grow_indexed_region walk from the centre voxel of the 3 largest grains "
                                     f"({', '.join(str(int(sizes[g])) for g in grains)} voxels) of FCC Al 400 grains, "
                                     f"{int(Imask.sum())} voxels, 2048x2048 detector, 361 projections, drop_off 0.05")},
@@ -650,7 +713,7 @@ def run_map(args):
     n_seeds = int(sum(len(r) for r in rows))
     tried = int(sum((r[:, 6] > 0).sum() for r in rows))  # seeds that were indexed (not skipped)
     line = {"metric": "sample mapping time", "value": dt, "unit": "s", "n_gpus": 1, "higher_is_better": False,
-            "dtype": "f64", "data": "synthetic",
+            "dtype": SCORER_DTYPE, "data": "synthetic",
             "config": {"workload": (f"GrainMapping iteration on BCC Fe 6 grains, {int(mask.sum())} voxels, "
                                     f"1024x1024 detector, 181 projections, {N_ORIENT}-orientation grid, "
                                     f"Nr_seed 400, up to {args.map_iters} iterations")},
@@ -760,6 +823,8 @@ def main():
     ap.add_argument("--grow-voxels", type=int, default=262144, help="voxels per batched-grow iteration")
     ap.add_argument("--plain-voxels", type=int, default=2000, help="voxels timed one call each")
     ap.add_argument("--seeds", type=int, default=64, help="seed voxels per step per GPU")
+    ap.add_argument("--output", default="completeness", choices=["completeness", "full"],
+                    help="seeding-scan output: completeness only (bit-packed mask) or the four MEX columns")
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--cpu-trials", type=int, default=8192)

@@ -31,7 +31,9 @@ EXPORTS = [
     "grc_fit_spot_count", "grc_fit_spot_fill", "grc_centroid_residual_adjoint", "grc_fit_grains_lm",
     "grc_fit_grains_nm", "grc_fit_grains_rms", "grc_fit_geometry_lm", "grc_fit_geometry_cost",
     "grc_fit_geometry_rms", "grc_score_trials_device", "grc_fit_orientation_nm", "grc_pair_spots",
-    "grc_walk_best_first", "grc_grow_best_first",
+    "grc_walk_best_first", "grc_grow_best_first", "grc_score_trials_argmax_device", "grc_forward_comp_argmax_device",
+    "grc_set_median", "grc_seed_candidates_device", "grc_seed_refine_device", "grc_local_grid_device",
+    "grc_map_key", "grc_upload_masks_if_changed",
 ]
 
 # grc_walk_score_fn of the C header
@@ -117,6 +119,14 @@ def load(path: str | None = None):
         "grc_fit_geometry_cost": [vp, f, i, f, f, f, f, f, i64, f],
         "grc_fit_geometry_rms": [vp, f, i, f, f, f, f, f, f, i64, f],
         "grc_score_trials_device": [vp, f, i64, f, i64, f, f, i64, f],
+        "grc_score_trials_argmax_device": [vp, f, i64, f, i64, f, f, i64, i64, f, f, f],
+        "grc_forward_comp_argmax_device": [vp, f, i64, f, i64, f, f, f],
+        "grc_set_median": [vp, i],
+        "grc_seed_candidates_device": [vp, f, i64, f, f, i64, i, f, f, f],
+        "grc_seed_refine_device": [vp, f, i64, f, i, i, d, i, f, f, f, f],
+        "grc_local_grid_device": [vp, f, i64, i, d, f, f],
+        "grc_map_key": [f, i64, i64],
+        "grc_upload_masks_if_changed": [vp, f, i64, i64, i64, i64, C.POINTER(i)],
         "grc_fit_orientation_nm": [vp, f, f, i64, d, i, i, d, d, f, f, f, f, f],
         "grc_pair_spots": [vp, f, f, i64, f, i64, f, f, i64, C.POINTER(i64)],
         "grc_walk_best_first": [WALK_SCORE_FN, vp, i64, i64, i64, f, f, f, f, f, d, d, d, d, f, f, f, f, f, i64,
@@ -129,9 +139,16 @@ def load(path: str | None = None):
         fn.argtypes = args
         fn.restype = i
     L.grc_last_error.restype = C.c_char_p
+    L.grc_map_key.restype = C.c_uint64
     L.grc_ctx_stream.restype = vp
     _lib = L
     return L
+
+
+def map_key(proj_bin_bw, samples: int = 1 << 20) -> int:
+    """grc_map_key of a host float32 map (no GPU needed)."""
+    a = f32(proj_bin_bw)
+    return int(load().grc_map_key(_ptr(a), a.size, samples))
 
 
 def _ptr(a):
@@ -279,6 +296,15 @@ class Context:
         else:  # a device array (torch tensor): ordered with the stream that produced it
             self._dev(self.L.grc_upload_masks, _ptr(proj_bin_bw), detzsize, detysize, nrot)
 
+    def upload_masks_if_changed(self, proj_bin_bw, detzsize: int, detysize: int, nrot: int,
+                                samples: int = 1 << 20) -> bool:
+        """Upload the map unless its content key and size equal the last keyed upload's."""
+        a = f32(proj_bin_bw)
+        up = C.c_int(0)
+        self._check(self.L.grc_upload_masks_if_changed(self.h, _ptr(a), detzsize, detysize, nrot, samples,
+                                                       C.byref(up)))
+        return bool(up.value)
+
     def set_geometry(self, S, B, hkl, rot_angles, RotDet, param):
         keep = [f32(x) for x in (S, B, hkl, rot_angles, RotDet, param)]
         self._check(self.L.grc_set_geometry(self.h, *[_ptr(a) for a in keep]))
@@ -401,11 +427,42 @@ class Context:
     def edt(self, d_mask, detzsize: int, detysize: int, nrot: int, d_map):
         self._dev(self.L.grc_edt, _ptr(d_mask), detzsize, detysize, nrot, _ptr(d_map))
 
+    def set_median(self, enable: bool):
+        """False: seeding scans count from the bit-packed hit mask and leave column 4 NaN."""
+        self._check(self.L.grc_set_median(self.h, 1 if enable else 0))
+
+    def forward_comp_argmax_device(self, d_pos, n_vox: int, d_q, n_q: int, d_out, d_best, d_best_c):
+        """Seeding scan plus the first maximum of completeness per voxel (d_out may be None)."""
+        self._dev(self.L.grc_forward_comp_argmax_device, _ptr(d_pos), n_vox, _ptr(d_q), n_q, _ptr(d_out),
+                  _ptr(d_best), _ptr(d_best_c))
+
+    def score_trials_argmax_device(self, d_pos, n_vox: int, d_q, n_q: int, d_trial_voxel, d_trial_orient,
+                                   n_trials: int, group_size: int, d_out, d_best, d_best_c):
+        """FP64 trial list plus the first maximum per group of ``group_size`` trials."""
+        self._dev(self.L.grc_score_trials_argmax_device, _ptr(d_pos), n_vox, _ptr(d_q), n_q, _ptr(d_trial_voxel),
+                  _ptr(d_trial_orient), n_trials, group_size, _ptr(d_out), _ptr(d_best), _ptr(d_best_c))
+
+    def seed_candidates_device(self, d_pos, n: int, d_q, n_q: int, n_top: int, d_idx, d_cand=None, d_out=None,
+                               d_q64=None):
+        """Seeding scan (completeness only) and the top ``n_top`` rows per seed."""
+        self._dev(self.L.grc_seed_candidates_device, _ptr(d_pos), n, _ptr(d_q), _ptr(d_q64), n_q, n_top, _ptr(d_idx),
+                  _ptr(d_cand), _ptr(d_out))
+
+    def seed_refine_device(self, d_pos, n: int, d_cand, k: int, nr: int, gridsize: float, d_best_q, d_best_c,
+                           d_order, n_x0: int = 0, d_x0=None):
+        """Local refine of every candidate: grid maxima in per-seed sortrows order (+ fit start points)."""
+        self._dev(self.L.grc_seed_refine_device, _ptr(d_pos), n, _ptr(d_cand), k, nr, gridsize, n_x0, _ptr(d_best_q),
+                  _ptr(d_best_c), _ptr(d_order), _ptr(d_x0))
+
+    def local_grid_device(self, d_cand, n_cand: int, nr: int, gridsize: float, d_rows, d_rows_f32=None):
+        """ori_local_sampling grids of n_cand quaternions in unique(q,'rows') order."""
+        self._dev(self.L.grc_local_grid_device, _ptr(d_cand), n_cand, nr, gridsize, _ptr(d_rows), _ptr(d_rows_f32))
+
     def set_timing(self, enable: bool):
         self._check(self.L.grc_set_timing(self.h, int(bool(enable))))
 
     def set_path(self, path: int):
-        """0 = by size, 1 = per-trial kernel, 2 = projection-window sweep."""
+        """0 = by size, 1 = per-trial kernel, 2 = CTA sweep, 3 = warp scan."""
         self._check(self.L.grc_set_path(self.h, int(path)))
 
     def last_stats(self) -> dict:

@@ -19,7 +19,7 @@ CSRC = os.path.join(PKG, "csrc")
 INC = os.path.join(ROOT, "include")
 LIB = os.path.join(PKG, "libgrainrecon_b200.so")
 BUILD_DIR = os.path.join(PKG, "_build")
-SOURCES = ["grc_score.cu", "grc_aux.cu", "grc_fit.cu", "grc_seed.cu", "grc_capi.cu", "grc_walk.cu"]
+SOURCES = ["grc_score.cu", "grc_scan.cu", "grc_select.cu", "grc_aux.cu", "grc_fit.cu", "grc_seed.cu", "grc_capi.cu", "grc_walk.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xptxas", "-warn-spills",
               "--expt-relaxed-constexpr"]

@@ -63,14 +63,14 @@ __global__ void pos_rows_k(const float *rows, int stride, int64_t n, const doubl
     }
 }
 
-__global__ void epi_forward_k(const TrialRes *res, int64_t n, float *out) {
+__global__ void epi_forward_k(const TrialRes *res, int64_t n, float *out, int median) {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
         const TrialRes r = res[i];
         float4 o;
         o.x = (float)r.simu;
         o.y = (float)r.inter;
         o.z = (float)((double)r.inter / (double)r.simu);  // Nr_intersect/Nr_simu, NaN for 0/0
-        o.w = (float)r.median;
+        o.w = median ? (float)r.median : CUDART_NAN_F;    // no median in completeness-only calls
         reinterpret_cast<float4 *>(out)[i] = o;
     }
 }
@@ -312,8 +312,8 @@ cudaError_t launch_pos_rows(const float *rows, int stride, int64_t n, const doub
     pos_rows_k<<<blocks_for(n), kB, 0, s>>>(rows, stride, n, p1, vpos);
     return cudaGetLastError();
 }
-cudaError_t launch_epi_forward(const TrialRes *res, int64_t n, float *out4, cudaStream_t s) {
-    epi_forward_k<<<blocks_for(n), kB, 0, s>>>(res, n, out4);
+cudaError_t launch_epi_forward(const TrialRes *res, int64_t n, float *out4, bool median, cudaStream_t s) {
+    epi_forward_k<<<blocks_for(n), kB, 0, s>>>(res, n, out4, median ? 1 : 0);
     return cudaGetLastError();
 }
 cudaError_t launch_epi_grow(const TrialRes *res, const float *rows6, int64_t m, const double *p1, float *out7,

@@ -48,7 +48,14 @@ struct grc_ctx {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     bool timing = false;
     bool timed_last = false;
-    int force_path = 0;  // 0 = by size, 1 = per-trial kernel, 2 = projection-window sweep
+    int force_path = 0;  // 0 = by size, 1 = per-trial kernel, 2 = CTA sweep, 3 = warp scan
+    bool median = true;  // seeding-scan entries: false = completeness only (bit-packed mask)
+    DevBuf bits, gkey;   // bit-packed hit mask of the resident map; per-group argmax keys
+    DevBuf sgrid, sgrid32, stv, sto, sbest;  // seeding-stage grids, trial lists, grid maxima
+    bool bits_ok = false;
+    uint32_t bits_hit = 0;
+    uint64_t map_key = 0;  // content key of the resident map (grc_upload_masks_if_changed), 0 = none
+    int64_t plane_words = 0;
     grc_stats stats{};
 };
 
@@ -114,6 +121,7 @@ void refresh_hit(grc_ctx *ctx) {
     size_t n = 0;
     while (n < ctx->h_vals.size() && (double)ctx->h_vals[n] <= thr) ++n;
     ctx->geo.n_hit = (uint32_t)n;
+    if (ctx->bits_hit != ctx->geo.n_hit) ctx->bits_ok = false;  // the packed mask follows the threshold
     ctx->geo.n_vals = (uint32_t)std::max<int64_t>(1, ctx->mc.n_distinct);
     int bits = 0;
     while (bits < 32 && (int64_t(1) << bits) < ctx->mc.n_distinct) ++bits;
@@ -235,6 +243,8 @@ int upload_device_map(grc_ctx *ctx, const float *d_map, int64_t dz, int64_t dy, 
         cudaFree(ctx->mc.vals);
     }
     ctx->mc = mc;
+    ctx->bits_ok = false;  // packed again from the new codes when first needed
+    ctx->map_key = 0;      // an upload that came without a key
     ctx->h_vals.swap(hv);
     ctx->mz = dz;
     ctx->my = dy;
@@ -278,6 +288,26 @@ int check_ready(grc_ctx *ctx) {
     return GRC_OK;
 }
 
+// Bit-packed hit mask of the resident map (bit = code < n_hit), built on the device the first time a
+// completeness-only scan needs it and again after a new map or threshold: 1 bit per pixel,
+// plane_words 32-bit words per projection (a 16-byte multiple).
+int ensure_bits(grc_ctx *ctx) {
+    const grc::Geo &g = ctx->geo;
+    if (ctx->bits_ok && ctx->bits_hit == g.n_hit) return GRC_OK;
+    const int64_t pw = (g.plane + 127) / 128 * 4;
+    TRY(ensure(ctx, ctx->bits, sizeof(uint32_t) * pw * g.nrot));
+    if (g.n_hit < 255u)
+        CU(grc::launch_pack_bits(ctx->mc.codes8, 1, g.plane, g.nrot, g.n_hit, pw, (uint32_t *)ctx->bits.p,
+                                 ctx->stream));
+    else
+        CU(grc::launch_pack_bits(ctx->mc.codes, g.code_bits <= 16 ? 2 : 4, g.plane, g.nrot, g.n_hit, pw,
+                                 (uint32_t *)ctx->bits.p, ctx->stream));
+    ctx->plane_words = pw;
+    ctx->bits_hit = g.n_hit;
+    ctx->bits_ok = true;
+    return GRC_OK;
+}
+
 grc::ScoreBufs bufs(grc_ctx *ctx) {
     grc::ScoreBufs b{};
     b.geo = (const grc::Geo *)ctx->geo_dev.p;
@@ -291,6 +321,8 @@ grc::ScoreBufs bufs(grc_ctx *ctx) {
     b.refine_list = (int64_t *)ctx->rlist.p;
     b.res = (grc::TrialRes *)ctx->res.p;
     b.work_counter = (int *)ctx->counter.p;
+    b.bits = ctx->bits_ok ? (const uint32_t *)ctx->bits.p : nullptr;
+    b.plane_words = ctx->plane_words;
     return b;
 }
 
@@ -302,9 +334,14 @@ int stage_geo(grc_ctx *ctx) {
     return GRC_OK;
 }
 
-int run_score(grc_ctx *ctx, const grc::Work &w, int64_t n_trials) {
+// Scores n_trials trials into ctx->res.  comp: completeness only (no median; the packed hit mask).
+// gkey (optional): first-maximum keys of every group of gsize consecutive trials, zeroed here.
+int run_score(grc_ctx *ctx, const grc::Work &w, int64_t n_trials, bool comp = false,
+              unsigned long long *gkey = nullptr, int64_t gsize = 0) {
     TRY(ensure(ctx, ctx->counter, 8 * sizeof(int)));
     TRY(stage_geo(ctx));
+    if (comp) TRY(ensure_bits(ctx));
+    if (gkey) CU(cudaMemsetAsync(gkey, 0, sizeof(unsigned long long) * ((n_trials + gsize - 1) / gsize), ctx->stream));
     int launches = 0;
     cudaEvent_t e0 = ctx->timing ? ctx->ev0 : nullptr, e1 = ctx->timing ? ctx->ev1 : nullptr;
     const int64_t round = ctx->force_path == 1 ? 0 : grc::sweep_round_trials(ctx->geo, ctx->num_sms);
@@ -317,24 +354,52 @@ int run_score(grc_ctx *ctx, const grc::Work &w, int64_t n_trials) {
     // kernels are within 3% of each other up to 16,384 trials.
     const bool shared_voxels = !w.items && !w.trial_voxel && !w.diag && w.n_or >= 64;
     const int64_t from = shared_voxels ? (round + 15) / 16 : (round + 1) / 2;
-    if (round > 0 && (ctx->force_path == 2 || n_trials >= from)) {
-        // projection-window sweep (L2-resident map windows) for large trial counts
+    bool fused_key = false;
+    if (round > 0 && (ctx->force_path >= 2 || n_trials >= from)) {
+        // projection-window scans (L2-resident map windows) for large trial counts: the CTA sweep,
+        // or the warp scan when asked for by grc_set_path(3)
         TRY(ensure(ctx, ctx->rlist, sizeof(int64_t) * n_trials));
-        e = grc::launch_sweep(ctx->geo, bufs(ctx), w, n_trials, ctx->num_sms, ctx->stream, e0, e1, &launches);
-        ctx->stats.path = 2;
+        grc::ScoreBufs b = bufs(ctx);
+        if (comp && gkey) {  // completeness mode folds the first maximum per group in
+            b.group_key = gkey;
+            b.group_size = gsize;
+            fused_key = true;
+        }
+        const int mode = comp ? grc::kScanComp : grc::kScanFull;
+        if (ctx->force_path == 3) {
+            e = grc::launch_scan(ctx->geo, b, w, n_trials, ctx->num_sms, mode, ctx->stream, e0, e1, &launches);
+            ctx->stats.path = 3;
+        } else {
+            e = grc::launch_sweep(ctx->geo, b, w, n_trials, ctx->num_sms, ctx->stream, e0, e1, &launches, 0, mode);
+            ctx->stats.path = 2;
+        }
     } else {
         e = grc::launch_score(ctx->geo, bufs(ctx), w, ctx->num_sms, ctx->stream, e0, e1, &launches);
         ctx->stats.path = 1;
     }
     if (e != cudaSuccess) return fail(ctx, GRC_ECUDA, "scorer launch: %s", cudaGetErrorString(e));
+    if (gkey && !fused_key) {
+        CU(grc::launch_group_argmax((const grc::TrialRes *)ctx->res.p, n_trials, gsize, gkey, ctx->stream));
+        ++launches;
+    }
     ctx->timed_last = ctx->timing;
     ctx->stats.trials = n_trials;
     ctx->stats.kernel_launches += launches;
     return GRC_OK;
 }
 
-// Seeding batch on device buffers: n_vox voxels x n_q orientations.
-int forward_device(grc_ctx *ctx, const float *d_pos, int64_t n_vox, const float *d_q, int64_t n_q, float *d_out) {
+// First maximum per group from the keys of run_score into best/best_c (either may be NULL).
+int decode_groups(grc_ctx *ctx, int64_t n_groups, int32_t *best, float *best_c) {
+    if (!best && !best_c) return GRC_OK;
+    CU(grc::launch_group_decode((const unsigned long long *)ctx->gkey.p, n_groups, best, best_c, ctx->stream));
+    ++ctx->stats.kernel_launches;
+    return GRC_OK;
+}
+
+// Seeding batch on device buffers: n_vox voxels x n_q orientations.  d_out (4 floats per trial)
+// may be NULL when only the first maximum per voxel (best, best_c) is wanted.
+int forward_device(grc_ctx *ctx, const float *d_pos, int64_t n_vox, const float *d_q, int64_t n_q, float *d_out,
+                   int32_t *best = nullptr, float *best_c = nullptr) {
     TRY(check_ready(ctx));
     ctx->stats = grc_stats{};
     if (n_vox <= 0 || n_q <= 0) return GRC_OK;
@@ -353,9 +418,17 @@ int forward_device(grc_ctx *ctx, const float *d_pos, int64_t n_vox, const float 
     w.chunk = (int32_t)chunk;
     w.chunks_per_voxel = (n_q + chunk - 1) / chunk;
     w.n_items = n_vox * w.chunks_per_voxel;
-    TRY(run_score(ctx, w, n_vox * n_q));
-    CU(grc::launch_epi_forward((const grc::TrialRes *)ctx->res.p, n_vox * n_q, d_out, ctx->stream));
-    ctx->stats.kernel_launches += 3;
+    const bool want_best = best || best_c;
+    if (want_best) TRY(ensure(ctx, ctx->gkey, sizeof(unsigned long long) * n_vox));
+    TRY(run_score(ctx, w, n_vox * n_q, !ctx->median, want_best ? (unsigned long long *)ctx->gkey.p : nullptr,
+                  n_q));
+    if (d_out) {
+        CU(grc::launch_epi_forward((const grc::TrialRes *)ctx->res.p, n_vox * n_q, d_out, ctx->median,
+                                   ctx->stream));
+        ++ctx->stats.kernel_launches;
+    }
+    if (want_best) TRY(decode_groups(ctx, n_vox, best, best_c));
+    ctx->stats.kernel_launches += 2;
     return GRC_OK;
 }
 
@@ -522,7 +595,8 @@ int grc_ctx_destroy(grc_ctx *ctx) {
         DevBuf *all[] = {&ctx->nm, &ctx->sp_keys, &ctx->sp_ids, &ctx->sp_keys2, &ctx->sp_ids2, &ctx->cell_cnt, &ctx->cell_off, &ctx->pr_raw, &ctx->pr_keys, &ctx->pr_keys2, &ctx->pr_ids, &ctx->pr_ids2, &ctx->pcount, &ctx->fgeo, &ctx->fne, &ctx->ftrial, &ctx->fcost0, &ctx->fcost1, &ctx->fimp, &ctx->fhw,
                          &ctx->tvoxel, &ctx->rlist, &ctx->geo_dev, &ctx->rot_cs, &ctx->hkl, &ctx->pos, &ctx->U, &ctx->res, &ctx->in1, &ctx->in2,
                          &ctx->in3, &ctx->out, &ctx->items, &ctx->torient, &ctx->counts, &ctx->offsets,
-                         &ctx->tmp, &ctx->counter, &ctx->p1, &ctx->bad};
+                         &ctx->tmp, &ctx->counter, &ctx->p1, &ctx->bad, &ctx->bits, &ctx->gkey,
+                         &ctx->sgrid, &ctx->sgrid32, &ctx->stv, &ctx->sto, &ctx->sbest};
         for (DevBuf *b : all) cudaFree(b->p);
         if (ctx->has_masks) {
             cudaFree(ctx->mc.codes);
@@ -828,15 +902,25 @@ int grc_compete_device(grc_ctx *ctx, const float *d_rows5, int64_t m, const floa
     return compete_device(ctx, d_rows5, m, d_id, n_neigb, d_euler, n_grain, param1, d_out, d_trial_out);
 }
 
-int grc_score_trials_device(grc_ctx *ctx, const double *d_pos, int64_t n_vox, const double *d_q, int64_t n_q,
-                            const int32_t *d_tv, const int32_t *d_to, int64_t n_trials, float *d_out) {
-    if (!ctx) return GRC_EINVAL;
-    Lock l(ctx);
+}  // extern "C"
+
+namespace {
+
+// grc_score_trials_device and its argmax form (context lock held).  d_out may be NULL when
+// group_size > 0 (first maximum per group only).
+int score_trials(grc_ctx *ctx, const double *d_pos, int64_t n_vox, const double *d_q, int64_t n_q,
+                 const int32_t *d_tv, const int32_t *d_to, int64_t n_trials, float *d_out, int64_t group_size,
+                 int32_t *best, float *best_c) {
     TRY(check_ready(ctx));
     ctx->stats = grc_stats{};
     if (n_trials < 0 || n_vox < 0 || n_q < 0) return fail(ctx, GRC_EINVAL, "negative size");
+    if (group_size < 0 || (group_size > 0 && n_trials % group_size != 0))
+        return fail(ctx, GRC_EINVAL, "trials: n_trials must be a multiple of group_size");
     if (n_trials == 0) return GRC_OK;
-    if (!d_pos || !d_q || !d_out || n_vox < 1 || n_q < 1) return fail(ctx, GRC_EINVAL, "trials: NULL buffer or no rows");
+    if (!d_pos || !d_q || (!d_out && group_size == 0) || n_vox < 1 || n_q < 1)
+        return fail(ctx, GRC_EINVAL, "trials: NULL buffer or no rows");
+    TRY(need_device(ctx, best, "trials: d_best"));
+    TRY(need_device(ctx, best_c, "trials: d_best_c"));
     TRY(need_device(ctx, d_pos, "trials: d_pos"));
     TRY(need_device(ctx, d_q, "trials: d_q"));
     TRY(need_device(ctx, d_out, "trials: d_out"));
@@ -876,9 +960,195 @@ int grc_score_trials_device(grc_ctx *ctx, const double *d_pos, int64_t n_vox, co
         w.chunks_per_voxel = 1;
         w.n_items = n_trials;
     }
-    TRY(run_score(ctx, w, n_trials));
-    CU(grc::launch_epi_forward((const grc::TrialRes *)ctx->res.p, n_trials, d_out, ctx->stream));
-    ctx->stats.kernel_launches += 3 + (d_tv ? 1 : 0);
+    const int64_t n_groups = group_size > 0 ? n_trials / group_size : 0;
+    if (n_groups > 0) TRY(ensure(ctx, ctx->gkey, sizeof(unsigned long long) * n_groups));
+    TRY(run_score(ctx, w, n_trials, !ctx->median, n_groups > 0 ? (unsigned long long *)ctx->gkey.p : nullptr,
+                  group_size));
+    if (d_out) {
+        CU(grc::launch_epi_forward((const grc::TrialRes *)ctx->res.p, n_trials, d_out, ctx->median, ctx->stream));
+        ++ctx->stats.kernel_launches;
+    }
+    if (n_groups > 0) TRY(decode_groups(ctx, n_groups, best, best_c));
+    ctx->stats.kernel_launches += 2 + (d_tv ? 1 : 0);
+    return GRC_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int grc_score_trials_device(grc_ctx *ctx, const double *d_pos, int64_t n_vox, const double *d_q, int64_t n_q,
+                            const int32_t *d_tv, const int32_t *d_to, int64_t n_trials, float *d_out) {
+    if (!ctx) return GRC_EINVAL;
+    Lock l(ctx);
+    return score_trials(ctx, d_pos, n_vox, d_q, n_q, d_tv, d_to, n_trials, d_out, 0, nullptr, nullptr);
+}
+
+int grc_score_trials_argmax_device(grc_ctx *ctx, const double *d_pos, int64_t n_vox, const double *d_q, int64_t n_q,
+                                   const int32_t *d_tv, const int32_t *d_to, int64_t n_trials, int64_t group_size,
+                                   float *d_out, int32_t *d_best, float *d_best_c) {
+    if (!ctx) return GRC_EINVAL;
+    Lock l(ctx);
+    if (group_size < 1) return fail(ctx, GRC_EINVAL, "trials: group_size must be positive");
+    return score_trials(ctx, d_pos, n_vox, d_q, n_q, d_tv, d_to, n_trials, d_out, group_size, d_best, d_best_c);
+}
+
+int grc_forward_comp_argmax_device(grc_ctx *ctx, const float *d_pos, int64_t n_vox, const float *d_q, int64_t n_q,
+                                   float *d_out, int32_t *d_best, float *d_best_c) {
+    if (!ctx) return GRC_EINVAL;
+    Lock l(ctx);
+    if (n_vox < 0 || n_q < 0) return fail(ctx, GRC_EINVAL, "negative size");
+    if (n_vox > 0 && n_q > 0) {
+        if (!d_pos || !d_q) return fail(ctx, GRC_EINVAL, "NULL device buffer");
+        TRY(need_device(ctx, d_pos, "d_pos"));
+        TRY(need_device(ctx, d_q, "d_q"));
+        TRY(need_device(ctx, d_out, "d_out"));
+        TRY(need_device(ctx, d_best, "d_best"));
+        TRY(need_device(ctx, d_best_c, "d_best_c"));
+    }
+    return forward_device(ctx, d_pos, n_vox, d_q, n_q, d_out, d_best, d_best_c);
+}
+
+int grc_seed_candidates_device(grc_ctx *ctx, const float *d_pos, int64_t n, const float *d_q, const double *d_q64,
+                               int64_t n_q, int n_top, int32_t *d_idx, double *d_cand, float *d_out) {
+    if (!ctx) return GRC_EINVAL;
+    Lock l(ctx);
+    if (n < 0 || n_q < 0) return fail(ctx, GRC_EINVAL, "seed candidates: negative size");
+    if (n == 0) return GRC_OK;
+    if (!d_pos || !d_q || !d_idx || n_q < 1) return fail(ctx, GRC_EINVAL, "seed candidates: NULL buffer");
+    if (n_top < 1 || n_top > 4096 || n_top > n_q)
+        return fail(ctx, GRC_EINVAL, "seed candidates: n_top must lie in 1..min(4096, n_q)");
+    if (n > (int64_t)INT32_MAX || n_q > (int64_t)INT32_MAX) return fail(ctx, GRC_ECAPACITY, "seed candidates: too many rows");
+    TRY(need_device(ctx, d_pos, "d_pos"));
+    TRY(need_device(ctx, d_q, "d_q"));
+    TRY(need_device(ctx, d_q64, "d_q64"));
+    TRY(need_device(ctx, d_idx, "d_idx"));
+    TRY(need_device(ctx, d_cand, "d_cand"));
+    TRY(need_device(ctx, d_out, "d_out"));
+    const bool med = ctx->median;
+    ctx->median = false;  // the engine reads column 3 only
+    const int rc = forward_device(ctx, d_pos, n, d_q, n_q, d_out);
+    ctx->median = med;
+    TRY(rc);
+    CU(grc::launch_top_rows(nullptr, (const grc::TrialRes *)ctx->res.p, 1, n, n_q, n_top, d_idx, ctx->stream));
+    int launches = 1;
+    if (d_cand) {
+        CU(grc::launch_gather_rows(d_idx, n, n_top, n_q, d_q64 ? nullptr : d_q, d_q64, 0, 4, d_cand, ctx->stream));
+        ++launches;
+    }
+    ctx->stats.kernel_launches += launches;
+    return GRC_OK;
+}
+
+int grc_seed_refine_device(grc_ctx *ctx, const double *d_pos, int64_t n, const double *d_cand, int k, int nr,
+                           double gridsize, int n_x0, double *d_best_q, float *d_best_c, int32_t *d_order,
+                           double *d_x0) {
+    if (!ctx) return GRC_EINVAL;
+    Lock l(ctx);
+    if (n < 0 || k < 0) return fail(ctx, GRC_EINVAL, "seed refine: negative size");
+    if (n == 0 || k == 0) return GRC_OK;
+    if (!d_pos || !d_cand || !d_best_q || !d_best_c || !d_order) return fail(ctx, GRC_EINVAL, "seed refine: NULL buffer");
+    if (nr < 0 || grc::local_grid_rows(nr) > 1024 || !(gridsize > 0))
+        return fail(ctx, GRC_EINVAL, "seed refine: nr must give at most 1024 grid rows, gridsize > 0");
+    if (k > 4096) return fail(ctx, GRC_EINVAL, "seed refine: at most 4096 candidates per seed");
+    if (d_x0 && (n_x0 < 1 || n_x0 > k)) return fail(ctx, GRC_EINVAL, "seed refine: n_x0 must lie in 1..k");
+    const int64_t L = grc::local_grid_rows(nr), n_cand = n * (int64_t)k, n_trials = n_cand * L;
+    if (n_trials > (int64_t)INT32_MAX) return fail(ctx, GRC_ECAPACITY, "seed refine: more than 2^31-1 trials");
+    TRY(need_device(ctx, d_pos, "d_pos"));
+    TRY(need_device(ctx, d_cand, "d_cand"));
+    TRY(need_device(ctx, d_best_q, "d_best_q"));
+    TRY(need_device(ctx, d_best_c, "d_best_c"));
+    TRY(need_device(ctx, d_order, "d_order"));
+    TRY(need_device(ctx, d_x0, "d_x0"));
+    TRY(ensure(ctx, ctx->sgrid, sizeof(double) * 4 * n_trials));
+    TRY(ensure(ctx, ctx->sgrid32, sizeof(double) * 4 * n_trials));
+    TRY(ensure(ctx, ctx->stv, sizeof(int32_t) * n_trials));
+    TRY(ensure(ctx, ctx->sto, sizeof(int32_t) * n_trials));
+    TRY(ensure(ctx, ctx->sbest, sizeof(int32_t) * n_cand + sizeof(float) * n_cand + sizeof(double) * 4 * n_cand));
+    int32_t *gbest = (int32_t *)ctx->sbest.p;                                   // grid row of each maximum
+    float *cbest = (float *)(gbest + n_cand);                                   // its completeness
+    double *qbest = (double *)(((uintptr_t)(cbest + n_cand) + 15) & ~(uintptr_t)15);  // its FP64 grid row
+    CU(grc::launch_local_grid(d_cand, n_cand, nr, gridsize, (double *)ctx->sgrid.p, (double *)ctx->sgrid32.p, nullptr,
+                              ctx->stream));
+    CU(grc::launch_block_lists(n_trials, (int64_t)k * L, (int32_t *)ctx->stv.p, (int32_t *)ctx->sto.p, ctx->stream));
+    const bool med = ctx->median;
+    ctx->median = false;  // fit_OR_constrain_with_local_comp_cuda.m:105 reads column 3 only
+    const int rc = score_trials(ctx, d_pos, n, (const double *)ctx->sgrid32.p, n_trials, (const int32_t *)ctx->stv.p,
+                                (const int32_t *)ctx->sto.p, n_trials, nullptr, L, gbest, cbest);
+    ctx->median = med;
+    TRY(rc);
+    // each candidate's maximum as its FP64 grid row, then the candidates of every seed in
+    // sortrows(Output_max, 3, 'descend') order (:112): rows, completeness, candidate index, x0
+    CU(grc::launch_gather_rows(gbest, n_cand, 1, L, nullptr, (const double *)ctx->sgrid.p, L, 4, qbest, ctx->stream));
+    CU(grc::launch_top_rows(cbest, nullptr, 1, n, k, k, d_order, ctx->stream));
+    CU(grc::launch_gather_rows(d_order, n, k, k, nullptr, qbest, k, 4, d_best_q, ctx->stream));
+    CU(grc::launch_gather_floats(d_order, n, k, k, cbest, k, d_best_c, ctx->stream));
+    int launches = 6;
+    if (d_x0) {
+        CU(grc::launch_take_x0(d_best_q, n, k, n_x0, d_x0, ctx->stream));
+        ++launches;
+    }
+    ctx->stats.kernel_launches += launches;
+    return GRC_OK;
+}
+
+int grc_local_grid_device(grc_ctx *ctx, const double *d_cand, int64_t n_cand, int nr, double gridsize,
+                          double *d_rows, float *d_rows_f32) {
+    if (!ctx) return GRC_EINVAL;
+    Lock l(ctx);
+    if (n_cand < 0) return fail(ctx, GRC_EINVAL, "local grid: negative size");
+    if (n_cand == 0) return GRC_OK;
+    if (!d_cand || !d_rows) return fail(ctx, GRC_EINVAL, "local grid: NULL buffer");
+    if (nr < 0 || grc::local_grid_rows(nr) > 1024 || !(gridsize > 0))
+        return fail(ctx, GRC_EINVAL, "local grid: nr must give at most 1024 grid rows, gridsize > 0");
+    TRY(need_device(ctx, d_cand, "d_cand"));
+    TRY(need_device(ctx, d_rows, "d_rows"));
+    TRY(need_device(ctx, d_rows_f32, "d_rows_f32"));
+    CU(grc::launch_local_grid(d_cand, n_cand, nr, gridsize, d_rows, nullptr, d_rows_f32, ctx->stream));
+    return GRC_OK;
+}
+
+uint64_t grc_map_key(const float *map, int64_t n, int64_t samples) {
+    // FNV-1a over n and the bit patterns of the sampled values (every value when n <= samples)
+    uint64_t h = 1469598103934665603ull;
+    auto mix = [&](uint64_t v) {
+        for (int b = 0; b < 8; ++b) {
+            h ^= (v >> (8 * b)) & 0xffu;
+            h *= 1099511628211ull;
+        }
+    };
+    mix((uint64_t)n);
+    if (!map || n <= 0) return h | 1;
+    if (samples <= 0 || samples > n) samples = n;
+    for (int64_t k = 0; k < samples; ++k) {
+        const int64_t i = samples == n ? k : (int64_t)((__int128)k * (n - 1) / (samples - 1 > 0 ? samples - 1 : 1));
+        uint32_t bits;
+        std::memcpy(&bits, map + i, 4);
+        mix(((uint64_t)i << 32) | bits);
+    }
+    return h | 1;  // never 0, the "no key" value
+}
+
+int grc_upload_masks_if_changed(grc_ctx *ctx, const float *map, int64_t detzsize, int64_t detysize, int64_t nrot,
+                                int64_t samples, int *uploaded) {
+    if (!ctx) return GRC_EINVAL;
+    Lock l(ctx);
+    if (uploaded) *uploaded = 0;
+    if (!map) return fail(ctx, GRC_EINVAL, "proj_bin_bw is NULL");
+    if (detzsize < 1 || detysize < 1 || nrot < 1) return fail(ctx, GRC_EINVAL, "distance-map dimensions must be positive");
+    const uint64_t key = grc_map_key(map, detzsize * detysize * nrot, samples);
+    if (ctx->has_masks && ctx->map_key == key && ctx->mz == detzsize && ctx->my == detysize && ctx->mrot == nrot)
+        return GRC_OK;
+    TRY(upload_host_map(ctx, map, detzsize, detysize, nrot));
+    ctx->map_key = key;
+    if (uploaded) *uploaded = 1;
+    return GRC_OK;
+}
+
+int grc_set_median(grc_ctx *ctx, int enable) {
+    if (!ctx) return GRC_EINVAL;
+    Lock l(ctx);
+    ctx->median = enable != 0;
     return GRC_OK;
 }
 
@@ -1087,7 +1357,7 @@ int grc_last_stats(grc_ctx *ctx, grc_stats *out) {
 }
 
 int grc_set_path(grc_ctx *ctx, int path) {
-    if (!ctx || path < 0 || path > 2) return GRC_EINVAL;
+    if (!ctx || path < 0 || path > 3) return GRC_EINVAL;
     Lock l(ctx);
     ctx->force_path = path;
     return GRC_OK;
@@ -1233,7 +1503,7 @@ extern "C" int grc_forward_comp_noalloc(grc_ctx *ctx, const float *pos, const fl
     int launches = 0;
     cudaError_t e = grc::launch_score(ctx->geo, b, w, ctx->num_sms, ctx->stream, nullptr, nullptr, &launches);
     if (e != cudaSuccess) return fail(ctx, GRC_ECUDA, "noalloc scorer launch: %s", cudaGetErrorString(e));
-    CU(grc::launch_epi_forward(b.res, n_q, d_out, ctx->stream));
+    CU(grc::launch_epi_forward(b.res, n_q, d_out, true, ctx->stream));
     CU(cudaStreamSynchronize(ctx->stream));
     ctx->stats.trials = n_q;
     ctx->stats.kernel_launches = launches + 2;
@@ -1300,10 +1570,14 @@ int batch_enqueue(grc_batch *bt, float *d_out8, float *d_trial_out, int path, in
     w.n_items = m_lim;
     cudaError_t e = cudaSuccess;
     if (T > 0) {
-        const bool sweep = path == 2 || (path == 0 && grc::sweep_round_trials(ctx->geo, ctx->num_sms) > 0 &&
-                                         T * 2 >= grc::sweep_round_trials(ctx->geo, ctx->num_sms));
-        if (sweep && grc::sweep_round_trials(ctx->geo, ctx->num_sms) > 0)
+        // path 1: per-trial kernel; 2 (and 0 from half a round on): CTA sweep; 3: warp scan
+        const int64_t sr = grc::sweep_round_trials(ctx->geo, ctx->num_sms);
+        const int use = sr == 0 ? 1 : (path != 0 ? path : (T * 2 >= sr ? 2 : 1));
+        if (use == 2)
             e = grc::launch_sweep(ctx->geo, b, w, T, ctx->num_sms, ctx->stream, e0, e1, launches, slots);
+        else if (use == 3)
+            e = grc::launch_scan(ctx->geo, b, w, T, ctx->num_sms, grc::kScanFull, ctx->stream, e0, e1, launches,
+                                 slots);
         else
             e = grc::launch_score(ctx->geo, b, w, ctx->num_sms, ctx->stream, e0, e1, launches);
         if (e != cudaSuccess) return fail(ctx, GRC_ECUDA, "batch scorer launch: %s", cudaGetErrorString(e));
@@ -1486,7 +1760,7 @@ extern "C" int grc_batch_autotune(grc_batch *bt, float *d_out8, int64_t max_voxe
     struct Cand {
         int path, slots;
     };
-    const Cand cands[] = {{1, 0}, {2, 16}, {2, 32}, {2, 48}, {2, 64}};
+    const Cand cands[] = {{1, 0}, {2, 16}, {2, 32}, {2, 48}, {2, 64}, {3, 16}, {3, 32}, {3, 48}, {3, 64}};
     cudaEvent_t a, z;
     CU(cudaEventCreate(&a));
     CU(cudaEventCreate(&z));
@@ -1494,7 +1768,7 @@ extern "C" int grc_batch_autotune(grc_batch *bt, float *d_out8, int64_t max_voxe
     Cand pick{0, 0};
     int rc = GRC_OK;
     for (const Cand &c : cands) {
-        if (c.path == 2 && grc::sweep_round_trials(ctx->geo, ctx->num_sms) == 0) continue;
+        if (c.path >= 2 && grc::sweep_round_trials(ctx->geo, ctx->num_sms) == 0) continue;
         double t_best = 1e300;
         for (int rep = 0; rep < 2 && rc == GRC_OK; ++rep) {
             int launches = 0;

@@ -76,6 +76,11 @@ struct ScoreBufs {
     TrialRes *res;
     int *work_counter;        // 8 ints: [0..1] main-pass item counter (u64), [2..3] refine-pass
                               // item counter (u64), [4] trials left for the refine pass
+    const uint32_t *bits;     // hit mask, 1 bit per pixel (code < n_hit): plane_words words per
+                              // projection, pixel (dety-1)*detzsize + (detz-1) at bit p&31 of word p>>5
+    int64_t plane_words;
+    unsigned long long *group_key;  // optional first-maximum key per group of group_size trials
+    int64_t group_size;
 };
 
 size_t score_smem_bytes(int nrot, int nhkl);
@@ -86,10 +91,48 @@ cudaError_t launch_score(const Geo &g, const ScoreBufs &b, const Work &w, int nu
 // Trials one round of the projection-window sweep holds (grid x slots); 0 if the sweep
 // cannot serve this geometry.
 int64_t sweep_round_trials(const Geo &g, int num_sms);
-// Enqueue the projection-window sweep over n_trials trials (+ the list refine pass).
-// max_slots (1..64) caps the trials each CTA holds per round (tile height); 0 = 64.
+// Enqueue the radix refine pass over the trials a sweep listed (work_counter[4] of them).
+cudaError_t launch_refine_list(const Geo &g, const ScoreBufs &b, const Work &w, int num_sms, cudaStream_t s);
+// Trial scan with one trial per warp at a time (grc_scan.cu).  mode 0: counts and the exact median
+// from the 8-bit codes (+ the list refine pass); mode 1: counts only, from the bit-packed hit mask
+// (median NaN).  With b.group_key set, the first maximum of completeness of every group of
+// b.group_size consecutive trials is folded into group_key (group_key_of).
+constexpr int kScanFull = 0, kScanComp = 1;
+int64_t scan_round_trials(const Geo &g, int num_sms);
+cudaError_t launch_scan(const Geo &g, const ScoreBufs &b, const Work &w, int64_t n_trials, int num_sms, int mode,
+                        cudaStream_t s, cudaEvent_t ev0, cudaEvent_t ev1, int *launches, int max_slots = 0);
+// Seeding-stage ordering (grc_select.cu).  top_rows: per group of gsize rows, the indices of the
+// first n_top rows of sortrows(.., 'descend') on completeness (NaN first, stable) -- from a float
+// column (vals, stride floats apart) or, with vals NULL, from the trial results.  n_top <= 4096.
+cudaError_t launch_top_rows(const float *vals, const TrialRes *res, int64_t stride, int64_t n_groups, int64_t gsize,
+                            int n_top, int32_t *idx, cudaStream_t s);
+// out[(g*n_top + k)*row_len + c] = source row idx[g*n_top + k] + g*src_group_stride (float rows
+// widened to double, or double rows).
+cudaError_t launch_gather_rows(const int32_t *idx, int64_t n_groups, int n_top, int64_t gsize, const float *src_f,
+                               const double *src_d, int64_t src_group_stride, int row_len, double *out,
+                               cudaStream_t s);
+// out[g*n_top + r] = src[g*src_stride + idx[g*n_top + r]].
+cudaError_t launch_gather_floats(const int32_t *idx, int64_t n_groups, int n_top, int64_t gsize, const float *src,
+                                 int64_t src_stride, float *out, cudaStream_t s);
+// x0[(s*n_x0 + j)*3 + c] = rows[(s*k + j)*4 + 1 + c]: (b, c, d) of each seed's first n_x0 rows.
+cudaError_t launch_take_x0(const double *rows, int64_t n, int k, int n_x0, double *x0, cudaStream_t s);
+// ori_local_sampling grids of n_cand quaternions (4 doubles each): local_grid_rows(nr) rows per
+// candidate in unique(q,'rows') order into out, and (optional) the same rows rounded to float32,
+// widened back to double (out_r32) or as floats (out_f32).
+int local_grid_rows(int nr);
+cudaError_t launch_local_grid(const double *cand, int64_t n_cand, int nr, double gridsize, double *out,
+                              double *out_r32, float *out_f32, cudaStream_t s);
+cudaError_t launch_block_lists(int64_t n, int64_t per_voxel, int32_t *voxel, int32_t *orient, cudaStream_t s);
+// Bit-packed hit mask from the 8-bit (or full-width) codes: bit = code < n_hit.
+cudaError_t launch_pack_bits(const void *codes, int code_bytes, int64_t plane, int64_t nrot, uint32_t n_hit,
+                             int64_t plane_words, uint32_t *bits, cudaStream_t s);
+// Enqueue the projection-window sweep over n_trials trials (+ the list refine pass in full mode).
+// max_slots (1..64) caps the trials each CTA holds per round (tile height); 0 = 64.  mode as
+// launch_scan: kScanFull (8-bit codes, median) or kScanComp (bit-packed mask, counts only, and
+// the first maximum per group when b.group_key is set).
 cudaError_t launch_sweep(const Geo &g, const ScoreBufs &b, const Work &w, int64_t n_trials, int num_sms,
-                         cudaStream_t s, cudaEvent_t ev0, cudaEvent_t ev1, int *launches, int max_slots = 0);
+                         cudaStream_t s, cudaEvent_t ev0, cudaEvent_t ev1, int *launches, int max_slots = 0,
+                         int mode = 0);
 
 // Orientation / position preparation kernels.
 cudaError_t launch_quat_to_u(const float *q, int64_t n, double *U, cudaStream_t s);
@@ -100,7 +143,15 @@ cudaError_t launch_pos_rows(const float *rows, int stride, int64_t n, const doub
                             cudaStream_t s);
 
 // Epilogues: TrialRes -> MEX output layouts.
-cudaError_t launch_epi_forward(const TrialRes *res, int64_t n, float *out4, cudaStream_t s);
+// median false: column 4 is NaN (completeness-only calls).
+cudaError_t launch_epi_forward(const TrialRes *res, int64_t n, float *out4, bool median, cudaStream_t s);
+// First maximum of completeness per group of gsize consecutive trials (one warp per group) into
+// keys (zeroed by the caller; atomicMax of the same keys the completeness scan folds in), and the
+// keys decoded into the 0-based index within the group and its completeness.
+cudaError_t launch_group_argmax(const TrialRes *res, int64_t n_trials, int64_t gsize, unsigned long long *keys,
+                                cudaStream_t s);
+cudaError_t launch_group_decode(const unsigned long long *keys, int64_t n_groups, int32_t *best, float *best_c,
+                                cudaStream_t s);
 cudaError_t launch_epi_grow(const TrialRes *res, const float *rows6, int64_t m, const double *p1, float *out7,
                             cudaStream_t s);
 // CSR set-up for compete: counts from rows5 -> items / trial_orient.

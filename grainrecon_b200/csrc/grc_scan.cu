@@ -1,0 +1,576 @@
+// grc_scan.cu -- projection-window trial scan, one trial per warp at a time.
+//
+// The same work as the sweep of grc_score.cu (forward_comp.m:18-90 for every trial of a round,
+// every CTA walking the projections window by window so the map pixels being read stay in L2),
+// organised around the warp instead of the CTA:
+//   * a warp takes one trial (slot) of the window at a time and first writes that trial's FP32
+//     Gw table and window thresholds for all reflections into its own shared-memory table, so
+//     the per-item landing reads them instead of recomputing S*U*B*h;
+//   * reflections are tested with lanes on projections: every lane holds the incident direction
+//     k_w of one projection of the window, and a reflection is tested only when a bound over the
+//     whole window (centre and radius of the window's k_w) lets its wavelength window be met.
+//     About half of the (reflection, window) pairs are skipped that way, without one test per
+//     projection;
+//   * the survivors of a trial go through a per-warp queue, 32 at a time, through the FP32 landing
+//     chain with its FP64 band (landing_fp32 / landing_exact), and their pixels are counted in
+//     registers of the warp (completeness-only mode: one bit of the packed hit mask per pixel) or
+//     in the trial's 8-bit code histogram (full mode: Nr_simu, Nr_intersect and the exact median).
+// Ambiguous items keep their trial in the FP64 queue, which is drained at the end of the window.
+// The decisions are those of the sweep and of the oracle: same prefilter margins, same FP32
+// chain and band, same FP64 path; the window bound only skips reflections whose prefilter test
+// fails on every projection of the window.
+#include <cuda_runtime.h>
+#include <math_constants.h>
+#include <stdint.h>
+
+#include "grc_chain.cuh"
+#include "grc_internal.h"
+
+#ifndef GRC_SCAN_BLOCKS
+#define GRC_SCAN_BLOCKS 3
+#endif
+
+namespace grc {
+namespace {
+
+constexpr int kScanSlots = 96;      // most trials a CTA holds in one round
+constexpr int kScanSlotsBulk = 64;  // tile of multi-round work and of explicit voxel lists
+constexpr int kScanWinMin = 8;
+constexpr int kScanQueue = 64;      // < 32 left over + one reflection of 32 projections
+constexpr int kHistWords = 128;     // 256 u16 bins per slot, two per word
+constexpr unsigned kAll = 0xffffffffu;
+
+__device__ __forceinline__ int64_t scan_voxel_of(const Work &w, int64_t t) {
+    if (w.trial_voxel) return (int64_t)w.trial_voxel[t];
+    if (w.diag) return t;
+    return t / w.n_or;
+}
+
+__device__ __forceinline__ int64_t scan_orient_of(const Work &w, int64_t t, int64_t v) {
+    if (w.trial_orient) return (int64_t)w.trial_orient[t];
+    return w.diag ? t : (t - v * w.n_or);
+}
+
+struct ScanSmem {
+    RowF *rows;        // [rows_cap * nwin] omega rows of the window, vloc * nwin + wl
+    float4 *kcr;       // [rows_cap] centre (x, y, z) and radius of the window's k_w per voxel
+    float4 *hk;        // [nhkl] h as float
+    uint32_t *hist;    // full mode: [slots * kHistWords]
+    int2 *cnt;         // completeness mode: [slots] (Nr_simu, Nr_intersect)
+    float *subf;       // [slots * 12]
+    double *subd;      // [slots * 9]
+    int *vloc;         // [slots]
+    int64_t *vglob;    // [slots]
+    int64_t *vlist;    // [slots]
+    float4 *wgw;       // [kWarps * nhkl] per-warp Gw table of the warp's trial: x, y, z, 1/|G|
+    float4 *wwin;      // [kWarps * nhkl] its window thresholds (window_f)
+    uint32_t *queue;   // [kWarps * kScanQueue]
+    uint32_t *fqueue;  // [kWarps * kFallbackCap]
+};
+
+constexpr int kScanParts = 13;
+__host__ __device__ inline size_t scan_smem_layout(int mode, int nhkl, int rows_cap, int slots, int nwin,
+                                                   size_t *offs) {
+    size_t o = 0, i = 0;
+    auto put = [&](size_t bytes) {
+        o = (o + 15) & ~size_t(15);
+        offs[i++] = o;
+        o += bytes;
+    };
+    put(sizeof(RowF) * rows_cap * nwin);
+    put(sizeof(float4) * rows_cap);
+    put(sizeof(float4) * nhkl);
+    put(mode == kScanFull ? sizeof(uint32_t) * slots * kHistWords : 0);
+    put(mode == kScanComp ? sizeof(int2) * slots : 0);
+    put(sizeof(float) * slots * 12);
+    put(sizeof(double) * slots * 9);
+    put(sizeof(int) * slots);
+    put(sizeof(int64_t) * slots);
+    put(sizeof(int64_t) * slots);
+    put(sizeof(float4) * kWarps * nhkl);
+    put(sizeof(float4) * kWarps * nhkl);
+    put(sizeof(uint32_t) * kWarps * kScanQueue);
+    o = (o + 15) & ~size_t(15);
+    offs[i] = o;  // fqueue
+    o += sizeof(uint32_t) * kWarps * kFallbackCap;
+    return (o + 15) & ~size_t(15);
+}
+
+__device__ __forceinline__ ScanSmem scan_carve(unsigned char *base, int mode, int nhkl, int rows_cap, int slots,
+                                               int nwin) {
+    size_t offs[kScanParts + 1];
+    scan_smem_layout(mode, nhkl, rows_cap, slots, nwin, offs);
+    ScanSmem m;
+    m.rows = (RowF *)(base + offs[0]);
+    m.kcr = (float4 *)(base + offs[1]);
+    m.hk = (float4 *)(base + offs[2]);
+    m.hist = (uint32_t *)(base + offs[3]);
+    m.cnt = (int2 *)(base + offs[4]);
+    m.subf = (float *)(base + offs[5]);
+    m.subd = (double *)(base + offs[6]);
+    m.vloc = (int *)(base + offs[7]);
+    m.vglob = (int64_t *)(base + offs[8]);
+    m.vlist = (int64_t *)(base + offs[9]);
+    m.wgw = (float4 *)(base + offs[10]);
+    m.wwin = (float4 *)(base + offs[11]);
+    m.queue = (uint32_t *)(base + offs[12]);
+    m.fqueue = (uint32_t *)(base + offs[13]);
+    return m;
+}
+
+__device__ __forceinline__ float warp_sum(float x) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(kAll, x, o);
+    return x;
+}
+
+__device__ __forceinline__ float warp_max(float x) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) x = fmaxf(x, __shfl_xor_sync(kAll, x, o));
+    return x;
+}
+
+template <int MODE, int HPL, int WIN>
+__global__ void __launch_bounds__(kThreads, GRC_SCAN_BLOCKS)
+    scan_kernel(Geo g, ScoreBufs b, Work w, int64_t round_base, int64_t n_trials, int rows_cap, int slots) {
+    const int64_t cta_base = round_base + (int64_t)blockIdx.x * slots;
+    if (cta_base >= n_trials) return;
+    const int nslot = (int)min((int64_t)slots, n_trials - cta_base);
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const ScanSmem sm = scan_carve(smem_raw, MODE, g.nhkl, rows_cap, slots, WIN);
+    __shared__ int s_nv, s_next;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const unsigned lt = (1u << lane) - 1u;
+    uint32_t *wq = sm.queue + warp * kScanQueue;
+    uint32_t *fq = sm.fqueue + warp * kFallbackCap;
+    float4 *gwt = sm.wgw + warp * g.nhkl;
+    float4 *wnt = sm.wwin + warp * g.nhkl;
+
+    // ---- set-up: per-slot S*U*B, voxels, zeroed counters
+    if (tid < nslot) {
+        const int64_t t = cta_base + tid;
+        const int64_t v = scan_voxel_of(w, t);
+        const int64_t o = scan_orient_of(w, t, v);
+        double SUB[9];
+        sub_matrix(g, b.U + 9 * o, SUB);
+#pragma unroll
+        for (int i = 0; i < 9; ++i) {
+            sm.subd[9 * tid + i] = SUB[i];
+            sm.subf[12 * tid + i] = (float)SUB[i];
+        }
+        sm.vglob[tid] = v;
+        if (MODE == kScanComp) sm.cnt[tid] = make_int2(0, 0);
+    }
+    if (MODE == kScanFull)
+        for (int i = tid; i < slots * kHistWords; i += kThreads) sm.hist[i] = 0;
+    for (int i = tid; i < g.nhkl; i += kThreads)
+        sm.hk[i] = make_float4((float)b.hkl[3 * i], (float)b.hkl[3 * i + 1], (float)b.hkl[3 * i + 2], 0.f);
+    __syncthreads();
+    if (tid == 0) {
+        int nv = 0;
+        for (int s = 0; s < nslot; ++s) {
+            if (s == 0 || sm.vglob[s] != sm.vglob[s - 1]) sm.vlist[nv++] = sm.vglob[s];
+            sm.vloc[s] = nv - 1;
+        }
+        s_nv = nv;
+    }
+    __syncthreads();
+    const int nv = s_nv;
+    const int64_t pw = b.plane_words;
+
+    for (int w0 = 0; w0 < g.nrot; w0 += WIN) {
+        const int nw = min(WIN, g.nrot - w0);
+        // ---- omega rows of this window for every voxel of the round
+        for (int i = tid; i < nv * nw; i += kThreads) {
+            const int vl = i / nw, wl = i - vl * nw;
+            sm.rows[vl * WIN + wl] = row_f32(g, omega_row(g, b.rot_cs[w0 + wl], b.vpos + 3 * sm.vlist[vl]));
+        }
+        if (tid == 0) s_next = 0;
+        __syncthreads();
+        // ---- per voxel: centre and radius of the window's k_w (lanes on projections).  The radius
+        // carries 1e-5 on top, far above the FP32 rounding of the prefilter's dot products.
+        for (int vl = warp; vl < nv; vl += kWarps) {
+            float kx = 0.f, ky = 0.f, kz = 0.f;
+            const bool in = lane < nw;
+            if (in) {
+                const float4 k4 = reinterpret_cast<const float4 *>(sm.rows + vl * WIN + lane)[3];
+                kx = k4.x;
+                ky = k4.y;
+                kz = k4.z;
+            }
+            const float inv = 1.0f / (float)nw;
+            const float cx = warp_sum(kx) * inv, cy = warp_sum(ky) * inv, cz = warp_sum(kz) * inv;
+            const float dx = kx - cx, dy = ky - cy, dz = kz - cz;
+            const float d = warp_max(in ? sqrtf(dx * dx + dy * dy + dz * dz) : 0.f);
+            if (lane == 0) sm.kcr[vl] = make_float4(cx, cy, cz, d * 1.0001f + 1e-5f);
+        }
+        __syncthreads();
+
+        const uint8_t *wcodes = MODE == kScanFull ? b.codes8 + (int64_t)w0 * g.plane : nullptr;
+        const uint32_t *wbits = MODE == kScanComp ? b.bits + (int64_t)w0 * pw : nullptr;
+        int fn = 0;  // ambiguous items of this warp (any of its trials), drained at the window end
+
+        // FP64 path of one ambiguous item: counted at once (shared atomics; these items are rare)
+        auto exact = [&](uint32_t item, bool valid) {
+            const int s2 = (int)(item >> 16), wl = (int)((item >> 8) & 255u), ih = (int)(item & 255u);
+            if (!valid) return;
+            const int64_t r64 =
+                landing_exact(b.geo, b.rot_cs, b.vpos + 3 * sm.vglob[s2], b.hkl, sm.subd + 9 * s2, w0 + wl, ih);
+            if (r64 < 0) return;
+            if (MODE == kScanComp) {
+                const int64_t iw = w0 + wl, ip = r64 - iw * g.plane;
+                const uint32_t word = __ldg(b.bits + iw * pw + (ip >> 5));
+                atomicAdd(&sm.cnt[s2].x, 1);
+                if ((word >> (ip & 31)) & 1u) atomicAdd(&sm.cnt[s2].y, 1);
+            } else {
+                const uint32_t code = __ldg(b.codes8 + r64);
+                atomicAdd(&sm.hist[s2 * kHistWords + (code >> 1)], 1u << ((code & 1u) * 16));
+            }
+        };
+        auto drain_exact = [&](bool all) {
+            while (fn >= 32 || (all && fn > 0)) {
+                const int take = fn >= 32 ? 32 : fn;
+                fn -= take;
+                const bool v2 = lane < take;
+                const uint32_t it2 = v2 ? fq[fn + lane] : 0u;
+                __syncwarp();
+                exact(it2, v2);
+                __syncwarp();
+            }
+        };
+
+        // slots are handed out one at a time, so the warps of a CTA reach the end-of-window barrier
+        // together however unevenly the selected reflections fall on the slots
+        for (;;) {
+            int s = 0;
+            if (lane == 0) s = atomicAdd(&s_next, 1);
+            s = __shfl_sync(kAll, s, 0);
+            if (s >= nslot) break;
+            const int vl = sm.vloc[s];
+            const float4 kc = sm.kcr[vl];
+            const float *sf = sm.subf + 12 * s;
+            // ---- the trial's Gw table and the reflections its window bound keeps
+            unsigned live[HPL];
+#pragma unroll
+            for (int j = 0; j < HPL; ++j) {
+                const int ih = lane + 32 * j;
+                bool ok = false;
+                if (ih < g.nhkl) {
+                    const float4 gv = gw_of(sf, sm.hk[ih]);
+                    const float4 wv = window_f(g, gv);
+                    gwt[ih] = gv;
+                    wnt[ih] = wv;
+                    const float Gn = (gv.x * gv.x + gv.y * gv.y + gv.z * gv.z) * gv.w;
+                    const float tc = -fmaf(kc.x, gv.x, fmaf(kc.y, gv.y, kc.z * gv.z));
+                    const float rg = kc.w * Gn;
+                    ok = (tc - rg < wv.y) && (tc + rg > wv.x);
+                }
+                live[j] = __ballot_sync(kAll, ok);
+            }
+            __syncwarp();
+            float kx = CUDART_NAN_F, ky = CUDART_NAN_F, kz = CUDART_NAN_F;
+            if (lane < nw) {
+                const float4 k4 = reinterpret_cast<const float4 *>(sm.rows + vl * WIN + lane)[3];
+                kx = k4.x;
+                ky = k4.y;
+                kz = k4.z;
+            }
+            const RowF *vr = sm.rows + vl * WIN;
+            int c_simu = 0, c_inter = 0;  // completeness mode: this trial's counts in this window
+            // a selected pixel is read when its batch is evaluated and counted after the next batch
+            // has been computed, so the gather's latency overlaps the landing arithmetic
+            bool pend_sel = false;
+            uint32_t pend_val = 0;
+            int pend_bit = 0;
+            auto apply_pending = [&]() {
+                if (MODE == kScanComp) {
+                    const bool hit = pend_sel && ((pend_val >> pend_bit) & 1u);
+                    c_simu += __popc(__ballot_sync(kAll, pend_sel));
+                    c_inter += __popc(__ballot_sync(kAll, hit));
+                } else if (pend_sel) {
+                    atomicAdd(&sm.hist[s * kHistWords + (pend_val >> 1)], 1u << ((pend_val & 1u) * 16));
+                }
+                pend_sel = false;
+            };
+            auto fast = [&](uint32_t item, bool valid) {
+                const int wl = (int)(item >> 8), ih = (int)(item & 255u);
+                int ip = -1;
+                if (valid) {
+                    const float4 gv = gwt[ih];
+                    const float4 wv = wnt[ih];
+                    ip = landing_fp32(g, vr[wl], gv, wv.z, wv.w);
+                }
+                const bool amb = ip == -2;
+                const unsigned m = __ballot_sync(kAll, amb);
+                if (amb) fq[fn + __popc(m & lt)] = ((uint32_t)s << 16) | item;
+                fn += __popc(m);
+                const bool sel = ip >= 0;
+                uint32_t val = 0;
+                if (sel) {
+                    if (MODE == kScanComp)
+                        val = __ldg(wbits + (int64_t)wl * pw + (ip >> 5));
+                    else
+                        val = __ldg(wcodes + (int64_t)wl * g.plane + ip);
+                }
+                apply_pending();
+                pend_sel = sel;
+                pend_val = val;
+                pend_bit = ip & 31;
+            };
+            int qn = 0;
+#pragma unroll
+            for (int j = 0; j < HPL; ++j) {
+                unsigned m = live[j];
+                while (m) {
+                    const int ih = 32 * j + __ffs(m) - 1;
+                    m &= m - 1;
+                    const float4 gv = gwt[ih];
+                    const float4 wv = wnt[ih];
+                    const float t = -fmaf(kx, gv.x, fmaf(ky, gv.y, kz * gv.z));
+                    const bool pass = (t > wv.x) && (t < wv.y);
+                    const unsigned bm = __ballot_sync(kAll, pass);
+                    if (pass) wq[qn + __popc(bm & lt)] = ((uint32_t)lane << 8) | (uint32_t)ih;
+                    qn += __popc(bm);
+                    if (qn >= 32) {
+                        __syncwarp();
+                        qn -= 32;
+                        const uint32_t item = wq[qn + lane];
+                        __syncwarp();
+                        fast(item, true);
+                        __syncwarp();
+                        drain_exact(false);
+                    }
+                }
+            }
+            __syncwarp();
+            if (qn > 0) {  // the trial's last, partial batch
+                const bool valid = lane < qn;
+                const uint32_t item = valid ? wq[lane] : 0u;
+                __syncwarp();
+                fast(item, valid);
+                __syncwarp();
+                drain_exact(false);
+            }
+            apply_pending();
+            if (MODE == kScanComp && lane == 0) {
+                atomicAdd(&sm.cnt[s].x, c_simu);
+                atomicAdd(&sm.cnt[s].y, c_inter);
+            }
+        }
+        drain_exact(true);
+        __syncthreads();  // rows are rebuilt for the next window
+    }
+
+    // ---- finalize
+    if constexpr (MODE == kScanFull) {
+        for (int s = warp; s < nslot; s += kWarps) hist8_finish(g, b, sm.hist + s * kHistWords, cta_base + s);
+    } else {
+    for (int base = warp * 32; base < nslot; base += kWarps * 32) {
+        const int s = base + lane;
+        const bool in = s < nslot;
+        const int64_t t = cta_base + s;
+        int simu = 0, inter = 0;
+        if (in) {
+            const int2 c = sm.cnt[s];
+            simu = c.x;
+            inter = c.y;
+            TrialRes r;
+            r.simu = simu;
+            r.inter = inter;
+            r.median = CUDART_NAN;  // not computed in this mode
+            b.res[t] = r;
+        }
+        if (b.group_key) fold_group_key(b, in, t, simu, inter);
+    }
+    }
+}
+
+template <int MODE, int HPL>
+cudaError_t launch_scan_t(const Geo &g, const ScoreBufs &b, const Work &w, int64_t n_trials, int num_sms,
+                          cudaStream_t s, cudaEvent_t ev0, cudaEvent_t ev1, int *launches, int max_slots) {
+    // Tiles as the sweep: kScanSlotsBulk trials per CTA; an implicit seeding list may take up to
+    // kScanSlots when that fits the call into one round; explicit lists keep one row set per
+    // voxel-run start of their aligned 32-trial blocks.
+    const bool explicit_voxels = w.trial_voxel || w.diag || w.n_or <= 0;
+    const bool caller_tile = max_slots >= 1 && max_slots <= kScanSlots;
+    if (!caller_tile) max_slots = kScanSlotsBulk;
+    auto rows_for = [&](int sl) {
+        int rc = (int)(w.n_or >= sl ? 2 : (w.n_or > 0 ? sl / w.n_or + 2 : sl));
+        if (explicit_voxels) rc = w.starts_per_32 > 0 ? 1 + ((sl + 31) / 32 + 1) * w.starts_per_32 : sl;
+        return rc > sl ? sl : rc;
+    };
+    size_t offs[kScanParts + 1];
+    using ScanFn = void (*)(Geo, ScoreBufs, Work, int64_t, int64_t, int, int);
+    const ScanFn k8 = scan_kernel<MODE, HPL, kScanWinMin>;
+    const size_t smem_max = scan_smem_layout(MODE, g.nhkl, rows_for(max_slots), max_slots, kScanWinMin, offs);
+    cudaError_t e = cudaFuncSetAttribute(k8, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_max);
+    if (e != cudaSuccess) return e;
+    int per_sm = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k8, kThreads, smem_max);
+    if (e != cudaSuccess) return e;
+    if (per_sm < 1) return cudaErrorInvalidConfiguration;
+    const int64_t grid = (int64_t)per_sm * num_sms;
+    if (!caller_tile && !explicit_voxels && n_trials > grid * max_slots && n_trials <= grid * kScanSlots) {
+        int per_sm1 = 0;
+        const size_t smem1 = scan_smem_layout(MODE, g.nhkl, rows_for(kScanSlots), kScanSlots, kScanWinMin, offs);
+        if (cudaFuncSetAttribute(k8, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem1) == cudaSuccess &&
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm1, k8, kThreads, smem1) == cudaSuccess &&
+            per_sm1 == per_sm)
+            max_slots = kScanSlots;
+    }
+    const int64_t rounds = (n_trials + grid * max_slots - 1) / (grid * max_slots);
+    int slots = (int)((n_trials + rounds * grid - 1) / (rounds * grid));
+    if (slots < 1) slots = 1;
+    const int rows_cap = rows_for(slots);
+    // the widest projection window (32 or 16, else 8) whose rows keep the grid's CTAs per SM
+    ScanFn kern = k8;
+    size_t smem = scan_smem_layout(MODE, g.nhkl, rows_cap, slots, kScanWinMin, offs);
+    bool refused = false;
+    const int cands[2] = {32, 16};
+    for (int cand : cands) {
+        if (MODE == kScanFull && (int64_t)cand * g.plane > 2147483647LL) continue;
+        const ScanFn kc = cand == 32 ? (ScanFn)scan_kernel<MODE, HPL, 32> : (ScanFn)scan_kernel<MODE, HPL, 16>;
+        const size_t smem_c = scan_smem_layout(MODE, g.nhkl, rows_cap, slots, cand, offs);
+        int per_c = 0;
+        if (cudaFuncSetAttribute(kc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_c) != cudaSuccess ||
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_c, kc, kThreads, smem_c) != cudaSuccess) {
+            refused = true;
+            continue;
+        }
+        if (per_c >= per_sm) {
+            kern = kc;
+            smem = smem_c;
+            break;
+        }
+    }
+    if (refused) cudaGetLastError();  // a refused window query is not an error of this launch
+    e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    const int64_t per_round = grid * slots;
+    e = cudaMemsetAsync(b.work_counter, 0, 8 * sizeof(int), s);
+    if (e != cudaSuccess) return e;
+    if (ev0) cudaEventRecord(ev0, s);
+    for (int64_t base = 0; base < n_trials; base += per_round) {
+        const int64_t left = (n_trials - base + slots - 1) / slots;
+        const int gr = (int)(left < grid ? left : grid);
+        kern<<<gr, kThreads, smem, s>>>(g, b, w, base, n_trials, rows_cap, slots);
+        ++*launches;
+    }
+    if (ev1) cudaEventRecord(ev1, s);
+    if (MODE == kScanFull) {
+        e = launch_refine_list(g, b, w, num_sms, s);
+        if (e != cudaSuccess) return e;
+        ++*launches;
+    }
+    return cudaGetLastError();
+}
+
+template <typename CodeT>
+__global__ void pack_bits_k(const CodeT *codes, int64_t plane, int64_t nrot, uint32_t n_hit, int64_t pw,
+                            uint32_t *bits) {
+    // one thread per bit of the padded layout; a warp covers one 32-bit word
+    const int64_t per_plane = pw * 32, total = nrot * per_plane;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;  // a multiple of 32
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += stride) {
+        const int64_t iw = i / per_plane, p = i - iw * per_plane;
+        const bool hit = p < plane && (uint32_t)codes[iw * plane + p] < n_hit;
+        const unsigned m = __ballot_sync(kAll, hit);
+        if ((threadIdx.x & 31) == 0) bits[i >> 5] = m;
+    }
+}
+
+// One warp per group: the first maximum of completeness over the group's trials.
+__global__ void group_argmax_k(const TrialRes *res, int64_t n_trials, int64_t gsize, unsigned long long *keys) {
+    const int lane = threadIdx.x & 31;
+    const int64_t n_groups = (n_trials + gsize - 1) / gsize;
+    const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+    for (int64_t grp = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); grp < n_groups; grp += warps) {
+        const int64_t t0 = grp * gsize, n = min(gsize, n_trials - t0);
+        unsigned long long key = 0ull;
+        for (int64_t i = lane; i < n; i += 32) {
+            const TrialRes r = res[t0 + i];
+            const unsigned long long k = group_key_of(r.simu, r.inter, i);
+            key = k > key ? k : key;
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const unsigned long long y = shfl_xor_u64(key, o);
+            key = y > key ? y : key;
+        }
+        if (lane == 0) atomicMax(keys + grp, key);
+    }
+}
+
+__global__ void group_decode_k(const unsigned long long *keys, int64_t n_groups, int32_t *best, float *best_c) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n_groups; i += (int64_t)gridDim.x * blockDim.x) {
+        const unsigned long long k = keys[i];
+        const uint32_t hi = (uint32_t)(k >> 32), lo = (uint32_t)k;
+        if (best) best[i] = (int32_t)(0xffffffffu - lo);
+        if (best_c) best_c[i] = hi == 0u ? CUDART_NAN_F : __uint_as_float(hi - 1u);
+    }
+}
+
+}  // namespace
+
+cudaError_t launch_group_argmax(const TrialRes *res, int64_t n_trials, int64_t gsize, unsigned long long *keys,
+                                cudaStream_t s) {
+    if (n_trials <= 0 || gsize <= 0) return cudaSuccess;
+    const int64_t n_groups = (n_trials + gsize - 1) / gsize;
+    const int64_t want = (n_groups + 7) / 8;
+    const int blocks = (int)(want < 65535 * 4 ? want : 65535 * 4);
+    group_argmax_k<<<blocks, 256, 0, s>>>(res, n_trials, gsize, keys);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_group_decode(const unsigned long long *keys, int64_t n_groups, int32_t *best, float *best_c,
+                                cudaStream_t s) {
+    if (n_groups <= 0) return cudaSuccess;
+    const int64_t want = (n_groups + 255) / 256;
+    const int blocks = (int)(want < 65535 ? want : 65535);
+    group_decode_k<<<blocks, 256, 0, s>>>(keys, n_groups, best, best_c);
+    return cudaGetLastError();
+}
+
+int64_t scan_round_trials(const Geo &g, int num_sms) {
+    // 16-bit histogram bins (full mode) and 13-bit items; hit codes below the saturation code
+    if (g.n_hit >= 255u || g.nhkl > 128 || (int64_t)g.nrot * g.nhkl > 65535 ||
+        (int64_t)kScanWinMin * g.plane > 2147483647LL)
+        return 0;
+    return (int64_t)num_sms * GRC_SCAN_BLOCKS * kScanSlotsBulk;
+}
+
+cudaError_t launch_scan(const Geo &g, const ScoreBufs &b, const Work &w, int64_t n_trials, int num_sms, int mode,
+                        cudaStream_t s, cudaEvent_t ev0, cudaEvent_t ev1, int *launches, int max_slots) {
+    const int hpl = (g.nhkl + 31) / 32;
+    if (mode == kScanComp && !b.bits) return cudaErrorInvalidValue;
+#define GRC_DISPATCH(H)                                                                                    \
+    if (hpl == H)                                                                                          \
+        return mode == kScanComp                                                                           \
+                   ? launch_scan_t<kScanComp, H>(g, b, w, n_trials, num_sms, s, ev0, ev1, launches, max_slots) \
+                   : launch_scan_t<kScanFull, H>(g, b, w, n_trials, num_sms, s, ev0, ev1, launches, max_slots);
+    GRC_DISPATCH(1)
+    GRC_DISPATCH(2)
+    GRC_DISPATCH(3)
+    GRC_DISPATCH(4)
+#undef GRC_DISPATCH
+    return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_pack_bits(const void *codes, int code_bytes, int64_t plane, int64_t nrot, uint32_t n_hit,
+                             int64_t plane_words, uint32_t *bits, cudaStream_t s) {
+    const int64_t total = nrot * plane_words * 32;
+    const int threads = 256;
+    const int64_t want = (total + threads - 1) / threads;
+    const int blocks = (int)(want < 65535 * 8 ? want : 65535 * 8);
+    if (code_bytes == 1)
+        pack_bits_k<uint8_t><<<blocks, threads, 0, s>>>((const uint8_t *)codes, plane, nrot, n_hit, plane_words, bits);
+    else if (code_bytes == 2)
+        pack_bits_k<uint16_t><<<blocks, threads, 0, s>>>((const uint16_t *)codes, plane, nrot, n_hit, plane_words,
+                                                          bits);
+    else
+        pack_bits_k<uint32_t><<<blocks, threads, 0, s>>>((const uint32_t *)codes, plane, nrot, n_hit, plane_words,
+                                                          bits);
+    return cudaGetLastError();
+}
+
+}  // namespace grc

@@ -29,6 +29,7 @@
 #include <stdint.h>
 
 #include "grc_internal.h"
+#include "grc_chain.cuh"
 
 // Resident CTAs per SM the scoring kernel is compiled for (register budget).
 #ifndef GRC_MIN_BLOCKS
@@ -40,232 +41,6 @@
 
 namespace grc {
 namespace {
-
-constexpr unsigned kFull = 0xffffffffu;
-
-// FP64 constants of one (voxel, omega) pair, forward_comp.m:17-26,42,51.
-struct OmegaRow {
-    double kx, ky, kz, L2;  // unit incident direction (lab), L2 of forward_comp.m:42
-    double ax, ay, az, num; // center - SamposW; t-numerator of forward_comp.m:51
-    double r2d, r3d, c, s;  // RotDet(:,2).d, RotDet(:,3).d with d = SamposW - D0; cos/sin omega
-};
-
-// The same row for the FP32 chain, kept in shared memory: the terms that do not depend on
-// the reflection are folded in (RotDet(1,:) * ax and the pixel scale), plus
-// k_w = Omega^T k_in for the prefilter.
-struct __align__(16) RowF {
-    float cN, ky, kz, L2;   // cN = R(1,1) ax
-    float cY, ay, az, num;  // cY = R(1,2) ax / pxy
-    float u0, v0, c, s;     // u0 = dety0 - r2d / pxy, v0 = detz0 - r3d / pxz
-    float wx, wy, wz, cZ;   // k_w; cZ = R(1,3) ax / pxz
-};
-static_assert(sizeof(RowF) == 64, "RowF layout");
-
-// Pixel-rounding ambiguity band of the FP32 landing chain.  Its error against the
-// FP64 chain stays below 1.4e-3 px on the 1024^2 / 2048^2 geometries (measured over
-// 3.4e5 landings); landings closer than this to a half-pixel boundary are recomputed
-// in FP64, so every decision equals the FP64 one.  A build with -DGRC_AUDIT re-decides
-// every FP32 decision in FP64: at 0.006 px it found no disagreement in 1.14e10 decisions
-// (FCC Al 2048^2 x 361 and BCC Fe 1024^2 x 181 scans), at 0.001 px two in 1.7e9.
-#ifndef GRC_AMBIG_PX
-#define GRC_AMBIG_PX 0.006f
-#endif
-constexpr float kAmbigPx = GRC_AMBIG_PX;
-
-__device__ __forceinline__ size_t align16(size_t x) { return (x + 15) & ~size_t(15); }
-
-__device__ __forceinline__ OmegaRow omega_row(const Geo &g, const double2 cs, const double *__restrict__ vp) {
-    const double px = vp[0], py = vp[1] - g.rao, pz = vp[2];
-    const double spx = g.S[0] * px + g.S[1] * py + g.S[2] * pz;
-    const double spy = g.S[3] * px + g.S[4] * py + g.S[5] * pz;
-    const double spz = g.S[6] * px + g.S[7] * py + g.S[8] * pz;
-    const double L = g.lss + g.lsd;
-    const double c = cs.x, s = cs.y;
-    const double swx = c * spx - s * spy, swy = s * spx + c * spy, swz = spz;
-    const double gx = g.lss + swx, gy = swy - g.p0y + g.rao, gz = swz - g.p0z;
-    const double ngp = sqrt(gx * gx + gy * gy + gz * gz);
-    OmegaRow r;
-    r.kx = gx / ngp;
-    r.ky = gy / ngp;
-    r.kz = gz / ngp;
-    r.L2 = (g.lsd - swx) * ngp / gx;  // (Lsd - SamposW_x) / cos(alpha)
-    r.ax = g.lsd - swx;
-    r.ay = gy * L / gx - swy;
-    r.az = gz * L / gx - swz;
-    const double dx = swx - g.lsd, dy = swy - g.dety00 + g.rao, dz = swz - g.detz00;
-    r.num = -(g.R[0] * dx + g.R[3] * dy + g.R[6] * dz);
-    r.r2d = g.R[1] * dx + g.R[4] * dy + g.R[7] * dz;
-    r.r3d = g.R[2] * dx + g.R[5] * dy + g.R[8] * dz;
-    r.c = c;
-    r.s = s;
-    return r;
-}
-
-// FP32 row from the FP64 one (the folded constants are formed in FP64 and rounded once).
-__device__ __forceinline__ RowF row_f32(const Geo &g, const OmegaRow &r) {
-    RowF f;
-    f.cN = (float)(g.R[0] * r.ax);
-    f.ky = (float)r.ky; f.kz = (float)r.kz; f.L2 = (float)r.L2;
-    f.cY = (float)(g.R[1] * r.ax / g.pxy);
-    f.ay = (float)r.ay; f.az = (float)r.az; f.num = (float)r.num;
-    f.u0 = (float)(g.dety0 - r.r2d / g.pxy);
-    f.v0 = (float)(g.detz0 - r.r3d / g.pxz);
-    f.c = (float)r.c; f.s = (float)r.s;
-    f.wx = (float)(r.c * r.kx + r.s * r.ky);
-    f.wy = (float)(-r.s * r.kx + r.c * r.ky);
-    f.wz = (float)r.kz;
-    f.cZ = (float)(g.R[2] * r.ax / g.pxz);
-    return f;
-}
-
-// Omega table of one voxel in shared memory (all threads of the CTA).
-__device__ void build_rows(const Geo &g, const double2 *__restrict__ rot_cs, const double *__restrict__ vp,
-                           RowF *rows) {
-    for (int iw = threadIdx.x; iw < g.nrot; iw += blockDim.x) rows[iw] = row_f32(g, omega_row(g, rot_cs[iw], vp));
-}
-
-// SUB = S*U*B (FP64, 9 values) of one trial.
-__device__ __forceinline__ void sub_matrix(const Geo &g, const double *__restrict__ U, double *SUB) {
-    double SU[9];
-#pragma unroll
-    for (int i = 0; i < 3; ++i)
-#pragma unroll
-        for (int j = 0; j < 3; ++j)
-            SU[3 * i + j] = g.S[3 * i] * U[j] + g.S[3 * i + 1] * U[3 + j] + g.S[3 * i + 2] * U[6 + j];
-#pragma unroll
-    for (int i = 0; i < 3; ++i)
-#pragma unroll
-        for (int j = 0; j < 3; ++j)
-            SUB[3 * i + j] = SU[3 * i] * g.B[j] + SU[3 * i + 1] * g.B[3 + j] + SU[3 * i + 2] * g.B[6 + j];
-}
-
-// Gw = S*U*B*h and |Gw| (forward_comp.m:15-16): FP32 table in shared memory plus the
-// FP64 SUB matrix kept for the exact recomputation of ambiguous reflections.
-__device__ __forceinline__ float4 window_of(const Geo &g, float G_f);
-
-__device__ void build_gw(const Geo &g, const double *__restrict__ hkl, const double *__restrict__ U, float4 *gw,
-                         float4 *win, double *sub) {
-    const int ih = threadIdx.x;
-    if (ih >= g.nhkl && ih >= 9) return;
-    double SUB[9];
-    sub_matrix(g, U, SUB);
-    if (ih < 9) sub[ih] = SUB[ih];  // threads 0..8 write SUB even when nhkl < 9
-    if (ih >= g.nhkl) return;
-    const double h = hkl[3 * ih], k = hkl[3 * ih + 1], l = hkl[3 * ih + 2];
-    const double x = SUB[0] * h + SUB[1] * k + SUB[2] * l;
-    const double y = SUB[3] * h + SUB[4] * k + SUB[5] * l;
-    const double z = SUB[6] * h + SUB[7] * k + SUB[8] * l;
-    const double Gd = sqrt(x * x + y * y + z * z);
-    gw[ih] = make_float4((float)x, (float)y, (float)z, (float)(1.0 / Gd));
-    win[ih] = window_of(g, (float)Gd);
-}
-
-// Exact FP64 evaluation of one reflection: the linear map index of its pixel, or -1
-// when select3 of forward_comp.m:61-65 rejects it.  Algebraic form of
-// forward_comp.m:28-59: sin(theta) = -cos(beta), cos(theta) = sin(beta), sin(phiy)
-// expanded, and the ray/plane intersection without normalising K_out.
-__device__ __forceinline__ int64_t landing_fp64(const Geo &g, const OmegaRow &r, double gxw, double gyw,
-                                                double gzw, int iw, double *lam_out = nullptr) {
-    const double G = sqrt(gxw * gxw + gyw * gyw + gzw * gzw);
-    const double Gtx = r.c * gxw - r.s * gyw, Gty = r.s * gxw + r.c * gyw, Gtz = gzw;
-    const double x = (r.kx * Gtx + r.ky * Gty + r.kz * Gtz) / G;  // cos(beta)
-    const double lam = 2.0 * (2.0 * CUDART_PI / G) * (-x);        // 2 d sin(theta)
-    if (lam_out) *lam_out = lam;
-    if (!(x < 0.0 && x > g.cbmax && lam > g.lmin && lam < g.lmax)) return -1;
-    const double st = -x, ct = sqrt(1.0 - x * x);
-    const double s2 = 2.0 * st * ct, c2 = 1.0 - 2.0 * st * st;
-    const double konst = sqrt(Gty * Gty + Gtz * Gtz);
-    const double gy = Gty / konst, gz = Gtz / konst;
-    const double cphx = gy * r.ky + gz * r.kz;
-    const double sphx = sqrt(fmax(0.0, 1.0 - cphx * cphx));
-    const double sphy = sphx * c2 - cphx * s2;
-    const double diff = r.L2 * s2 / sphy;
-    const double Kx = r.ax, Ky = r.ay + diff * gy, Kz = r.az + diff * gz;
-    const double nK = g.R[0] * Kx + g.R[3] * Ky + g.R[6] * Kz;
-    const double f = r.num / nK;
-    const double y2 = f * (g.R[1] * Kx + g.R[4] * Ky + g.R[7] * Kz) + r.r2d;
-    const double z2 = f * (g.R[2] * Kx + g.R[5] * Ky + g.R[8] * Kz) + r.r3d;
-    const double u = g.dety0 - y2 / g.pxy, v = g.detz0 - z2 / g.pxz;
-    // 1 <= round(u) <= detysize  <=>  0.5 <= u < detysize + 0.5 (round half away from zero)
-    if (!(u >= 0.5 && u < g.detysize + 0.5 && v >= 0.5 && v < g.detzsize + 0.5)) return -1;
-    const double ru = round(u), rv = round(v);
-    if (ru >= g.bsy0 && ru <= g.bsy1 && rv >= g.bsz0 && rv <= g.bsz1) return -1;
-    return (int64_t)iw * g.plane + (int64_t)(ru - 1.0) * g.detzsize + (int64_t)(rv - 1.0);
-}
-
-// The exact path for one ambiguous item: FP64 omega row and Gw rebuilt from the inputs.
-// Kept out of line (rarely taken) and reads the geometry from its global-memory copy.
-__device__ __noinline__ int64_t landing_exact(const Geo *__restrict__ gd, const double2 *__restrict__ rot_cs,
-                                              const double *__restrict__ vp, const double *__restrict__ hkl,
-                                              const double *sub, int iw, int ih) {
-    const Geo &g = *gd;
-    const OmegaRow r = omega_row(g, rot_cs[iw], vp);
-    const double h = hkl[3 * ih], k = hkl[3 * ih + 1], l = hkl[3 * ih + 2];
-    const double x = sub[0] * h + sub[1] * k + sub[2] * l;
-    const double y = sub[3] * h + sub[4] * k + sub[5] * l;
-    const double z = sub[6] * h + sub[7] * k + sub[8] * l;
-    return landing_fp64(g, r, x, y, z, iw);
-}
-
-// Window thresholds of one reflection on t = -(k_w . Gw) = |G|^2 lambda / (4 pi):
-// lambda in (lambda_min, lambda_max) and cos(beta) > cos(beta_max).  Returned as
-// (lo, hi) = the interval widened by the FP32 margin (prefilter) and (lo_in, hi_in)
-// = narrowed by it (inside, the FP32 decision is certain).
-__device__ __forceinline__ float4 window_of(const Geo &g, float G_f) {
-    const double G = G_f, G2 = G * G;
-    const double inv4pi = 0.25 / CUDART_PI;
-    double lo = g.lmin * G2 * inv4pi, hi = g.lmax * G2 * inv4pi;
-    if (g.cbmax > -1.0) hi = fmin(hi, -g.cbmax * G);
-    lo = fmax(lo, 0.0);
-    const double m = 1e-5 * G;  // >> FP32 error of k_w . G (~4e-7 |G|)
-    return make_float4((float)(lo - m), (float)(hi + m), (float)(lo + m), (float)(hi - m));
-}
-
-// FP32 landing chain (the algebra of landing_fp64 with the row's constant terms folded in).
-// Returns the in-plane map offset (dety-1)*detzsize + (detz-1), -1 for a certain rejection,
-// or -2 when the item lies within the ambiguity band of a decision boundary and must be
-// decided by landing_exact.
-__device__ __forceinline__ int landing_fp32(const Geo &g, const RowF &r, const float4 gw, float lo_in, float hi_in) {
-    // k_in . (Omega Gw) = (Omega^T k_in) . Gw: the prefilter's product, without rotating G
-    const float dot = r.wx * gw.x + r.wy * gw.y + r.wz * gw.z;
-    const float t = -dot;
-    if (!(t > lo_in && t < hi_in)) return -2;  // near the wavelength / Bragg-angle window edge
-    const float Gty = r.s * gw.x + r.c * gw.y, Gtz = gw.z;
-    // gw.w holds 1/|G|; reciprocal and square-root intrinsics (a few ulp) stay far inside
-    // the ambiguity band
-    const float x = dot * gw.w;
-    const float q = fmaxf(1.0f - x * x, 0.0f);
-    const float st = -x, ct = q * rsqrtf(q);
-    const float s2 = 2.0f * st * ct, c2 = 1.0f - 2.0f * st * st;
-    const float rk = rsqrtf(Gty * Gty + Gtz * Gtz);
-    const float gy = Gty * rk, gz = Gtz * rk;
-    const float cphx = gy * r.ky + gz * r.kz;
-    const float p = fmaxf(1.0f - cphx * cphx, 0.0f);
-    const float sphx = p * rsqrtf(p);
-    const float sphy = sphx * c2 - cphx * s2;
-    const float diff = __fdividef(r.L2 * s2, sphy);
-    const float Ky = r.ay + diff * gy, Kz = r.az + diff * gz;  // K_x = ax lives in cN, cY, cZ
-    const float nK = r.cN + g.Rf[3] * Ky + g.Rf[6] * Kz;
-    const float f = __fdividef(r.num, nK);
-    const float u = r.u0 - f * (r.cY + g.Ruf[0] * Ky + g.Ruf[1] * Kz);
-    const float v = r.v0 - f * (r.cZ + g.Rvf[0] * Ky + g.Rvf[1] * Kz);
-    if (!(fabsf(u) < 2e6f && fabsf(v) < 2e6f)) {  // detectors have at most 10^6 pixels per side
-        // far off the detector (or NaN): certain rejection only for finite values
-        return (isfinite(u) && isfinite(v)) ? -1 : -2;
-    }
-    // nearest integer by the 1.5*2^23 addition (|u|, |v| < 2^22 here): the sum's low mantissa
-    // bits hold the rounded value, read back as an integer without a conversion instruction.
-    // Within the ambiguity band of a half-pixel the item goes to the exact path, so the tie
-    // rule of the rounding never decides anything.
-    constexpr float kRound = 12582912.0f;
-    const float tu = __fadd_rn(u, kRound), tv = __fadd_rn(v, kRound);
-    const float ru = __fsub_rn(tu, kRound), rv = __fsub_rn(tv, kRound);
-    if (fabsf(u - ru) > 0.5f - kAmbigPx || fabsf(v - rv) > 0.5f - kAmbigPx) return -2;
-    const int iu = __float_as_int(tu) - 0x4B400000, iv = __float_as_int(tv) - 0x4B400000;
-    if (!(iu >= 1 && iu <= g.detysize && iv >= 1 && iv <= g.detzsize)) return -1;
-    if (ru >= g.bsy0f && ru <= g.bsy1f && rv >= g.bsz0f && rv <= g.bsz1f) return -1;
-    return (int)((uint32_t)(iu - 1) * (uint32_t)g.detzsize + (uint32_t)(iv - 1));  // < 2^31 pixels per plane
-}
 
 // Counts + histogram of codes below kHistBins (scoring pass).
 template <typename CodeT>
@@ -715,7 +490,8 @@ struct SweepSmem {
 // Shared-memory layout of one CTA holding `slots` trials and rows of `rows_cap` voxels:
 // kSweepParts arrays, offsets returned in offs[].
 constexpr int kSweepParts = 10;
-__host__ __device__ inline size_t sweep_smem_layout(int nhkl, int rows_cap, int slots, int nwin, size_t *offs) {
+__host__ __device__ inline size_t sweep_smem_layout(int nhkl, int rows_cap, int slots, int nwin, size_t *offs,
+                                                    int mode = kScanFull) {
     size_t o = 0, i = 0;
     auto put = [&](size_t bytes) {
         o = (o + 15) & ~size_t(15);
@@ -724,7 +500,7 @@ __host__ __device__ inline size_t sweep_smem_layout(int nhkl, int rows_cap, int 
     };
     put(sizeof(RowF) * rows_cap * nwin);
     put(sizeof(float4) * nhkl);
-    put(sizeof(uint32_t) * slots * kHist8Words);
+    put(sizeof(uint32_t) * slots * (mode == kScanFull ? kHist8Words : 1));
     put(sizeof(float) * slots * 12);
     put(sizeof(double) * slots * 9);
     put(sizeof(int) * slots);
@@ -735,9 +511,10 @@ __host__ __device__ inline size_t sweep_smem_layout(int nhkl, int rows_cap, int 
     return (o + 15) & ~size_t(15);
 }
 
-__device__ __forceinline__ SweepSmem sweep_carve(unsigned char *base, int nhkl, int rows_cap, int slots, int nwin) {
+__device__ __forceinline__ SweepSmem sweep_carve(unsigned char *base, int nhkl, int rows_cap, int slots, int nwin,
+                                                 int mode) {
     size_t offs[kSweepParts];
-    sweep_smem_layout(nhkl, rows_cap, slots, nwin, offs);
+    sweep_smem_layout(nhkl, rows_cap, slots, nwin, offs, mode);
     SweepSmem m;
     m.rows = (RowF *)(base + offs[0]);
     m.hk = (float4 *)(base + offs[1]);
@@ -752,26 +529,11 @@ __device__ __forceinline__ SweepSmem sweep_carve(unsigned char *base, int nhkl, 
     return m;
 }
 
-// Gw (FP32) of one reflection from the slot's S*U*B and h; .w = 1/|Gw|.
-__device__ __forceinline__ float4 gw_of(const float *sf, const float4 h) {
-    const float x = sf[0] * h.x + sf[1] * h.y + sf[2] * h.z;
-    const float y = sf[3] * h.x + sf[4] * h.y + sf[5] * h.z;
-    const float z = sf[6] * h.x + sf[7] * h.y + sf[8] * h.z;
-    return make_float4(x, y, z, rsqrtf(x * x + y * y + z * z));
-}
-
-// Window on t = -(k_w . Gw) in FP32 (see window_of) from rG = 1/|G|; the 1e-5 |G|
-// margins dominate its FP32 rounding.
-__device__ __forceinline__ float4 window_f(const Geo &g, const float4 gv) {
-    const float G2 = gv.x * gv.x + gv.y * gv.y + gv.z * gv.z, G = G2 * gv.w;
-    float lo = g.lo4pif * G2, hi = g.hi4pif * G2;
-    if (g.cbmaxf > -1.0f) hi = fminf(hi, -g.cbmaxf * G);
-    lo = fmaxf(lo, 0.0f);
-    const float m = 1e-5f * G;
-    return make_float4(lo - m, hi + m, lo + m, hi - m);
-}
-
-template <int HPL, int WIN>
+// MODE kScanFull: per slot a 256-bin histogram of the 8-bit codes (counts and exact median);
+// kScanComp: per slot one packed counter (Nr_simu in the low 16 bits, Nr_intersect in the high
+// 16; both stay below 2^16 because the sweep takes at most 65,535 reflections per trial), the hit
+// read from the bit-packed mask, no median.
+template <int HPL, int WIN, int MODE>
 __global__ void __launch_bounds__(kThreads, GRC_SWEEP_BLOCKS) sweep_kernel(Geo g, ScoreBufs b, Work w, int64_t round_base,
                                                             int64_t n_trials, int rows_cap, int slots) {
     constexpr int nwin = WIN;  // projections per window
@@ -779,7 +541,7 @@ __global__ void __launch_bounds__(kThreads, GRC_SWEEP_BLOCKS) sweep_kernel(Geo g
     if (cta_base >= n_trials) return;
     const int nslot = (int)min((int64_t)slots, n_trials - cta_base);
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    const SweepSmem sm = sweep_carve(smem_raw, g.nhkl, rows_cap, slots, nwin);
+    const SweepSmem sm = sweep_carve(smem_raw, g.nhkl, rows_cap, slots, nwin, MODE);
     __shared__ int s_nv, s_next;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const unsigned lt = (1u << lane) - 1u;
@@ -800,7 +562,7 @@ __global__ void __launch_bounds__(kThreads, GRC_SWEEP_BLOCKS) sweep_kernel(Geo g
         }
         sm.vglob[tid] = v;
     }
-    for (int i = tid; i < slots * kHist8Words; i += kThreads) sm.hist[i] = 0;
+    for (int i = tid; i < slots * (MODE == kScanFull ? kHist8Words : 1); i += kThreads) sm.hist[i] = 0;
     for (int i = tid; i < g.nhkl; i += kThreads)
         sm.hk[i] = make_float4((float)b.hkl[3 * i], (float)b.hkl[3 * i + 1], (float)b.hkl[3 * i + 2], 0.f);
     __syncthreads();
@@ -814,18 +576,23 @@ __global__ void __launch_bounds__(kThreads, GRC_SWEEP_BLOCKS) sweep_kernel(Geo g
     }
     __syncthreads();
     const int nv = s_nv;
+    const int64_t pw = b.plane_words;
 
     // Selected pixels reach the histogram one batch late: the code of batch k is loaded
     // when batch k is evaluated and applied after batch k+1 has been computed, so the
     // L2 latency of the gather overlaps the next landing computations.  The histogram is
     // the only per-selection update: Nr_simu is its total and Nr_intersect the total of its
     // codes below n_hit (< 255, so the saturated bin never holds a hit).
-    int pend_off = -1;   // this lane's pending offset in the projection window (or -1)
+    int pend_off = -1;   // full: the pending offset in the projection window; completeness: its bit (or -1)
     int pend_slot = 0;
-    uint32_t pend_code = 0;
+    uint32_t pend_code = 0;  // full: the 8-bit code; completeness: the mask word
     auto apply_pending = [&]() {
-        if (pend_off >= 0)
-            atomicAdd(&sm.hist[pend_slot * kHist8Words + (pend_code >> 1)], 1u << ((pend_code & 1u) * 16));
+        if (pend_off >= 0) {
+            if (MODE == kScanFull)
+                atomicAdd(&sm.hist[pend_slot * kHist8Words + (pend_code >> 1)], 1u << ((pend_code & 1u) * 16));
+            else
+                atomicAdd(&sm.hist[pend_slot], 1u + (((pend_code >> pend_off) & 1u) << 16));
+        }
         pend_off = -1;
     };
 
@@ -833,10 +600,21 @@ __global__ void __launch_bounds__(kThreads, GRC_SWEEP_BLOCKS) sweep_kernel(Geo g
         const int nw = min(nwin, g.nrot - w0);
         // codes of the window's first pixel; offsets within the window fit 32 bits
         // (nwin * plane < 2^31, launch_sweep_t)
-        const uint8_t *wcodes = b.codes8 + (int64_t)w0 * g.plane;
-        auto sink = [&](int off, int s) {  // warp-synchronous: every lane calls it once per batch
+        const uint8_t *wcodes = MODE == kScanFull ? b.codes8 + (int64_t)w0 * g.plane : nullptr;
+        const uint32_t *wbits = MODE == kScanComp ? b.bits + (int64_t)w0 * pw : nullptr;
+        // warp-synchronous: every lane calls it once per batch; ip = in-plane pixel or -1
+        auto sink = [&](int wl, int ip, int s) {
             uint32_t code = 0;
-            if (off >= 0) code = __ldg(wcodes + off);
+            int off = -1;
+            if (ip >= 0) {
+                if (MODE == kScanFull) {
+                    off = wl * (int)g.plane + ip;
+                    code = __ldg(wcodes + off);
+                } else {
+                    off = ip & 31;
+                    code = __ldg(wbits + (int64_t)wl * pw + (ip >> 5));
+                }
+            }
             apply_pending();
             pend_off = off;
             pend_slot = s;
@@ -851,14 +629,14 @@ __global__ void __launch_bounds__(kThreads, GRC_SWEEP_BLOCKS) sweep_kernel(Geo g
         __syncthreads();
         int qn = 0, fn = 0;
         auto fast = [&](uint32_t item, bool valid) {
-            int r = -1;
+            int ip = -1;
             const int s = (int)(item >> 16), wl = (int)((item >> 8) & 255u), ih = (int)(item & 255u);
             if (valid) {
                 const float4 gv = gw_of(sm.subf + 12 * s, sm.hk[ih]);
                 const float4 win = window_f(g, gv);
-                const int ip = landing_fp32(g, sm.rows[sm.vloc[s] * nwin + wl], gv, win.z, win.w);
-                r = ip >= 0 ? wl * (int)g.plane + ip : ip;
+                ip = landing_fp32(g, sm.rows[sm.vloc[s] * nwin + wl], gv, win.z, win.w);
 #ifdef GRC_AUDIT
+                const int r = ip >= 0 ? wl * (int)g.plane + ip : ip;
                 // audit build: every certain FP32 decision is re-decided by the FP64 path
                 if (r != -2) {
                     const int64_t r64 = landing_exact(b.geo, b.rot_cs, b.vpos + 3 * sm.vglob[s], b.hkl,
@@ -868,21 +646,21 @@ __global__ void __launch_bounds__(kThreads, GRC_SWEEP_BLOCKS) sweep_kernel(Geo g
                 }
 #endif
             }
-            const bool amb = r == -2;
+            const bool amb = ip == -2;
             const unsigned m = __ballot_sync(kFull, amb);
             if (amb) fq[fn + __popc(m & lt)] = item;
             fn += __popc(m);
-            sink(r >= 0 ? r : -1, s);
+            sink(wl, ip >= 0 ? ip : -1, s);
         };
         auto exact = [&](uint32_t item, bool valid) {
             const int s = (int)(item >> 16), wl = (int)((item >> 8) & 255u), ih = (int)(item & 255u);
-            int r = -1;
+            int ip = -1;
             if (valid) {
                 const int64_t r64 =
                     landing_exact(b.geo, b.rot_cs, b.vpos + 3 * sm.vglob[s], b.hkl, sm.subd + 9 * s, w0 + wl, ih);
-                r = r64 >= 0 ? (int)(r64 - (int64_t)w0 * g.plane) : -1;
+                ip = r64 >= 0 ? (int)(r64 - (int64_t)(w0 + wl) * g.plane) : -1;
             }
-            sink(r, s);
+            sink(wl, ip, s);
         };
         auto drain = [&](bool all) {
             while (qn >= 32 || (all && qn > 0)) {
@@ -959,65 +737,25 @@ __global__ void __launch_bounds__(kThreads, GRC_SWEEP_BLOCKS) sweep_kernel(Geo g
         __syncthreads();  // rows are rebuilt for the next window
     }
 
-    // ---- finalize: one warp per slot, exact median from the 8-bit histogram
-    for (int s = warp; s < nslot; s += kWarps) {
-        const uint32_t *h = sm.hist + s * kHist8Words;
-        // lane owns bins [8*lane, 8*lane+8)
-        uint32_t bins[8];
-        uint32_t local = 0, hits = 0;
-#pragma unroll
-        for (int i = 0; i < 4; ++i) {
-            const uint32_t wv = h[4 * lane + i];
-            bins[2 * i] = wv & 0xffffu;
-            bins[2 * i + 1] = wv >> 16;
-        }
-        const uint32_t sat = __shfl_sync(kFull, bins[7], 31);  // bin 255: saturated codes (>= 255)
-        if (lane == 31) bins[7] = 0;  // not part of the exact range
-#pragma unroll
-        for (int i = 0; i < 8; ++i) {
-            local += bins[i];
-            if ((uint32_t)(8 * lane + i) < g.n_hit) hits += bins[i];
-        }
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) hits += __shfl_xor_sync(kFull, hits, o);
-        uint32_t incl = local;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const uint32_t y = __shfl_up_sync(kFull, incl, o);
-            if (lane >= o) incl += y;
-        }
-        const uint32_t inr = __shfl_sync(kFull, incl, 31);
-        const int n = (int)(inr + sat), inter = (int)hits;  // Nr_simu, Nr_intersect
-        const uint32_t excl = incl - local;
-        const uint32_t ra = (uint32_t)(n + 1) / 2, rb = (uint32_t)n / 2 + 1;
-        int ca = -1, cb = -1;
-        if (n > 0 && rb <= inr) {
-            uint32_t cum = excl;
-#pragma unroll
-            for (int i = 0; i < 8; ++i) {
-                if (ca < 0 && cum < ra && ra <= cum + bins[i]) ca = 8 * lane + i;
-                if (cb < 0 && cum < rb && rb <= cum + bins[i]) cb = 8 * lane + i;
-                cum += bins[i];
+    // ---- finalize: one warp per slot, exact median from the 8-bit histogram; or the counters
+    if constexpr (MODE == kScanFull) {
+        for (int s = warp; s < nslot; s += kWarps) hist8_finish(g, b, sm.hist + s * kHist8Words, cta_base + s);
+    } else {
+        for (int base = warp * 32; base < nslot; base += kWarps * 32) {
+            const int s = base + lane;
+            const bool in = s < nslot;
+            int simu = 0, inter = 0;
+            if (in) {
+                const uint32_t c = sm.hist[s];
+                simu = (int)(c & 0xffffu);
+                inter = (int)(c >> 16);
+                TrialRes r;
+                r.simu = simu;
+                r.inter = inter;
+                r.median = CUDART_NAN;  // not computed in this mode
+                b.res[cta_base + s] = r;
             }
-        }
-        const unsigned ma = __ballot_sync(kFull, ca >= 0), mb = __ballot_sync(kFull, cb >= 0);
-        ca = ma ? __shfl_sync(kFull, ca, __ffs(ma) - 1) : -1;
-        cb = mb ? __shfl_sync(kFull, cb, __ffs(mb) - 1) : -1;
-        if (lane == 0) {
-            const int64_t t = cta_base + s;
-            TrialRes r;
-            r.simu = n;
-            r.inter = inter;
-            if (n == 0) {
-                r.median = 2000.0;  // forward_comp.m:89
-            } else if (ca >= 0 && cb >= 0) {
-                r.median = ((double)b.vals[ca] + (double)b.vals[cb]) / 2.0;
-            } else {
-                r.median = CUDART_NAN;
-                const int k = atomicAdd(b.work_counter + 4, 1);
-                b.refine_list[k] = t;
-            }
-            b.res[t] = r;
+            if (b.group_key) fold_group_key(b, in, cta_base + s, simu, inter);
         }
     }
 }
@@ -1124,7 +862,7 @@ cudaError_t launch_score_t(const Geo &g, const ScoreBufs &b, const Work &w, int 
 }
 
 
-template <int HPL, typename CodeT>
+template <int HPL, typename CodeT, int MODE>
 cudaError_t launch_sweep_t(const Geo &g, const ScoreBufs &b, const Work &w, int64_t n_trials, int num_sms,
                            cudaStream_t s, cudaEvent_t ev0, cudaEvent_t ev1, int *launches, int max_slots) {
     // The tile is kSlotsBulk trials per CTA.  An implicit seeding list (a few voxels per CTA) may
@@ -1145,11 +883,11 @@ cudaError_t launch_sweep_t(const Geo &g, const ScoreBufs &b, const Work &w, int6
         return rc > sl ? sl : rc;
     };
     size_t offs[kSweepParts];
-    const size_t smem_max = sweep_smem_layout(g.nhkl, rows_for(max_slots), max_slots, kWinMin, offs);
+    const size_t smem_max = sweep_smem_layout(g.nhkl, rows_for(max_slots), max_slots, kWinMin, offs, MODE);
     const size_t smem_r = refine_smem_bytes(g.nrot, g.nhkl);
     int per_sm = 0;
     using SweepFn = void (*)(Geo, ScoreBufs, Work, int64_t, int64_t, int, int);
-    const SweepFn k8 = sweep_kernel<HPL, kWinMin>;
+    const SweepFn k8 = sweep_kernel<HPL, kWinMin, MODE>;
     cudaError_t e = cudaFuncSetAttribute(k8, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_max);
     if (e != cudaSuccess) return e;
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k8, kThreads, smem_max);
@@ -1162,7 +900,7 @@ cudaError_t launch_sweep_t(const Geo &g, const ScoreBufs &b, const Work &w, int6
     if (!caller_tile && !explicit_voxels && n_trials > grid * max_slots && n_trials <= grid * kSlots) {
         // one round of up to kSlots trials per CTA, if the larger tile keeps the same CTAs per SM
         int per_sm1 = 0;
-        const size_t smem1 = sweep_smem_layout(g.nhkl, rows_for(kSlots), kSlots, kWinMin, offs);
+        const size_t smem1 = sweep_smem_layout(g.nhkl, rows_for(kSlots), kSlots, kWinMin, offs, MODE);
         if (cudaFuncSetAttribute(k8, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem1) == cudaSuccess &&
             cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm1, k8, kThreads, smem1) == cudaSuccess &&
             per_sm1 == per_sm) {
@@ -1177,12 +915,12 @@ cudaError_t launch_sweep_t(const Geo &g, const ScoreBufs &b, const Work &w, int6
     // the widest projection window whose rows keep the grid's CTAs per SM (and 32-bit map
     // offsets within a window)
     SweepFn kern = k8;
-    size_t smem = sweep_smem_layout(g.nhkl, rows_cap, slots, kWinMin, offs);
+    size_t smem = sweep_smem_layout(g.nhkl, rows_cap, slots, kWinMin, offs, MODE);
     bool refused = false;
     for (int cand : kWinWide) {
         if ((int64_t)cand * g.plane > 2147483647LL) continue;
-        const SweepFn kc = cand == 32 ? (SweepFn)sweep_kernel<HPL, 32> : (SweepFn)sweep_kernel<HPL, 16>;
-        const size_t smem_c = sweep_smem_layout(g.nhkl, rows_cap, slots, cand, offs);
+        const SweepFn kc = cand == 32 ? (SweepFn)sweep_kernel<HPL, 32, MODE> : (SweepFn)sweep_kernel<HPL, 16, MODE>;
+        const size_t smem_c = sweep_smem_layout(g.nhkl, rows_cap, slots, cand, offs, MODE);
         int per_c = 0;
         if (cudaFuncSetAttribute(kc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_c) != cudaSuccess ||
             cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_c, kc, kThreads, smem_c) != cudaSuccess) {
@@ -1209,8 +947,10 @@ cudaError_t launch_sweep_t(const Geo &g, const ScoreBufs &b, const Work &w, int6
         ++*launches;
     }
     if (ev1) cudaEventRecord(ev1, s);
-    refine_list_kernel<HPL, CodeT><<<grid_r, kThreads, smem_r, s>>>(g, b, w);
-    ++*launches;
+    if (MODE == kScanFull) {  // completeness mode has no median to refine
+        refine_list_kernel<HPL, CodeT><<<grid_r, kThreads, smem_r, s>>>(g, b, w);
+        ++*launches;
+    }
     return cudaGetLastError();
 }
 
@@ -1349,13 +1089,47 @@ int64_t sweep_round_trials(const Geo &g, int num_sms) {
 }
 
 cudaError_t launch_sweep(const Geo &g, const ScoreBufs &b, const Work &w, int64_t n_trials, int num_sms,
-                         cudaStream_t s, cudaEvent_t ev0, cudaEvent_t ev1, int *launches, int max_slots) {
+                         cudaStream_t s, cudaEvent_t ev0, cudaEvent_t ev1, int *launches, int max_slots, int mode) {
+    const int hpl = (g.nhkl + 31) / 32;
+    const bool c16 = g.code_bits <= 16;
+    if (mode == kScanComp && !b.bits) return cudaErrorInvalidValue;
+#define GRC_DISPATCH(H)                                                                                          \
+    if (hpl == H) {                                                                                              \
+        if (mode == kScanComp)                                                                                   \
+            return launch_sweep_t<H, uint16_t, kScanComp>(g, b, w, n_trials, num_sms, s, ev0, ev1, launches,      \
+                                                          max_slots);                                            \
+        return c16 ? launch_sweep_t<H, uint16_t, kScanFull>(g, b, w, n_trials, num_sms, s, ev0, ev1, launches,    \
+                                                            max_slots)                                           \
+                   : launch_sweep_t<H, uint32_t, kScanFull>(g, b, w, n_trials, num_sms, s, ev0, ev1, launches,    \
+                                                            max_slots);                                          \
+    }
+    GRC_DISPATCH(1)
+    GRC_DISPATCH(2)
+    GRC_DISPATCH(3)
+    GRC_DISPATCH(4)
+#undef GRC_DISPATCH
+    return cudaErrorInvalidValue;
+}
+
+namespace {
+template <int HPL, typename CodeT>
+cudaError_t launch_refine_list_t(const Geo &g, const ScoreBufs &b, const Work &w, int num_sms, cudaStream_t s) {
+    const size_t smem_r = refine_smem_bytes(g.nrot, g.nhkl);
+    int grid_r = 0;
+    cudaError_t e = prep_launch(refine_list_kernel<HPL, CodeT>, smem_r, num_sms, (int64_t)num_sms * 4, &grid_r);
+    if (e != cudaSuccess) return e;
+    refine_list_kernel<HPL, CodeT><<<grid_r, kThreads, smem_r, s>>>(g, b, w);
+    return cudaGetLastError();
+}
+}  // namespace
+
+cudaError_t launch_refine_list(const Geo &g, const ScoreBufs &b, const Work &w, int num_sms, cudaStream_t s) {
     const int hpl = (g.nhkl + 31) / 32;
     const bool c16 = g.code_bits <= 16;
 #define GRC_DISPATCH(H)                                                                                     \
     if (hpl == H)                                                                                           \
-        return c16 ? launch_sweep_t<H, uint16_t>(g, b, w, n_trials, num_sms, s, ev0, ev1, launches, max_slots) \
-                   : launch_sweep_t<H, uint32_t>(g, b, w, n_trials, num_sms, s, ev0, ev1, launches, max_slots);
+        return c16 ? launch_refine_list_t<H, uint16_t>(g, b, w, num_sms, s)                                 \
+                   : launch_refine_list_t<H, uint32_t>(g, b, w, num_sms, s);
     GRC_DISPATCH(1)
     GRC_DISPATCH(2)
     GRC_DISPATCH(3)

@@ -16,15 +16,19 @@ after the other:
    (GrainMapping_engine_gpu_comp.m:180-181), then region growth.
 
 Steps 1-5 depend only on the seed position and the static distance map, so here they run
-for a whole batch of seeds at once: one scan launch, one local-refine launch over
-``n_seeds x Nr_seed x 730`` trials, one batched Nelder-Mead (every simplex on the device,
-one scorer launch per step for all seeds), one final launch.  Step 6 changes the sample
-maps and stays sequential: ``GrainMapping_engine_gpu_comp`` commits the batch's results
-in seed order, discarding a result whose seed an earlier growth made redundant, and
-re-indexes a moved centre (the replace_center loop, :256-300) on the spot.
+for a whole batch of seeds at once: one call for the scan and the top-N selection
+(grc_seed_candidates_device), one for the local refine of every candidate with its grid
+maxima and their order (grc_seed_refine_device, n_seeds x Nr_seed x 730 trials), one
+batched Nelder-Mead (every simplex on the device, one scorer launch per step for all
+seeds), one final scoring.  Step 6 changes the sample maps and stays sequential:
+``GrainMapping_engine_gpu_comp`` commits the batch's results in seed order, discarding a
+result whose seed an earlier growth made redundant, and re-indexes a moved centre (the
+replace_center loop, :256-300) on the spot.
 
-Every scorer evaluation goes through libgrainrecon_b200.so; torch only holds device
-buffers and does the small sorts between launches.
+Scans, sorts, grids and maxima all run in libgrainrecon_b200.so; torch only holds the
+device buffers.  The scan and the refine read column 3 only (GrainMapping_engine_gpu_comp.m:103,
+fit_OR_constrain_with_local_comp_cuda.m:105), so they run completeness-only on the
+bit-packed hit mask; the final scoring computes the median the accept rule reads.
 """
 from __future__ import annotations
 
@@ -111,45 +115,6 @@ def fitted_orientation(x):
     return np.array(ang), rod, rod2quat(rod)
 
 
-# ---- device helpers -------------------------------------------------------------------------------
-
-def sort_desc_nan_first(C, dim: int = -1):
-    """Indices of ``sortrows(.., 'descend')`` on one column: stable, NaN rows first."""
-    import torch
-    return torch.sort(C, dim=dim, descending=True, stable=True).indices
-
-
-def local_grids(qc, nr: int = NR_LOCAL, gridsize: float = GRID_LOCAL):
-    """``ori_local_sampling(q, nr, gridsize)`` for every row of qc (n x 4, float64, device).
-
-    Returns (n, (nr+1)^3 + 1, 4): the centre row and the (b, c, d) grid with
-    q0 = sqrt(1 - (b^2 + c^2 + d^2)), in ``unique(q, 'rows')`` order (ascending by q0, then
-    b, c, d).  A grid point equal to the centre stays in as an adjacent twin; it scores the
-    same, so a first-maximum search picks the same orientation as on the de-duplicated list."""
-    import torch
-    n = qc.shape[0]
-    steps = torch.arange(nr + 1, dtype=torch.float64, device=qc.device) * gridsize - gridsize * nr / 2
-    b = qc[:, 1, None] + steps[None, :]
-    c = qc[:, 2, None] + steps[None, :]
-    d = qc[:, 3, None] + steps[None, :]
-    m = nr + 1
-    B = b[:, :, None, None].expand(n, m, m, m).reshape(n, -1)
-    Cc = c[:, None, :, None].expand(n, m, m, m).reshape(n, -1)
-    D = d[:, None, None, :].expand(n, m, m, m).reshape(n, -1)
-    q0 = torch.sqrt(1 - (B * B + Cc * Cc + D * D))
-    grid = torch.stack([q0, B, Cc, D], dim=-1)
-    rows = torch.cat([qc[:, None, :], grid], dim=1)
-    # lexicographic order by stable sorts from the last key to the first
-    for k in (3, 2, 1, 0):
-        o = torch.sort(rows[:, :, k], dim=1, stable=True).indices
-        rows = torch.gather(rows, 1, o[:, :, None].expand_as(rows))
-    return rows
-
-
-def _f32(t):
-    return t.float().double()
-
-
 class SeedIndexer:
     """Steps 1-5 of the seeding stage for batches of seeds on one context.
 
@@ -165,57 +130,43 @@ class SeedIndexer:
         self.fit = fit
         self.stats = {"scan_trials": 0, "local_trials": 0, "fit_seeds": 0, "fit_evals": 0, "final_trials": 0}
 
-    # 1. scan of the whole grid (ForwardCalc_OR_space_comp_cuda: float32 pos and q)
-    def scan(self, pos):
+    # 1-2. scan of the whole grid (ForwardCalc_OR_space_comp_cuda: float32 pos and q) and the top
+    # Nr_seed rows by completeness
+    def candidates(self, pos):
+        """Scan of every seed (n x 3 mm) against the grid and the first ``nr_seed`` rows of
+        sortrows(Output, 3, 'descend') per seed: (n, k, 4) float64 orientations of the grid."""
         import torch
         p = torch.as_tensor(np.ascontiguousarray(pos, np.float32), device=self.dev).reshape(-1, 3).contiguous()
         n, N = p.shape[0], self.q.shape[0]
-        out = torch.empty(n * N * 4, dtype=torch.float32, device=self.dev)
-        self.ctx.forward_comp_device(p, n, self.q32, N, out)
+        k = min(self.nr_seed, N)
+        idx = torch.empty(n * k, dtype=torch.int32, device=self.dev)
+        cand = torch.empty(n * k * 4, dtype=torch.float64, device=self.dev)
+        self.ctx.seed_candidates_device(p, n, self.q32, N, k, idx, cand, None, self.q)
         self.stats["scan_trials"] += n * N
-        return out.view(n, N, 4)
+        return cand.view(n, k, 4)
 
-    # 2. top Nr_seed rows by completeness
-    def top(self, out, q_rows):
-        """q_rows: (n, N, 4) or (N, 4) orientations of the scored rows; returns (n, k, 4) float64."""
-        import torch
-        k = min(self.nr_seed, out.shape[1])
-        idx = sort_desc_nan_first(out[:, :, 2].double(), dim=1)[:, :k]
-        if q_rows.dim() == 2:
-            return q_rows[idx]
-        return torch.gather(q_rows, 1, idx[:, :, None].expand(-1, -1, 4))
-
-    def score_pairs(self, pos64, q64, tv, to):
-        import torch
-        out = torch.empty(tv.numel() * 4, dtype=torch.float32, device=self.dev)
-        self.ctx.score_trials_device(pos64, pos64.shape[0], q64, q64.shape[0], tv, to, tv.numel(), out)
-        return out.view(-1, 4)
-
-    # 3. local refine of every candidate; best row of each grid
-    def local_best(self, pos, cand, nr: int = NR_LOCAL, gridsize: float = GRID_LOCAL):
-        """cand: (n, k, 4) float64.  Returns (best_q (n, k, 4), best_C (n, k) float64 with NaN)."""
+    # 3. local refine of every candidate: each grid's first maximum, candidates in sortrows order
+    def refine(self, pos, cand, n_x0: int, nr: int = NR_LOCAL, gridsize: float = GRID_LOCAL):
+        """cand: (n, k, 4) float64.  Returns, per seed in sortrows(Output_max, 3, 'descend') order:
+        best_q (n, k, 4) float64, best_c (n, k) float32 (NaN for 0/0), order (n, k) int32 (the
+        candidate each row came from) and x0 (n, n_x0, 3), the fit's start points."""
         import torch
         n, k = cand.shape[0], cand.shape[1]
-        pos32 = _f32(torch.as_tensor(np.ascontiguousarray(pos, np.float64), device=self.dev).reshape(-1, 3))
+        pos32 = np.ascontiguousarray(pos, np.float64).reshape(-1, 3).astype(np.float32).astype(np.float64)
+        d_pos = torch.as_tensor(pos32, device=self.dev).contiguous()
         L = (nr + 1) ** 3 + 1
         best_q = torch.empty(n, k, 4, dtype=torch.float64, device=self.dev)
-        best_c = torch.empty(n, k, dtype=torch.float64, device=self.dev)
+        best_c = torch.empty(n, k, dtype=torch.float32, device=self.dev)
+        order = torch.empty(n, k, dtype=torch.int32, device=self.dev)
+        x0 = torch.empty(n, n_x0, 3, dtype=torch.float64, device=self.dev)
         per = max(1, TRIALS_PER_LAUNCH // max(1, k * L))
+        cand = cand.contiguous()
         for s0 in range(0, n, per):
             s1 = min(n, s0 + per)
-            m = s1 - s0
-            grids = local_grids(cand[s0:s1].reshape(-1, 4), nr, gridsize)          # (m*k, L, 4)
-            q32 = _f32(grids.reshape(-1, 4)).contiguous()                           # MEX q is single
-            tv = torch.arange(m, dtype=torch.int32, device=self.dev).repeat_interleave(k * L)
-            to = torch.arange(m * k * L, dtype=torch.int32, device=self.dev)
-            res = self.score_pairs(pos32[s0:s1].contiguous(), q32, tv, to).view(m, k, L, 4)
-            C = res[..., 2].double()
-            Cm = torch.where(torch.isnan(C), torch.full_like(C, -math.inf), C)
-            j = torch.argmax(Cm, dim=2)                                             # first maximum
-            best_q[s0:s1] = torch.gather(grids.view(m, k, L, 4), 2, j[:, :, None, None].expand(-1, -1, 1, 4))[:, :, 0]
-            best_c[s0:s1] = torch.gather(C, 2, j[:, :, None])[:, :, 0]
-            self.stats["local_trials"] += m * k * L
-        return best_q, best_c
+            self.ctx.seed_refine_device(d_pos[s0:s1], s1 - s0, cand[s0:s1], k, nr, gridsize, best_q[s0:s1],
+                                        best_c[s0:s1], order[s0:s1], n_x0, x0[s0:s1])
+            self.stats["local_trials"] += (s1 - s0) * k * L
+        return best_q, best_c, order, x0
 
     # 4. batched fminsearchbnd on 1 - C
     def fit_nm(self, pos, x0):
@@ -231,7 +182,7 @@ class SeedIndexer:
         self.ctx.fit_orientation_nm(p, x0, n, x, fval, ev, it, fl, FIT_HALF_WIDTH, FIT_MAX_EVALS, FIT_MAX_EVALS,
                                     FIT_TOL_F, FIT_TOL_X)
         self.stats["fit_seeds"] += n
-        self.stats["fit_evals"] += int(ev.sum().item())
+        self.stats["fit_evals"] += int(ev.cpu().numpy().sum())
         return x, fval, ev, it, fl
 
     # 5. Euler round trip and final scoring (FP64 U, FP64 pos)
@@ -250,17 +201,13 @@ class SeedIndexer:
     def fit_candidates(self, seed_ids, pos, cand, fit_all: bool = False):
         """fit_OR_constrain_with_local_comp_cuda for a batch: cand (n, k, 4) -> rows (n, 18) and the
         1-based candidate index that gave each row (confident_index_list)."""
-        import torch
         pos = np.asarray(pos, np.float64).reshape(-1, 3)
         n, k = cand.shape[0], cand.shape[1]
-        best_q, best_c = self.local_best(pos, cand)
-        order = sort_desc_nan_first(best_c, dim=1)                                  # sortrows(Output_max, 3, 'descend')
         nfit = k if fit_all else 1
-        sel = order[:, :nfit]
-        x0 = torch.gather(best_q, 1, sel[:, :, None].expand(-1, -1, 4))[:, :, 1:].contiguous()
+        _, _, order, x0 = self.refine(pos, cand, nfit)
         pos_rep = np.repeat(pos, nfit, axis=0)
         if self.fit:
-            x, _, _, _, _ = self.fit_nm(pos_rep, x0)
+            x, _, _, _, _ = self.fit_nm(pos_rep, x0.reshape(-1, 3))
         else:
             x = x0.reshape(-1, 3)
         out, eul, rod, quat = self.final(pos_rep, x)
@@ -273,28 +220,29 @@ class SeedIndexer:
         rows = rows.reshape(n, nfit, 18)
         Cs = np.where(np.isnan(rows[:, :, 6]), -np.inf, rows[:, :, 6])
         pick = np.argmax(Cs, axis=1)                                                 # max(indexing_result(:,7))
-        cand_id = sel.cpu().numpy()[np.arange(n), pick] + 1
+        cand_id = order[:, :nfit].cpu().numpy()[np.arange(n), pick] + 1
         return rows[np.arange(n), pick], cand_id
 
     def index(self, seed_ids, pos, fit_all: bool = False):
         """Steps 1-5 for seeds at ``pos`` (n x 3 mm) against the full grid."""
-        out = self.scan(pos)
-        cand = self.top(out, self.q)
-        return self.fit_candidates(seed_ids, pos, cand, fit_all)
+        return self.fit_candidates(seed_ids, pos, self.candidates(pos), fit_all)
 
     def index_local(self, seed_id, pos, q_center, nr: int = NR_RECENTRE, gridsize: float = GRID_LOCAL):
         """Re-indexing at a moved centre: ori_local_sampling(q, 4) scanned, then steps 2-5."""
         import torch
-        qc = torch.as_tensor(np.asarray(q_center, np.float64).reshape(1, 4), device=self.dev)
-        grid = local_grids(qc, nr, gridsize)[0]                                     # (126, 4)
+        qc = torch.as_tensor(np.asarray(q_center, np.float64).reshape(4), device=self.dev)
+        L = (nr + 1) ** 3 + 1
+        grid = torch.empty(L * 4, dtype=torch.float64, device=self.dev)
+        grid32 = torch.empty(L * 4, dtype=torch.float32, device=self.dev)
+        self.ctx.local_grid_device(qc, 1, nr, gridsize, grid, grid32)
         p = np.asarray(pos, np.float64).reshape(1, 3)
-        p32 = _f32(torch.as_tensor(p, device=self.dev))
-        tv = torch.zeros(grid.shape[0], dtype=torch.int32, device=self.dev)
-        to = torch.arange(grid.shape[0], dtype=torch.int32, device=self.dev)
-        out = self.score_pairs(p32.contiguous(), _f32(grid).contiguous(), tv, to).view(1, -1, 4)
-        self.stats["scan_trials"] += grid.shape[0]
-        cand = self.top(out, grid[None])
-        return self.fit_candidates([seed_id], p, cand)
+        d_p = torch.as_tensor(p.astype(np.float32), device=self.dev).reshape(-1)
+        k = min(self.nr_seed, L)
+        idx = torch.empty(k, dtype=torch.int32, device=self.dev)
+        cand = torch.empty(k * 4, dtype=torch.float64, device=self.dev)
+        self.ctx.seed_candidates_device(d_p, 1, grid32, L, k, idx, cand, None, grid)
+        self.stats["scan_trials"] += L
+        return self.fit_candidates([seed_id], p, cand.view(1, k, 4))
 
 
 # ---- measured spots: pairing and the grain-centre fit ------------------------------------------------

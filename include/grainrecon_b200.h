@@ -66,6 +66,26 @@ int grc_upload_masks_device(grc_ctx *ctx, const float *d_proj_bin_bw, int64_t de
                             int64_t nrot);
 
 /*
+ * Content key of a distance map, for a caller that keeps one map resident across calls: a 64-bit
+ * FNV-1a hash of n and of `samples` values spread evenly over the array, first and last
+ * included (every value when samples <= 0 or samples >= n); never 0.  MATLAB frees each call's
+ * single(reshape(proj_bin_bw,1,[])) temporary (ForwardCalc_OR_space_comp_cuda.m:22), so a later
+ * call's array can sit at the same address with other contents: compare keys, not pointers.  A
+ * map changed only between sampled positions keeps its key; a caller that edits maps in place
+ * uploads with grc_upload_masks.  A host function: no GPU work.  (No counterpart in the
+ * reference, which uploads the map on every call.)
+ */
+uint64_t grc_map_key(const float *proj_bin_bw, int64_t n, int64_t samples);
+
+/*
+ * grc_upload_masks when the map's key (grc_map_key with `samples`) or dimensions differ from
+ * those of the last upload through this entry; *uploaded (optional) says whether it uploaded.
+ * Any other upload (grc_upload_masks*, a drop-in entry with a map) clears the recorded key.
+ */
+int grc_upload_masks_if_changed(grc_ctx *ctx, const float *proj_bin_bw, int64_t detzsize, int64_t detysize,
+                                int64_t nrot, int64_t samples, int *uploaded);
+
+/*
  * Geometry shared by all scorer calls: S, B, RotDet (9 floats, row-major),
  * hkl (3*nhkl floats), rot_angles (nrot floats, degrees) and the 20-float
  * param vector [nhkl nrot Lsam2sou Lsam2det P0y P0z dety00 detz00 pixelysize
@@ -209,6 +229,76 @@ int grc_score_trials_device(grc_ctx *ctx, const double *d_pos, int64_t n_vox, co
                             float *d_out);
 
 /*
+ * The same trial list in completeness-only form with the first maximum of every group of
+ * group_size consecutive trials (n_trials a multiple of group_size): d_best[g] = 0-based index
+ * within group g of its first trial of largest completeness (NaN ignored: MATLAB max), d_best_c[g]
+ * that completeness (NaN when every trial of the group is 0/0).  This is the local refine of
+ * fit_OR_constrain_with_local_comp_cuda.m:100-110 ([~,ind0] = max(Output(1+nr_per_OR*(j-1):
+ * nr_per_OR*j, 3)), one group per candidate grid) and :60 (one group).  d_out (4 floats per trial,
+ * column 4 as set by grc_set_median) may be NULL; d_best and d_best_c may be NULL.
+ */
+int grc_score_trials_argmax_device(grc_ctx *ctx, const double *d_pos, int64_t n_vox, const double *d_q, int64_t n_q,
+                                   const int32_t *d_trial_voxel, const int32_t *d_trial_orient, int64_t n_trials,
+                                   int64_t group_size, float *d_out, int32_t *d_best, float *d_best_c);
+
+/*
+ * Seeding scan with the first maximum over each voxel's orientations: grc_forward_comp_device
+ * plus d_best[v] (0-based orientation index of voxel v's first largest completeness, NaN
+ * ignored) and d_best_c[v] (that completeness).  d_out may be NULL.
+ */
+int grc_forward_comp_argmax_device(grc_ctx *ctx, const float *d_pos, int64_t n_vox, const float *d_q, int64_t n_q,
+                                   float *d_out, int32_t *d_best, float *d_best_c);
+
+/*
+ * Seeding steps 1-2 for n seeds in one call (GrainMapping_engine_gpu_comp.m:72-111): the
+ * completeness-only scan of every seed (d_pos: 3 floats per seed [mm]) against the n_q
+ * orientations of d_q (4 floats [q0 q1 q2 q3] each, as the MEX receives them), then per seed the
+ * first n_top rows of sortrows(Output, 3, 'descend') -- NaN first, larger completeness next, equal
+ * values in grid order.  d_idx (n*n_top int32): 0-based rows of d_q, best first; d_cand (optional,
+ * n*n_top*4 doubles): those rows, taken from d_q64 (the same orientations in double, optional) or
+ * else widened from d_q; d_out (optional, 4*n*n_q floats): the scan, column 4 NaN.
+ * 1 <= n_top <= min(4096, n_q).
+ */
+int grc_seed_candidates_device(grc_ctx *ctx, const float *d_pos, int64_t n, const float *d_q, const double *d_q64,
+                               int64_t n_q, int n_top, int32_t *d_idx, double *d_cand, float *d_out);
+
+/*
+ * Seeding step 3 for n seeds with k candidates each (fit_OR_constrain_with_local_comp_cuda.m:12-49,
+ * 100-116): every candidate's ori_local_sampling(q, nr, gridsize) grid ((nr+1)^3 + 1 rows in
+ * unique(q,'rows') order, scored rounded to float32 as the MEX receives them) at its seed, in
+ * completeness-only mode, and the first maximum of each grid; then per seed the candidates in
+ * sortrows(Output_max, 3, 'descend') order.  d_pos: 3 doubles per seed; d_cand: n*k*4 doubles.
+ * Out, per seed in that order: d_best_q (n*k*4 doubles, the FP64 grid row of each maximum),
+ * d_best_c (n*k floats, its completeness), d_order (n*k int32, the 0-based candidate it came
+ * from), and optionally d_x0 (n*n_x0*3 doubles: [b c d] of the first n_x0 rows, the start points
+ * of the orientation fit, :116).  At most 1024 grid rows (nr <= 9) and 4096 candidates per seed.
+ */
+int grc_seed_refine_device(grc_ctx *ctx, const double *d_pos, int64_t n, const double *d_cand, int k, int nr,
+                           double gridsize, int n_x0, double *d_best_q, float *d_best_c, int32_t *d_order,
+                           double *d_x0);
+
+/*
+ * ori_local_sampling(q, nr, gridsize) (ori_local_sampling.m:12-34) of n_cand quaternions (4 doubles
+ * each): (nr+1)^3 + 1 rows per candidate [sqrt(1-(b^2+c^2+d^2)) b c d] with the centre row, in
+ * unique(q,'rows') order (a row equal to another stays beside it), into d_rows (doubles) and
+ * optionally d_rows_f32 (the same rows rounded to float32).  nr <= 9.
+ */
+int grc_local_grid_device(grc_ctx *ctx, const double *d_cand, int64_t n_cand, int nr, double gridsize,
+                          double *d_rows, float *d_rows_f32);
+
+/*
+ * Median of the seeding-scan entries (grc_forward_comp, grc_forward_comp_device,
+ * grc_score_trials_device and the two argmax forms above).  1 (default): the reference's four
+ * columns, dis_median exact.  0: completeness only -- column 4 is NaN and Nr_simu, Nr_intersect
+ * come from a bit-packed hit mask (1 bit per pixel: distance <= the hit threshold), which the
+ * context builds on the device from its resident map when first needed.  The seeding engine reads
+ * column 3 only: GrainMapping_engine_gpu_comp.m:103 sorts the scan on it and
+ * fit_OR_constrain_with_local_comp_cuda.m:60,105 take its maximum.  Grow and compete always
+ * compute the median (their accept rule reads it), and so does grc_forward_comp_noalloc.
+ */
+int grc_set_median(grc_ctx *ctx, int enable);
+
+/*
  * Batched orientation fit of the seeding stage: for each of n seeds, a bounded
  * Nelder-Mead (fminsearchbnd over (q1, q2, q3), bounds max(x0-hw,-1)..min(x0+hw,1),
  * q0 = sqrt(1 - q1^2 - q2^2 - q3^2)) minimising 1 - completeness at the seed position.
@@ -285,7 +375,7 @@ int grc_forward_comp_noalloc(grc_ctx *ctx, const float *pos, const float *d_q, i
  * per-voxel argmax into d_out8, and the optional map update) with no host
  * synchronisation; grc_batch_capture records that sequence into a CUDA graph that
  * grc_batch_replay launches.  grc_batch_autotune times the scoring tile shapes
- * (per-trial kernel, or the projection-window sweep holding 16/32/48/64 trials per CTA)
+ * (per-trial kernel, or the CTA sweep or warp scan holding 16/32/48/64 trials per CTA)
  * on the first max_voxels voxels, keeps the fastest for this batch and caches it per
  * geometry for later batches.  grc_batch_set_maps makes every run also write each
  * voxel's completeness, grain id, dis_median, Nr_intersect and VisitFlag = 0.5 into
@@ -368,7 +458,7 @@ typedef struct {
     int64_t refined;         /* trials whose median needed the exact refine pass */
     int64_t kernel_launches; /* kernels enqueued by the call */
     double score_ms;         /* device time of the scoring kernel(s) (CUDA events), 0 if not timed */
-    int64_t path;            /* 1 = per-trial kernel, 2 = projection-window sweep */
+    int64_t path;            /* 1 = per-trial kernel, 2 = CTA sweep, 3 = warp scan */
     int64_t audit_checked;   /* audit builds only: FP32 decisions re-decided in FP64 */
     int64_t audit_mismatch;  /* audit builds only: of those, decisions that differed */
 } grc_stats;
@@ -376,11 +466,13 @@ int grc_last_stats(grc_ctx *ctx, grc_stats *out);
 /* 1 = record CUDA events around the scoring kernel of each call (for benchmarks). */
 int grc_set_timing(grc_ctx *ctx, int enable);
 /*
- * Scoring kernel selection: 0 = by size (default: the projection-window sweep, which
- * keeps the map windows L2-resident, once a call holds 1/16 of a sweep round of trials --
- * 1,776 on 148 SMs -- when each voxel carries at least 64 orientations, or half a round
- * otherwise; the per-trial kernel below that), 1 = always the per-trial kernel,
- * 2 = always the sweep.  Results are identical; only speed differs.
+ * Scoring kernel selection: 0 = by size (default: the projection-window sweep, which keeps the
+ * map windows L2-resident, once a call holds 1/16 of a round of trials -- 1,776 on 148 SMs --
+ * when each voxel carries at least 64 orientations, or half a round otherwise; the per-trial
+ * kernel below that), 1 = always the per-trial kernel, 2 = always the sweep, 3 = always the warp
+ * scan (the same windows with one trial per warp at a time; slower on the benchmark
+ * geometries).  Results are identical; only speed differs.  Batches (grc_batch_*) read the same
+ * codes for their tile choice.
  */
 int grc_set_path(grc_ctx *ctx, int path);
 

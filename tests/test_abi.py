@@ -57,3 +57,24 @@ def test_no_cpu_fallback_in_product_path():
             if f.endswith((".py", ".cu", ".h", ".cuh")):
                 txt = open(os.path.join(dirpath, f)).read()
                 assert "oracle" not in re.sub(r"#.*|//.*", "", txt).replace("the oracle", ""), f
+
+
+def test_map_key_follows_content_not_address():
+    """grc_map_key (a host function): equal contents in different buffers give equal keys; a
+    changed sampled value, a different size or a changed value of a fully sampled map change it."""
+    import numpy as np
+    rng = np.random.default_rng(0)
+    a = rng.random(1_000_003).astype(np.float32)
+    b = a.copy()
+    assert _lib.map_key(a, 4096) == _lib.map_key(b, 4096) != 0
+    b[0] += 1  # the first value is always sampled
+    assert _lib.map_key(a, 4096) != _lib.map_key(b, 4096)
+    b[:] = a
+    b[-1] += 1  # and the last
+    assert _lib.map_key(a, 4096) != _lib.map_key(b, 4096)
+    assert _lib.map_key(a[:-1], 4096) != _lib.map_key(a, 4096)
+    small = rng.random(1000).astype(np.float32)
+    for i in (1, 500, 998):  # every value of a map no larger than the sample count
+        c = small.copy()
+        c[i] = -c[i]
+        assert _lib.map_key(c, 4096) != _lib.map_key(small, 4096)

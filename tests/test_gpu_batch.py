@@ -52,7 +52,7 @@ def test_batch_graph_replay_and_autotune(setup):
     b = ctx.batch(dev["rows5"], m, dev["ids"], ids.size, dev["eul"], len(eul), param1)
     out = torch.zeros(8 * m, dtype=torch.float32, device="cuda")
     tune = b.autotune(out)
-    assert tune["path"] in (1, 2) and tune["ms"] > 0
+    assert tune["path"] in (1, 2, 3) and tune["ms"] > 0
     assert b.info()["path"] == tune["path"]
     out.zero_()
     b.capture(out)

@@ -1,9 +1,9 @@
 """Parity on the full benchmark geometries and the grid-argmax known-answer case.
 
 * BCC Fe, 1024^2 detector, 181 projections, 86 reflections (the CPU-runnable configuration) and
-  FCC Al, 2048^2 detector, 361 projections, 64 reflections (the seeding configuration), on both
-  scoring kernels: Nr_simu, Nr_intersect, completeness, dis_median and the per-voxel argmax over
-  orientations equal the oracle's on every trial.  The one allowance is a trial holding a
+  FCC Al, 2048^2 detector, 361 projections, 64 reflections (the seeding configuration), on every
+  scoring kernel and on the completeness-only scan: Nr_simu, Nr_intersect, completeness,
+  dis_median and the per-voxel argmax over orientations equal the oracle's on every trial.  The one allowance is a trial holding a
   reflection whose oracle landing lies within 1e-9 px of a rounding boundary (or whose
   wavelength or Bragg angle lies within a relative 1e-12 of a window bound): there two correct
   FP64 evaluations may round apart, so its counts may differ by at most that number.  Such
@@ -63,16 +63,22 @@ def _parity(s, ctx, host, n_vox, n_q, seed):
         ref, edges, tight = O.orientation_scan(pos, q, S9, B9, hkl, host, rot, R9, p, tight=True)
         ref = ref.reshape(-1, 4)
         exact = tight == 0
-        for path in (1, 2):
+        # every kernel with the median, then the completeness-only scan (bit-packed mask, no median)
+        for path, median in ((1, True), (2, True), (3, True), (2, False), (3, False)):
             ctx.set_path(path)
+            ctx.set_median(median)
             gpu = ctx.forward_comp(pos, q, S9, B9, hkl, None, rot, R9, p).reshape(-1, 4)
             assert ctx.last_stats()["path"] == path
-            np.testing.assert_array_equal(gpu[exact], ref[exact], err_msg=f"kernel path {path}")
+            cols = 4 if median else 3
+            np.testing.assert_array_equal(gpu[exact, :cols], ref[exact, :cols], err_msg=f"kernel path {path}")
+            if not median:
+                assert np.isnan(gpu[:, 3]).all()
             d = np.abs(gpu[~exact, :2] - ref[~exact, :2]).max(axis=1) if (~exact).any() else np.zeros(0)
             assert np.all(d <= tight[~exact])
             if exact.all():
                 assert _first_max(gpu[:, 2]) == _first_max(ref[:, 2])
         ctx.set_path(0)
+        ctx.set_median(True)
         n_all += len(q)
         n_listed += int((edges > 0).sum())
         n_tight += int((~exact).sum())

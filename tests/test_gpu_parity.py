@@ -24,9 +24,9 @@ GOLD = os.path.join(os.path.dirname(__file__), "golden", "forward_comp_fe_tiny.n
 MED_RTOL = 1e-6
 
 
-@pytest.fixture(scope="module", params=[1, 2], ids=["per-trial", "sweep"])
+@pytest.fixture(scope="module", params=[1, 2, 3], ids=["per-trial", "sweep", "scan"])
 def ctx(request):
-    """Every parity test runs on both scoring kernels (results must be identical)."""
+    """Every parity test runs on every scoring kernel (results must be identical)."""
     c = Context(0)
     c.set_path(request.param)
     yield c
@@ -172,7 +172,7 @@ def test_refine_path_and_wide_codes(ctx, fe_small):
         assert info["code_bits"] == (16 if nlev < 65536 else 32)
         st = ctx.last_stats()
         assert st["refined"] > 0
-        assert st["path"] in (1, 2)
+        assert st["path"] in (1, 2, 3)
         ref, _, edges = O.orientation_scan(pos, q, S9, B9, hkl, dmap, rot, R9, p, tight=True)
         compare_forward(gpu, ref.reshape(-1, 4), edges, f"levels={nlev}")
 

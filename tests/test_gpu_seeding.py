@@ -116,13 +116,14 @@ def test_trial_list_voxel_orders(scene):
             tv = tv.astype(np.int32)
             to = rng.integers(0, 730, n).astype(np.int32)
             res = {}
-            for path in (2, 1):
+            for path in (2, 3, 1):
                 ctx.set_path(path)
                 out = torch.empty(n * 4, dtype=torch.float32, device="cuda")
                 ctx.score_trials_device(d(pos), 40, d(qs), 730, d(tv), d(to), n, out)
                 res[path] = out.view(-1, 4).cpu().numpy()
                 assert ctx.last_stats()["path"] == path, name
             np.testing.assert_array_equal(res[2], res[1], err_msg=name)
+            np.testing.assert_array_equal(res[3], res[1], err_msg=name)
             assert np.nanmax(res[2][:, 2]) > 0.9, name  # near-true orientations are scored
     finally:
         ctx.set_path(0)
