@@ -33,7 +33,8 @@ EXPORTS = [
     "grc_fit_geometry_rms", "grc_score_trials_device", "grc_fit_orientation_nm", "grc_pair_spots",
     "grc_walk_best_first", "grc_grow_best_first", "grc_score_trials_argmax_device", "grc_forward_comp_argmax_device",
     "grc_set_median", "grc_seed_candidates_device", "grc_seed_refine_device", "grc_local_grid_device",
-    "grc_map_key", "grc_upload_masks_if_changed",
+    "grc_map_key", "grc_upload_masks_if_changed", "grc_upload_spot_masks", "grc_save_packed_masks",
+    "grc_load_packed_masks",
 ]
 
 # grc_walk_score_fn of the C header
@@ -126,6 +127,9 @@ def load(path: str | None = None):
         "grc_seed_refine_device": [vp, f, i64, f, i, i, d, i, f, f, f, f],
         "grc_local_grid_device": [vp, f, i64, i, d, f, f],
         "grc_map_key": [f, i64, i64],
+        "grc_upload_spot_masks": [vp, f, i64, i64, i64],
+        "grc_save_packed_masks": [vp, C.c_char_p],
+        "grc_load_packed_masks": [vp, C.c_char_p],
         "grc_upload_masks_if_changed": [vp, f, i64, i64, i64, i64, C.POINTER(i)],
         "grc_fit_orientation_nm": [vp, f, f, i64, d, i, i, d, d, f, f, f, f, f],
         "grc_pair_spots": [vp, f, f, i64, f, i64, f, f, i64, C.POINTER(i64)],
@@ -304,6 +308,17 @@ class Context:
         self._check(self.L.grc_upload_masks_if_changed(self.h, _ptr(a), detzsize, detysize, nrot, samples,
                                                        C.byref(up)))
         return bool(up.value)
+
+    def upload_spot_masks(self, proj_bin, detzsize: int, detysize: int, nrot: int):
+        """Binary spot images (nonzero = spot; host array or device tensor) -> device bwdist map."""
+        a = proj_bin if hasattr(proj_bin, "data_ptr") else np.ascontiguousarray(proj_bin, dtype=np.uint8).reshape(-1)
+        self._dev(self.L.grc_upload_spot_masks, _ptr(a), detzsize, detysize, nrot)
+
+    def save_packed_masks(self, path: str):
+        self._check(self.L.grc_save_packed_masks(self.h, os.fsencode(path)))
+
+    def load_packed_masks(self, path: str):
+        self._check(self.L.grc_load_packed_masks(self.h, os.fsencode(path)))
 
     def set_geometry(self, S, B, hkl, rot_angles, RotDet, param):
         keep = [f32(x) for x in (S, B, hkl, rot_angles, RotDet, param)]

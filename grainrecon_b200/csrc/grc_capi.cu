@@ -356,8 +356,8 @@ int run_score(grc_ctx *ctx, const grc::Work &w, int64_t n_trials, bool comp = fa
     const int64_t from = shared_voxels ? (round + 15) / 16 : (round + 1) / 2;
     bool fused_key = false;
     if (round > 0 && (ctx->force_path >= 2 || n_trials >= from)) {
-        // projection-window scans (L2-resident map windows) for large trial counts: the CTA sweep,
-        // or the warp scan when asked for by grc_set_path(3)
+        // projection-window scans (L2-resident map windows) for large trial counts: the warp scan,
+        // or the CTA sweep when asked for by grc_set_path(2)
         TRY(ensure(ctx, ctx->rlist, sizeof(int64_t) * n_trials));
         grc::ScoreBufs b = bufs(ctx);
         if (comp && gkey) {  // completeness mode folds the first maximum per group in
@@ -366,12 +366,12 @@ int run_score(grc_ctx *ctx, const grc::Work &w, int64_t n_trials, bool comp = fa
             fused_key = true;
         }
         const int mode = comp ? grc::kScanComp : grc::kScanFull;
-        if (ctx->force_path == 3) {
-            e = grc::launch_scan(ctx->geo, b, w, n_trials, ctx->num_sms, mode, ctx->stream, e0, e1, &launches);
-            ctx->stats.path = 3;
-        } else {
+        if (ctx->force_path == 2) {
             e = grc::launch_sweep(ctx->geo, b, w, n_trials, ctx->num_sms, ctx->stream, e0, e1, &launches, 0, mode);
             ctx->stats.path = 2;
+        } else {
+            e = grc::launch_scan(ctx->geo, b, w, n_trials, ctx->num_sms, mode, ctx->stream, e0, e1, &launches);
+            ctx->stats.path = 3;
         }
     } else {
         e = grc::launch_score(ctx->geo, bufs(ctx), w, ctx->num_sms, ctx->stream, e0, e1, &launches);
@@ -1145,6 +1145,149 @@ int grc_upload_masks_if_changed(grc_ctx *ctx, const float *map, int64_t detzsize
     return GRC_OK;
 }
 
+}  // extern "C"
+
+namespace {
+
+// Distance map from binary spot images on the device: bwdist (exact EDT) of every projection, then
+// the rank coding of upload_device_map.  d_mask: one byte per pixel (nonzero = spot).
+int upload_spot_device(grc_ctx *ctx, const uint8_t *d_mask, int64_t dz, int64_t dy, int64_t nrot) {
+    const int64_t n = dz * dy * nrot;
+    float *d_map = nullptr;
+    cudaError_t e = cudaMalloc(&d_map, sizeof(float) * n);
+    if (e != cudaSuccess) return fail(ctx, GRC_ECUDA, "cudaMalloc(distance map): %s", cudaGetErrorString(e));
+    e = grc::launch_edt(d_mask, dz, dy, nrot, d_map, ctx->stream);
+    int r = e == cudaSuccess ? upload_device_map(ctx, d_map, dz, dy, nrot)
+                             : fail(ctx, GRC_ECUDA, "bwdist: %s", cudaGetErrorString(e));
+    cudaStreamSynchronize(ctx->stream);
+    cudaFree(d_map);
+    return r;
+}
+
+int upload_spot_host(grc_ctx *ctx, const uint8_t *mask, int64_t dz, int64_t dy, int64_t nrot) {
+    const int64_t n = dz * dy * nrot;
+    uint8_t *d_mask = nullptr;
+    cudaError_t e = cudaMalloc(&d_mask, n);
+    if (e != cudaSuccess) return fail(ctx, GRC_ECUDA, "cudaMalloc(spot masks): %s", cudaGetErrorString(e));
+    e = cudaMemcpyAsync(d_mask, mask, n, cudaMemcpyHostToDevice, ctx->stream);
+    int r = e == cudaSuccess ? upload_spot_device(ctx, d_mask, dz, dy, nrot)
+                             : fail(ctx, GRC_ECUDA, "spot-mask upload: %s", cudaGetErrorString(e));
+    cudaStreamSynchronize(ctx->stream);
+    cudaFree(d_mask);
+    return r;
+}
+
+// Packed-mask file: this header, then nrot * plane_words little-endian 32-bit words (bit p&31 of
+// word p>>5 of each projection = spot pixel p, p = (dety-1)*detzsize + (detz-1)).
+struct PackedHeader {
+    char magic[8];          // "GRCMASK1"
+    uint32_t version;       // 1
+    uint32_t header_bytes;  // sizeof(PackedHeader)
+    int64_t detzsize, detysize, nrot, plane_words;
+    uint64_t key;           // FNV-1a of the words
+    uint64_t reserved[3];
+};
+static_assert(sizeof(PackedHeader) == 80, "packed-mask header layout");
+const char kPackedMagic[8] = {'G', 'R', 'C', 'M', 'A', 'S', 'K', '1'};
+
+uint64_t words_key(const uint32_t *w, int64_t n) {
+    uint64_t h = 1469598103934665603ull;
+    for (int64_t i = 0; i < n; ++i) {
+        uint32_t v = w[i];
+        for (int b = 0; b < 4; ++b) {
+            h ^= (v >> (8 * b)) & 0xffu;
+            h *= 1099511628211ull;
+        }
+    }
+    return h;
+}
+
+}  // namespace
+
+extern "C" {
+
+int grc_upload_spot_masks(grc_ctx *ctx, const uint8_t *proj_bin, int64_t detzsize, int64_t detysize, int64_t nrot) {
+    if (!ctx) return GRC_EINVAL;
+    Lock l(ctx);
+    if (!proj_bin) return fail(ctx, GRC_EINVAL, "proj_bin is NULL");
+    if (detzsize < 1 || detysize < 1 || nrot < 1) return fail(ctx, GRC_EINVAL, "spot-mask dimensions must be positive");
+    if (is_device_ptr(proj_bin)) return upload_spot_device(ctx, proj_bin, detzsize, detysize, nrot);
+    return upload_spot_host(ctx, proj_bin, detzsize, detysize, nrot);
+}
+
+int grc_save_packed_masks(grc_ctx *ctx, const char *path) {
+    if (!ctx) return GRC_EINVAL;
+    Lock l(ctx);
+    if (!path) return fail(ctx, GRC_EINVAL, "save: NULL path");
+    if (!ctx->has_masks) return fail(ctx, GRC_ENOMASK, "save: no map resident");
+    const int64_t plane = ctx->mz * ctx->my, pw = (plane + 127) / 128 * 4, nw = pw * ctx->mrot;
+    // spot pixels = distance 0 = code 0 when the smallest distinct value is 0
+    const uint32_t n_spot = (!ctx->h_vals.empty() && ctx->h_vals[0] == 0.0f) ? 1u : 0u;
+    uint32_t *d_bits = nullptr;
+    cudaError_t e = cudaMalloc(&d_bits, sizeof(uint32_t) * nw);
+    if (e != cudaSuccess) return fail(ctx, GRC_ECUDA, "save: cudaMalloc: %s", cudaGetErrorString(e));
+    std::vector<uint32_t> h((size_t)nw);
+    e = grc::launch_pack_bits(ctx->mc.codes8, 1, plane, ctx->mrot, n_spot, pw, d_bits, ctx->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(h.data(), d_bits, sizeof(uint32_t) * nw, cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    cudaFree(d_bits);
+    if (e != cudaSuccess) return fail(ctx, GRC_ECUDA, "save: %s", cudaGetErrorString(e));
+    PackedHeader hd{};
+    std::memcpy(hd.magic, kPackedMagic, 8);
+    hd.version = 1;
+    hd.header_bytes = sizeof(PackedHeader);
+    hd.detzsize = ctx->mz;
+    hd.detysize = ctx->my;
+    hd.nrot = ctx->mrot;
+    hd.plane_words = pw;
+    hd.key = words_key(h.data(), nw);
+    FILE *f = std::fopen(path, "wb");
+    if (!f) return fail(ctx, GRC_EINVAL, "save: cannot open %s", path);
+    const bool ok = std::fwrite(&hd, sizeof hd, 1, f) == 1 &&
+                    std::fwrite(h.data(), sizeof(uint32_t), (size_t)nw, f) == (size_t)nw;
+    const bool closed = std::fclose(f) == 0;
+    if (!ok || !closed) return fail(ctx, GRC_EINVAL, "save: write to %s failed", path);
+    return GRC_OK;
+}
+
+int grc_load_packed_masks(grc_ctx *ctx, const char *path) {
+    if (!ctx) return GRC_EINVAL;
+    Lock l(ctx);
+    if (!path) return fail(ctx, GRC_EINVAL, "load: NULL path");
+    FILE *f = std::fopen(path, "rb");
+    if (!f) return fail(ctx, GRC_EINVAL, "load: cannot open %s", path);
+    PackedHeader hd{};
+    if (std::fread(&hd, sizeof hd, 1, f) != 1 || std::memcmp(hd.magic, kPackedMagic, 8) != 0 || hd.version != 1 ||
+        hd.header_bytes != sizeof(PackedHeader)) {
+        std::fclose(f);
+        return fail(ctx, GRC_EINVAL, "load: %s is not a packed-mask file (version 1)", path);
+    }
+    if (hd.detzsize < 1 || hd.detysize < 1 || hd.nrot < 1 || hd.detzsize > 1000000 || hd.detysize > 1000000 ||
+        hd.nrot > GRC_MAX_NROT || hd.plane_words != (hd.detzsize * hd.detysize + 127) / 128 * 4) {
+        std::fclose(f);
+        return fail(ctx, GRC_EINVAL, "load: %s has an inconsistent header", path);
+    }
+    const int64_t nw = hd.plane_words * hd.nrot, plane = hd.detzsize * hd.detysize;
+    std::vector<uint32_t> h((size_t)nw);
+    const bool full = std::fread(h.data(), sizeof(uint32_t), (size_t)nw, f) == (size_t)nw;
+    std::fclose(f);
+    if (!full) return fail(ctx, GRC_EINVAL, "load: %s is truncated", path);
+    if (words_key(h.data(), nw) != hd.key) return fail(ctx, GRC_EINVAL, "load: %s fails its content key", path);
+    uint32_t *d_bits = nullptr;
+    uint8_t *d_mask = nullptr;
+    cudaError_t e = cudaMalloc(&d_bits, sizeof(uint32_t) * nw);
+    if (e == cudaSuccess) e = cudaMalloc(&d_mask, plane * hd.nrot);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(d_bits, h.data(), sizeof(uint32_t) * nw, cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess) e = grc::launch_unpack_bits(d_bits, plane, hd.nrot, hd.plane_words, d_mask, ctx->stream);
+    int r = e == cudaSuccess ? upload_spot_device(ctx, d_mask, hd.detzsize, hd.detysize, hd.nrot)
+                             : fail(ctx, GRC_ECUDA, "load: %s", cudaGetErrorString(e));
+    cudaStreamSynchronize(ctx->stream);
+    cudaFree(d_bits);
+    cudaFree(d_mask);
+    return r;
+}
+
 int grc_set_median(grc_ctx *ctx, int enable) {
     if (!ctx) return GRC_EINVAL;
     Lock l(ctx);
@@ -1570,9 +1713,9 @@ int batch_enqueue(grc_batch *bt, float *d_out8, float *d_trial_out, int path, in
     w.n_items = m_lim;
     cudaError_t e = cudaSuccess;
     if (T > 0) {
-        // path 1: per-trial kernel; 2 (and 0 from half a round on): CTA sweep; 3: warp scan
+        // path 1: per-trial kernel; 2: CTA sweep; 3 (and 0 from half a round on): warp scan
         const int64_t sr = grc::sweep_round_trials(ctx->geo, ctx->num_sms);
-        const int use = sr == 0 ? 1 : (path != 0 ? path : (T * 2 >= sr ? 2 : 1));
+        const int use = sr == 0 ? 1 : (path != 0 ? path : (T * 2 >= sr ? 3 : 1));
         if (use == 2)
             e = grc::launch_sweep(ctx->geo, b, w, T, ctx->num_sms, ctx->stream, e0, e1, launches, slots);
         else if (use == 3)

@@ -36,10 +36,12 @@ static_assert(sizeof(RowF) == 64, "RowF layout");
 // FP64 chain stays below 1.4e-3 px on the 1024^2 / 2048^2 geometries (measured over
 // 3.4e5 landings); landings closer than this to a half-pixel boundary are recomputed
 // in FP64, so every decision equals the FP64 one.  A build with -DGRC_AUDIT re-decides
-// every FP32 decision in FP64: at 0.006 px it found no disagreement in 1.14e10 decisions
-// (FCC Al 2048^2 x 361 and BCC Fe 1024^2 x 181 scans), at 0.001 px two in 1.7e9.
+// every FP32 decision in FP64 (CTA sweep): at 0.003 px it found no disagreement in
+// 1.72e10 decisions (FCC Al 2048^2 x 361 and BCC Fe 1024^2 x 181 scans, 64 seeds x 32,768
+// orientations each), at 0.001 px two in 1.7e9; the band keeps a third above the audited
+// 0.003 px.
 #ifndef GRC_AMBIG_PX
-#define GRC_AMBIG_PX 0.006f
+#define GRC_AMBIG_PX 0.004f
 #endif
 constexpr float kAmbigPx = GRC_AMBIG_PX;
 

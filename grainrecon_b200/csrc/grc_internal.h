@@ -123,6 +123,9 @@ int local_grid_rows(int nr);
 cudaError_t launch_local_grid(const double *cand, int64_t n_cand, int nr, double gridsize, double *out,
                               double *out_r32, float *out_f32, cudaStream_t s);
 cudaError_t launch_block_lists(int64_t n, int64_t per_voxel, int32_t *voxel, int32_t *orient, cudaStream_t s);
+// Packed mask back to one byte per pixel (1 = bit set), layout of the distance map.
+cudaError_t launch_unpack_bits(const uint32_t *bits, int64_t plane, int64_t nrot, int64_t plane_words, uint8_t *mask,
+                               cudaStream_t s);
 // Bit-packed hit mask from the 8-bit (or full-width) codes: bit = code < n_hit.
 cudaError_t launch_pack_bits(const void *codes, int code_bytes, int64_t plane, int64_t nrot, uint32_t n_hit,
                              int64_t plane_words, uint32_t *bits, cudaStream_t s);

@@ -4,21 +4,17 @@
 // every CTA walking the projections window by window so the map pixels being read stay in L2),
 // organised around the warp instead of the CTA:
 //   * a warp takes one trial (slot) of the window at a time and first writes that trial's FP32
-//     Gw table and window thresholds for all reflections into its own shared-memory table, so
-//     the per-item landing reads them instead of recomputing S*U*B*h;
-//   * reflections are tested with lanes on projections: every lane holds the incident direction
-//     k_w of one projection of the window, and a reflection is tested only when a bound over the
-//     whole window (centre and radius of the window's k_w) lets its wavelength window be met.
-//     About half of the (reflection, window) pairs are skipped that way, without one test per
-//     projection;
+//     Gw table and window thresholds for all reflections into its own shared-memory table; the
+//     prefilter keeps them in registers (lanes on reflections, as the sweep) and the per-item
+//     landing reads them from the table instead of recomputing S*U*B*h and the window;
 //   * the survivors of a trial go through a per-warp queue, 32 at a time, through the FP32 landing
-//     chain with its FP64 band (landing_fp32 / landing_exact), and their pixels are counted in
-//     registers of the warp (completeness-only mode: one bit of the packed hit mask per pixel) or
-//     in the trial's 8-bit code histogram (full mode: Nr_simu, Nr_intersect and the exact median).
+//     chain with its FP64 band (landing_fp32 / landing_exact), and the queue is emptied at the end
+//     of the trial, so every batch belongs to one trial: its pixels are counted in one register
+//     of the warp (completeness-only mode: one bit of the packed hit mask per pixel) or in the
+//     trial's 8-bit code histogram (full mode: Nr_simu, Nr_intersect and the exact median).
 // Ambiguous items keep their trial in the FP64 queue, which is drained at the end of the window.
 // The decisions are those of the sweep and of the oracle: same prefilter margins, same FP32
-// chain and band, same FP64 path; the window bound only skips reflections whose prefilter test
-// fails on every projection of the window.
+// chain and band, same FP64 path.
 #include <cuda_runtime.h>
 #include <math_constants.h>
 #include <stdint.h>
@@ -36,7 +32,6 @@ namespace {
 constexpr int kScanSlots = 96;      // most trials a CTA holds in one round
 constexpr int kScanSlotsBulk = 64;  // tile of multi-round work and of explicit voxel lists
 constexpr int kScanWinMin = 8;
-constexpr int kScanQueue = 64;      // < 32 left over + one reflection of 32 projections
 constexpr int kHistWords = 128;     // 256 u16 bins per slot, two per word
 constexpr unsigned kAll = 0xffffffffu;
 
@@ -53,10 +48,8 @@ __device__ __forceinline__ int64_t scan_orient_of(const Work &w, int64_t t, int6
 
 struct ScanSmem {
     RowF *rows;        // [rows_cap * nwin] omega rows of the window, vloc * nwin + wl
-    float4 *kcr;       // [rows_cap] centre (x, y, z) and radius of the window's k_w per voxel
     float4 *hk;        // [nhkl] h as float
-    uint32_t *hist;    // full mode: [slots * kHistWords]
-    int2 *cnt;         // completeness mode: [slots] (Nr_simu, Nr_intersect)
+    uint32_t *hist;    // full mode: [slots * kHistWords]; completeness mode: [slots] packed counters
     float *subf;       // [slots * 12]
     double *subd;      // [slots * 9]
     int *vloc;         // [slots]
@@ -64,11 +57,11 @@ struct ScanSmem {
     int64_t *vlist;    // [slots]
     float4 *wgw;       // [kWarps * nhkl] per-warp Gw table of the warp's trial: x, y, z, 1/|G|
     float4 *wwin;      // [kWarps * nhkl] its window thresholds (window_f)
-    uint32_t *queue;   // [kWarps * kScanQueue]
+    uint32_t *queue;   // [kWarps * kQueueCap]
     uint32_t *fqueue;  // [kWarps * kFallbackCap]
 };
 
-constexpr int kScanParts = 13;
+constexpr int kScanParts = 11;
 __host__ __device__ inline size_t scan_smem_layout(int mode, int nhkl, int rows_cap, int slots, int nwin,
                                                    size_t *offs) {
     size_t o = 0, i = 0;
@@ -78,10 +71,8 @@ __host__ __device__ inline size_t scan_smem_layout(int mode, int nhkl, int rows_
         o += bytes;
     };
     put(sizeof(RowF) * rows_cap * nwin);
-    put(sizeof(float4) * rows_cap);
     put(sizeof(float4) * nhkl);
-    put(mode == kScanFull ? sizeof(uint32_t) * slots * kHistWords : 0);
-    put(mode == kScanComp ? sizeof(int2) * slots : 0);
+    put(sizeof(uint32_t) * slots * (mode == kScanFull ? kHistWords : 1));
     put(sizeof(float) * slots * 12);
     put(sizeof(double) * slots * 9);
     put(sizeof(int) * slots);
@@ -89,7 +80,7 @@ __host__ __device__ inline size_t scan_smem_layout(int mode, int nhkl, int rows_
     put(sizeof(int64_t) * slots);
     put(sizeof(float4) * kWarps * nhkl);
     put(sizeof(float4) * kWarps * nhkl);
-    put(sizeof(uint32_t) * kWarps * kScanQueue);
+    put(sizeof(uint32_t) * kWarps * kQueueCap);
     o = (o + 15) & ~size_t(15);
     offs[i] = o;  // fqueue
     o += sizeof(uint32_t) * kWarps * kFallbackCap;
@@ -102,32 +93,18 @@ __device__ __forceinline__ ScanSmem scan_carve(unsigned char *base, int mode, in
     scan_smem_layout(mode, nhkl, rows_cap, slots, nwin, offs);
     ScanSmem m;
     m.rows = (RowF *)(base + offs[0]);
-    m.kcr = (float4 *)(base + offs[1]);
-    m.hk = (float4 *)(base + offs[2]);
-    m.hist = (uint32_t *)(base + offs[3]);
-    m.cnt = (int2 *)(base + offs[4]);
-    m.subf = (float *)(base + offs[5]);
-    m.subd = (double *)(base + offs[6]);
-    m.vloc = (int *)(base + offs[7]);
-    m.vglob = (int64_t *)(base + offs[8]);
-    m.vlist = (int64_t *)(base + offs[9]);
-    m.wgw = (float4 *)(base + offs[10]);
-    m.wwin = (float4 *)(base + offs[11]);
-    m.queue = (uint32_t *)(base + offs[12]);
-    m.fqueue = (uint32_t *)(base + offs[13]);
+    m.hk = (float4 *)(base + offs[1]);
+    m.hist = (uint32_t *)(base + offs[2]);
+    m.subf = (float *)(base + offs[3]);
+    m.subd = (double *)(base + offs[4]);
+    m.vloc = (int *)(base + offs[5]);
+    m.vglob = (int64_t *)(base + offs[6]);
+    m.vlist = (int64_t *)(base + offs[7]);
+    m.wgw = (float4 *)(base + offs[8]);
+    m.wwin = (float4 *)(base + offs[9]);
+    m.queue = (uint32_t *)(base + offs[10]);
+    m.fqueue = (uint32_t *)(base + offs[11]);
     return m;
-}
-
-__device__ __forceinline__ float warp_sum(float x) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(kAll, x, o);
-    return x;
-}
-
-__device__ __forceinline__ float warp_max(float x) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) x = fmaxf(x, __shfl_xor_sync(kAll, x, o));
-    return x;
 }
 
 template <int MODE, int HPL, int WIN>
@@ -141,7 +118,7 @@ __global__ void __launch_bounds__(kThreads, GRC_SCAN_BLOCKS)
     __shared__ int s_nv, s_next;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const unsigned lt = (1u << lane) - 1u;
-    uint32_t *wq = sm.queue + warp * kScanQueue;
+    uint32_t *wq = sm.queue + warp * kQueueCap;
     uint32_t *fq = sm.fqueue + warp * kFallbackCap;
     float4 *gwt = sm.wgw + warp * g.nhkl;
     float4 *wnt = sm.wwin + warp * g.nhkl;
@@ -159,10 +136,8 @@ __global__ void __launch_bounds__(kThreads, GRC_SCAN_BLOCKS)
             sm.subf[12 * tid + i] = (float)SUB[i];
         }
         sm.vglob[tid] = v;
-        if (MODE == kScanComp) sm.cnt[tid] = make_int2(0, 0);
     }
-    if (MODE == kScanFull)
-        for (int i = tid; i < slots * kHistWords; i += kThreads) sm.hist[i] = 0;
+    for (int i = tid; i < slots * (MODE == kScanFull ? kHistWords : 1); i += kThreads) sm.hist[i] = 0;
     for (int i = tid; i < g.nhkl; i += kThreads)
         sm.hk[i] = make_float4((float)b.hkl[3 * i], (float)b.hkl[3 * i + 1], (float)b.hkl[3 * i + 2], 0.f);
     __syncthreads();
@@ -187,24 +162,6 @@ __global__ void __launch_bounds__(kThreads, GRC_SCAN_BLOCKS)
         }
         if (tid == 0) s_next = 0;
         __syncthreads();
-        // ---- per voxel: centre and radius of the window's k_w (lanes on projections).  The radius
-        // carries 1e-5 on top, far above the FP32 rounding of the prefilter's dot products.
-        for (int vl = warp; vl < nv; vl += kWarps) {
-            float kx = 0.f, ky = 0.f, kz = 0.f;
-            const bool in = lane < nw;
-            if (in) {
-                const float4 k4 = reinterpret_cast<const float4 *>(sm.rows + vl * WIN + lane)[3];
-                kx = k4.x;
-                ky = k4.y;
-                kz = k4.z;
-            }
-            const float inv = 1.0f / (float)nw;
-            const float cx = warp_sum(kx) * inv, cy = warp_sum(ky) * inv, cz = warp_sum(kz) * inv;
-            const float dx = kx - cx, dy = ky - cy, dz = kz - cz;
-            const float d = warp_max(in ? sqrtf(dx * dx + dy * dy + dz * dz) : 0.f);
-            if (lane == 0) sm.kcr[vl] = make_float4(cx, cy, cz, d * 1.0001f + 1e-5f);
-        }
-        __syncthreads();
 
         const uint8_t *wcodes = MODE == kScanFull ? b.codes8 + (int64_t)w0 * g.plane : nullptr;
         const uint32_t *wbits = MODE == kScanComp ? b.bits + (int64_t)w0 * pw : nullptr;
@@ -220,8 +177,7 @@ __global__ void __launch_bounds__(kThreads, GRC_SCAN_BLOCKS)
             if (MODE == kScanComp) {
                 const int64_t iw = w0 + wl, ip = r64 - iw * g.plane;
                 const uint32_t word = __ldg(b.bits + iw * pw + (ip >> 5));
-                atomicAdd(&sm.cnt[s2].x, 1);
-                if ((word >> (ip & 31)) & 1u) atomicAdd(&sm.cnt[s2].y, 1);
+                atomicAdd(&sm.hist[s2], 1u + (((word >> (ip & 31)) & 1u) << 16));
             } else {
                 const uint32_t code = __ldg(b.codes8 + r64);
                 atomicAdd(&sm.hist[s2 * kHistWords + (code >> 1)], 1u << ((code & 1u) * 16));
@@ -239,58 +195,52 @@ __global__ void __launch_bounds__(kThreads, GRC_SCAN_BLOCKS)
             }
         };
 
-        // slots are handed out one at a time, so the warps of a CTA reach the end-of-window barrier
-        // together however unevenly the selected reflections fall on the slots
+        // slots are handed out one at a time, so the warps of a CTA reach the end-of-window
+        // barrier together however unevenly the selected reflections fall on the slots
         for (;;) {
             int s = 0;
             if (lane == 0) s = atomicAdd(&s_next, 1);
             s = __shfl_sync(kAll, s, 0);
             if (s >= nslot) break;
-            const int vl = sm.vloc[s];
-            const float4 kc = sm.kcr[vl];
             const float *sf = sm.subf + 12 * s;
-            // ---- the trial's Gw table and the reflections its window bound keeps
-            unsigned live[HPL];
+            // ---- the trial's Gw table (shared, for the landings) and prefilter (registers)
+            float gx[HPL], gy[HPL], gz[HPL], lo[HPL], hi[HPL];
 #pragma unroll
             for (int j = 0; j < HPL; ++j) {
                 const int ih = lane + 32 * j;
-                bool ok = false;
+                gx[j] = gy[j] = gz[j] = 0.f;
+                lo[j] = CUDART_INF_F;
+                hi[j] = -CUDART_INF_F;
                 if (ih < g.nhkl) {
                     const float4 gv = gw_of(sf, sm.hk[ih]);
                     const float4 wv = window_f(g, gv);
                     gwt[ih] = gv;
                     wnt[ih] = wv;
-                    const float Gn = (gv.x * gv.x + gv.y * gv.y + gv.z * gv.z) * gv.w;
-                    const float tc = -fmaf(kc.x, gv.x, fmaf(kc.y, gv.y, kc.z * gv.z));
-                    const float rg = kc.w * Gn;
-                    ok = (tc - rg < wv.y) && (tc + rg > wv.x);
+                    gx[j] = gv.x;
+                    gy[j] = gv.y;
+                    gz[j] = gv.z;
+                    lo[j] = wv.x;
+                    hi[j] = wv.y;
                 }
-                live[j] = __ballot_sync(kAll, ok);
             }
             __syncwarp();
-            float kx = CUDART_NAN_F, ky = CUDART_NAN_F, kz = CUDART_NAN_F;
-            if (lane < nw) {
-                const float4 k4 = reinterpret_cast<const float4 *>(sm.rows + vl * WIN + lane)[3];
-                kx = k4.x;
-                ky = k4.y;
-                kz = k4.z;
-            }
-            const RowF *vr = sm.rows + vl * WIN;
-            int c_simu = 0, c_inter = 0;  // completeness mode: this trial's counts in this window
+            const RowF *vr = sm.rows + sm.vloc[s] * WIN;
+            // completeness mode: this trial's counts in this window, packed as the shared counter
+            uint32_t cnt = 0;
             // a selected pixel is read when its batch is evaluated and counted after the next batch
-            // has been computed, so the gather's latency overlaps the landing arithmetic
-            bool pend_sel = false;
+            // has been computed, so the gather's latency overlaps the landing arithmetic; pend_bit
+            // is the pixel's bit (completeness) or 0 (full), -1 when the lane has none
+            int pend_bit = -1;
             uint32_t pend_val = 0;
-            int pend_bit = 0;
             auto apply_pending = [&]() {
                 if (MODE == kScanComp) {
-                    const bool hit = pend_sel && ((pend_val >> pend_bit) & 1u);
-                    c_simu += __popc(__ballot_sync(kAll, pend_sel));
-                    c_inter += __popc(__ballot_sync(kAll, hit));
-                } else if (pend_sel) {
+                    const bool sel = pend_bit >= 0;
+                    const bool hit = sel && ((pend_val >> pend_bit) & 1u);
+                    cnt += (uint32_t)__popc(__ballot_sync(kAll, sel)) + ((uint32_t)__popc(__ballot_sync(kAll, hit)) << 16);
+                } else if (pend_bit >= 0) {
                     atomicAdd(&sm.hist[s * kHistWords + (pend_val >> 1)], 1u << ((pend_val & 1u) * 16));
                 }
-                pend_sel = false;
+                pend_bit = -1;
             };
             auto fast = [&](uint32_t item, bool valid) {
                 const int wl = (int)(item >> 8), ih = (int)(item & 255u);
@@ -304,46 +254,39 @@ __global__ void __launch_bounds__(kThreads, GRC_SCAN_BLOCKS)
                 const unsigned m = __ballot_sync(kAll, amb);
                 if (amb) fq[fn + __popc(m & lt)] = ((uint32_t)s << 16) | item;
                 fn += __popc(m);
-                const bool sel = ip >= 0;
                 uint32_t val = 0;
-                if (sel) {
+                if (ip >= 0) {
                     if (MODE == kScanComp)
                         val = __ldg(wbits + (int64_t)wl * pw + (ip >> 5));
                     else
                         val = __ldg(wcodes + (int64_t)wl * g.plane + ip);
                 }
                 apply_pending();
-                pend_sel = sel;
+                pend_bit = ip >= 0 ? (MODE == kScanComp ? (ip & 31) : 0) : -1;
                 pend_val = val;
-                pend_bit = ip & 31;
             };
             int qn = 0;
+            for (int wl = 0; wl < nw; ++wl) {
+                const float4 kwv = reinterpret_cast<const float4 *>(vr + wl)[3];
 #pragma unroll
-            for (int j = 0; j < HPL; ++j) {
-                unsigned m = live[j];
-                while (m) {
-                    const int ih = 32 * j + __ffs(m) - 1;
-                    m &= m - 1;
-                    const float4 gv = gwt[ih];
-                    const float4 wv = wnt[ih];
-                    const float t = -fmaf(kx, gv.x, fmaf(ky, gv.y, kz * gv.z));
-                    const bool pass = (t > wv.x) && (t < wv.y);
+                for (int j = 0; j < HPL; ++j) {
+                    const float t = -fmaf(kwv.x, gx[j], fmaf(kwv.y, gy[j], kwv.z * gz[j]));
+                    const bool pass = (t > lo[j]) && (t < hi[j]);
                     const unsigned bm = __ballot_sync(kAll, pass);
-                    if (pass) wq[qn + __popc(bm & lt)] = ((uint32_t)lane << 8) | (uint32_t)ih;
+                    if (pass) wq[qn + __popc(bm & lt)] = ((uint32_t)wl << 8) | (uint32_t)(lane + 32 * j);
                     qn += __popc(bm);
-                    if (qn >= 32) {
-                        __syncwarp();
-                        qn -= 32;
-                        const uint32_t item = wq[qn + lane];
-                        __syncwarp();
-                        fast(item, true);
-                        __syncwarp();
-                        drain_exact(false);
-                    }
+                }
+                __syncwarp();
+                while (qn >= 32) {
+                    qn -= 32;
+                    const uint32_t item = wq[qn + lane];
+                    __syncwarp();
+                    fast(item, true);
+                    __syncwarp();
+                    drain_exact(false);
                 }
             }
-            __syncwarp();
-            if (qn > 0) {  // the trial's last, partial batch
+            if (qn > 0) {  // the trial's last, partial batch: every batch holds one trial
                 const bool valid = lane < qn;
                 const uint32_t item = valid ? wq[lane] : 0u;
                 __syncwarp();
@@ -352,10 +295,7 @@ __global__ void __launch_bounds__(kThreads, GRC_SCAN_BLOCKS)
                 drain_exact(false);
             }
             apply_pending();
-            if (MODE == kScanComp && lane == 0) {
-                atomicAdd(&sm.cnt[s].x, c_simu);
-                atomicAdd(&sm.cnt[s].y, c_inter);
-            }
+            if (MODE == kScanComp && lane == 0) atomicAdd(&sm.hist[s], cnt);
         }
         drain_exact(true);
         __syncthreads();  // rows are rebuilt for the next window
@@ -365,23 +305,23 @@ __global__ void __launch_bounds__(kThreads, GRC_SCAN_BLOCKS)
     if constexpr (MODE == kScanFull) {
         for (int s = warp; s < nslot; s += kWarps) hist8_finish(g, b, sm.hist + s * kHistWords, cta_base + s);
     } else {
-    for (int base = warp * 32; base < nslot; base += kWarps * 32) {
-        const int s = base + lane;
-        const bool in = s < nslot;
-        const int64_t t = cta_base + s;
-        int simu = 0, inter = 0;
-        if (in) {
-            const int2 c = sm.cnt[s];
-            simu = c.x;
-            inter = c.y;
-            TrialRes r;
-            r.simu = simu;
-            r.inter = inter;
-            r.median = CUDART_NAN;  // not computed in this mode
-            b.res[t] = r;
+        for (int base = warp * 32; base < nslot; base += kWarps * 32) {
+            const int s = base + lane;
+            const bool in = s < nslot;
+            const int64_t t = cta_base + s;
+            int simu = 0, inter = 0;
+            if (in) {
+                const uint32_t c = sm.hist[s];
+                simu = (int)(c & 0xffffu);
+                inter = (int)(c >> 16);
+                TrialRes r;
+                r.simu = simu;
+                r.inter = inter;
+                r.median = CUDART_NAN;  // not computed in this mode
+                b.res[t] = r;
+            }
+            if (b.group_key) fold_group_key(b, in, t, simu, inter);
         }
-        if (b.group_key) fold_group_key(b, in, t, simu, inter);
-    }
     }
 }
 
@@ -510,7 +450,25 @@ __global__ void group_decode_k(const unsigned long long *keys, int64_t n_groups,
     }
 }
 
+// Spot pixels of a packed mask back to bytes: mask[iw*plane + p] = bit p of projection iw.
+__global__ void unpack_bits_k(const uint32_t *bits, int64_t plane, int64_t nrot, int64_t pw, uint8_t *mask) {
+    const int64_t n = nrot * plane;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t iw = i / plane, p = i - iw * plane;
+        mask[i] = (uint8_t)((bits[iw * pw + (p >> 5)] >> (p & 31)) & 1u);
+    }
+}
+
 }  // namespace
+
+cudaError_t launch_unpack_bits(const uint32_t *bits, int64_t plane, int64_t nrot, int64_t plane_words, uint8_t *mask,
+                               cudaStream_t s) {
+    const int64_t n = nrot * plane;
+    if (n <= 0) return cudaSuccess;
+    const int64_t want = (n + 255) / 256;
+    unpack_bits_k<<<(int)(want < 65535 * 8 ? want : 65535 * 8), 256, 0, s>>>(bits, plane, nrot, plane_words, mask);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_group_argmax(const TrialRes *res, int64_t n_trials, int64_t gsize, unsigned long long *keys,
                                 cudaStream_t s) {

@@ -66,6 +66,29 @@ int grc_upload_masks_device(grc_ctx *ctx, const float *d_proj_bin_bw, int64_t de
                             int64_t nrot);
 
 /*
+ * Spot masks instead of a distance map: proj_bin holds one byte per pixel (nonzero = spot pixel),
+ * detzsize*detysize*nrot bytes in the layout of proj_bin_bw, host or device memory.  The distance
+ * map is computed on the device (exact Euclidean distance transform, bwdist semantics: 0 on
+ * spot pixels, +Inf for a projection without any) and made resident as by grc_upload_masks.
+ * Replaces the host bwdist of GrainMapping_fun.m:73-75 and the per-call upload of the float map.
+ */
+int grc_upload_spot_masks(grc_ctx *ctx, const uint8_t *proj_bin, int64_t detzsize, int64_t detysize, int64_t nrot);
+
+/*
+ * Packed spot-mask files.  grc_save_packed_masks writes the spot pixels (distance 0) of the
+ * resident map: an 80-byte header -- magic "GRCMASK1", version 1 (uint32), header size (uint32),
+ * detzsize, detysize, nrot, plane_words (int64), the FNV-1a key of the words (uint64), 24
+ * reserved bytes -- then nrot * plane_words 32-bit words, plane_words = ceil(detzsize*detysize/128)*4,
+ * pixel p = (dety-1)*detzsize + (detz-1) of a projection at bit p&31 of its word p>>5 (little
+ * endian).  1 bit per pixel: 189 MB for 361 projections of 2048^2.  grc_load_packed_masks checks
+ * the header and the key (GRC_EINVAL for a truncated, altered or foreign file) and makes the map
+ * resident through the device EDT.  (No counterpart in the reference, which keeps the masks in
+ * MATLAB .mat files and recomputes bwdist per run.)
+ */
+int grc_save_packed_masks(grc_ctx *ctx, const char *path);
+int grc_load_packed_masks(grc_ctx *ctx, const char *path);
+
+/*
  * Content key of a distance map, for a caller that keeps one map resident across calls: a 64-bit
  * FNV-1a hash of n and of `samples` values spread evenly over the array, first and last
  * included (every value when samples <= 0 or samples >= n); never 0.  MATLAB frees each call's
@@ -466,13 +489,13 @@ int grc_last_stats(grc_ctx *ctx, grc_stats *out);
 /* 1 = record CUDA events around the scoring kernel of each call (for benchmarks). */
 int grc_set_timing(grc_ctx *ctx, int enable);
 /*
- * Scoring kernel selection: 0 = by size (default: the projection-window sweep, which keeps the
- * map windows L2-resident, once a call holds 1/16 of a round of trials -- 1,776 on 148 SMs --
- * when each voxel carries at least 64 orientations, or half a round otherwise; the per-trial
- * kernel below that), 1 = always the per-trial kernel, 2 = always the sweep, 3 = always the warp
- * scan (the same windows with one trial per warp at a time; slower on the benchmark
- * geometries).  Results are identical; only speed differs.  Batches (grc_batch_*) read the same
- * codes for their tile choice.
+ * Scoring kernel selection: 0 = by size (default: the projection-window warp scan, which keeps
+ * the map windows L2-resident and runs one trial per warp at a time, once a call holds 1/16 of a
+ * round of trials -- 1,776 on 148 SMs -- when each voxel carries at least 64 orientations, or
+ * half a round otherwise; the per-trial kernel below that), 1 = always the per-trial kernel,
+ * 2 = always the CTA sweep (the same windows with the trials of a CTA mixed in its batches),
+ * 3 = always the warp scan.  Results are identical; only speed differs.  Batches (grc_batch_*)
+ * read the same codes for their tile choice.
  */
 int grc_set_path(grc_ctx *ctx, int path);
 

@@ -22,7 +22,8 @@ _NEIGB = np.array([[1, 1, 0], [1, -1, 0], [1, 0, 1], [1, 0, -1], [1, 0, 0], [0, 
                    [-1, 0, -1], [-1, 0, 0]], np.int64)  # grow_indexed_region.m:50-52, 18 neighbours
 
 
-def best_first_growth(score, I, Imask, DisMedian, Ninter, pos_indices, drop_off, maxD, indexed_comp, maxDmedian):
+def best_first_growth(score, I, Imask, DisMedian, Ninter, pos_indices, drop_off, maxD, indexed_comp, maxDmedian,
+                      stop_after=None):
     """The region walk of grow_indexed_region.m:6-137 with a pluggable scorer.
 
     ``score(vox)`` maps (k x 3) 1-based voxel indices to rows [Nr_simu, Nr_intersect, dis_median].
@@ -80,6 +81,8 @@ def best_first_growth(score, I, Imask, DisMedian, Ninter, pos_indices, drop_off,
         dist = neg[:n, 3] / seed_comp
         index = int(np.nanargmax(dist))
         reg_size += 1
+        if stop_after is not None and reg_size > stop_after:
+            break  # a bounded sample of the walk (timing only): stop after stop_after grown voxels
         if dist[index] > 1 - drop_off and reg_size < n_mask - 1:
             e = neg[index].copy()
             csum += e[3]

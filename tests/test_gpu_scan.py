@@ -96,13 +96,13 @@ def test_argmax_per_voxel(scene, median, path):
 
 @pytest.mark.parametrize("median,path", [(False, 2), (True, 2), (False, 3), (True, 3), (False, 1)])
 def test_argmax_per_group_of_trials(scene, median, path):
-    """Local-refine shape: groups of 730 consecutive trials of one voxel (one candidate grid each)."""
+    """Local-refine shape: groups of 729 consecutive trials of one voxel (one candidate grid each)."""
     import torch
     s, dmap, ctx = scene
     idx = s.voxel_indices()
     vox = idx[[5, 400]]
     pos = torch.from_numpy(s.vol.pos_of_index(vox).reshape(-1).astype(np.float64)).cuda()
-    gsize, n_groups = 730, 12
+    gsize, n_groups = 729, 12  # unique(q,'rows') keeps 729 or 730 rows of a 9^3 grid + centre
     cand = np.concatenate([s.grain_q[:4], G.cubic_fz_orientations(n_groups - 4, 21)])
     grids = np.concatenate([G.ori_local_sampling(c, 8, 0.004)[:gsize] for c in cand])
     assert grids.shape == (gsize * n_groups, 4)
