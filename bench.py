@@ -217,6 +217,7 @@ def run_ours(args):
     ctx.set_geometry(S9, B9, hkl, rot, R9, p)
     comp = args.output == "completeness"
     ctx.set_median(not comp)
+    ctx.set_path(args.path)
     S = args.seeds
     K, W = args.steps, args.warmup
     need = (K + W) * S * world
@@ -816,6 +817,8 @@ def main():
     ap.add_argument("--seeds", type=int, default=64, help="seed voxels per step per GPU")
     ap.add_argument("--output", default="completeness", choices=["completeness", "full"],
                     help="seeding-scan output: completeness only (bit-packed mask) or the four MEX columns")
+    ap.add_argument("--path", type=int, default=0, choices=[0, 1, 2, 3],
+                    help="scoring kernel (grc_set_path): 0 by size, 1 per-trial, 2 CTA sweep, 3 warp scan")
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--cpu-trials", type=int, default=8192)

@@ -366,7 +366,16 @@ int run_score(grc_ctx *ctx, const grc::Work &w, int64_t n_trials, bool comp = fa
             fused_key = true;
         }
         const int mode = comp ? grc::kScanComp : grc::kScanFull;
-        if (ctx->force_path == 2) {
+        // Full output over more than two scan rounds goes to the CTA sweep: its CTAs walk each
+        // projection window in step and share the gathered 8-bit codes in L2 (FCC Al 2048^2 x 361,
+        // 64 seeds x 32,768 orientations per call: 16.1 M trials/s against 13.5 M on the warp
+        // scan).  Completeness-only calls and calls of one or two rounds take the warp scan (one
+        // seed, full output: 15.9 against 15.3 M trials/s end to end; 64 seeds, completeness
+        // only: 19.7 against 17.4 M).
+        const bool sweep = ctx->force_path == 2 ||
+                           (ctx->force_path == 0 && !comp &&
+                            n_trials > 2 * grc::scan_round_trials(ctx->geo, ctx->num_sms));
+        if (sweep) {
             e = grc::launch_sweep(ctx->geo, b, w, n_trials, ctx->num_sms, ctx->stream, e0, e1, &launches, 0, mode);
             ctx->stats.path = 2;
         } else {
@@ -1575,7 +1584,8 @@ constexpr size_t kNaCounters = (sizeof(grc::Geo) + 255) & ~size_t(255);       //
 constexpr size_t kNaPos = kNaCounters + 256;                                   // 3 doubles
 constexpr size_t kNaU = kNaPos + 256;                                          // 9 doubles / orientation
 constexpr size_t kNaRes = kNaU + sizeof(double) * 9 * kNoAllocMaxQ;            // TrialRes / orientation
-constexpr size_t kNaBytes = kNaRes + sizeof(grc::TrialRes) * kNoAllocMaxQ;
+constexpr size_t kNaList = kNaRes + sizeof(grc::TrialRes) * kNoAllocMaxQ;      // refine list / orientation
+constexpr size_t kNaBytes = kNaList + sizeof(int64_t) * kNoAllocMaxQ;
 
 // Every GPU that loads this library holds this array until the process exits.
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNaBytes];
@@ -1637,20 +1647,27 @@ extern "C" int grc_forward_comp_noalloc(grc_ctx *ctx, const float *pos, const fl
     b.codes8 = ctx->mc.codes8;
     b.vals = ctx->mc.vals;
     b.res = (grc::TrialRes *)(base + kNaRes);
-    b.work_counter = (int *)(base + kNaCounters);  // zeroed by launch_score before its kernels
+    b.refine_list = (int64_t *)(base + kNaList);
+    b.work_counter = (int *)(base + kNaCounters);  // zeroed by the launchers before their kernels
     grc::Work w{};
     w.n_or = n_q;
     w.chunk = kSeedChunk;
     w.chunks_per_voxel = (n_q + kSeedChunk - 1) / kSeedChunk;
     w.n_items = w.chunks_per_voxel;
     int launches = 0;
-    cudaError_t e = grc::launch_score(ctx->geo, b, w, ctx->num_sms, ctx->stream, nullptr, nullptr, &launches);
+    // the kernel the regular entry takes for one voxel: the warp scan from 1/16 of a round (with
+    // at least 64 orientations), the per-trial kernel below; both write only the scratch above
+    const int64_t round = ctx->force_path == 1 ? 0 : grc::sweep_round_trials(ctx->geo, ctx->num_sms);
+    const bool scan = round > 0 && n_q >= 64 && (ctx->force_path >= 2 || n_q >= (round + 15) / 16);
+    cudaError_t e = scan ? grc::launch_scan(ctx->geo, b, w, n_q, ctx->num_sms, grc::kScanFull, ctx->stream, nullptr,
+                                            nullptr, &launches)
+                         : grc::launch_score(ctx->geo, b, w, ctx->num_sms, ctx->stream, nullptr, nullptr, &launches);
     if (e != cudaSuccess) return fail(ctx, GRC_ECUDA, "noalloc scorer launch: %s", cudaGetErrorString(e));
     CU(grc::launch_epi_forward(b.res, n_q, d_out, true, ctx->stream));
     CU(cudaStreamSynchronize(ctx->stream));
     ctx->stats.trials = n_q;
     ctx->stats.kernel_launches = launches + 2;
-    ctx->stats.path = 1;
+    ctx->stats.path = scan ? 3 : 1;
     return GRC_OK;
 }
 

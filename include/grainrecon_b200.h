@@ -376,7 +376,7 @@ int grc_pair_spots(grc_ctx *ctx, const double *d_pos, const double *d_q, int64_t
  * caller-owned device buffers.  Geometry and distance map must already be resident
  * (set up earlier with grc_set_geometry / grc_upload_masks).
  *
- * Its scratch is one fixed device array of about 5.8 MB, compiled into the library and
+ * Its scratch is one fixed device array of about 6.3 MB, compiled into the library and
  * held by every GPU that loads it until the process exits; n_q above
  * GRC_NOALLOC_MAX_ORIENTATIONS is rejected with GRC_ECAPACITY.  The first call on a
  * device looks up that array's device address (cudaGetSymbolAddress), so make that
@@ -492,7 +492,8 @@ int grc_set_timing(grc_ctx *ctx, int enable);
  * Scoring kernel selection: 0 = by size (default: the projection-window warp scan, which keeps
  * the map windows L2-resident and runs one trial per warp at a time, once a call holds 1/16 of a
  * round of trials -- 1,776 on 148 SMs -- when each voxel carries at least 64 orientations, or
- * half a round otherwise; the per-trial kernel below that), 1 = always the per-trial kernel,
+ * half a round otherwise; the CTA sweep for full-output calls of more than two rounds; the
+ * per-trial kernel below that), 1 = always the per-trial kernel,
  * 2 = always the CTA sweep (the same windows with the trials of a CTA mixed in its batches),
  * 3 = always the warp scan.  Results are identical; only speed differs.  Batches (grc_batch_*)
  * read the same codes for their tile choice.

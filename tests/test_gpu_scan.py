@@ -217,3 +217,35 @@ def test_keyed_upload_follows_content(scene):
         np.testing.assert_array_equal(ctx.forward_comp(pos, q, S9, B9, hkl, None, rot, R9, p), ref)
     finally:
         ctx.upload_masks(dmap, *dims)
+
+
+def test_size_rule_picks_kernel_by_output_mode(scene):
+    """grc_set_path(ctx, 0): full-output calls of more than two warp-scan rounds take the CTA sweep,
+    shorter ones and every completeness-only call the warp scan; the output does not depend on it."""
+    import torch
+    s, dmap, ctx = scene
+    idx = s.voxel_indices()
+    q = G.cubic_fz_orientations(30000, 13).astype(np.float32)
+    d_q = torch.from_numpy(q.reshape(-1)).cuda()
+    n_sm = torch.cuda.get_device_properties(0).multi_processor_count
+    rnd = n_sm * 3 * 64  # trials of one warp-scan round at 3 CTAs per SM
+    cases = ((1, True, 3), (3, True, 2 if 3 * len(q) > 2 * rnd else 3), (3, False, 3))
+    try:
+        for n_vox, median, path in cases:
+            pos = torch.from_numpy(s.vol.pos_of_index(idx[[9, 200, 333][:n_vox]]).astype(np.float32).reshape(-1)).cuda()
+            out = torch.empty(n_vox * len(q) * 4, dtype=torch.float32, device="cuda")
+            ctx.set_median(median)
+            ctx.set_path(0)
+            ctx.forward_comp_device(pos, n_vox, d_q, len(q), out)
+            torch.cuda.synchronize()
+            assert ctx.last_stats()["path"] == path
+            ref = torch.empty_like(out)
+            ctx.set_path(3 if path == 2 else 2)
+            ctx.forward_comp_device(pos, n_vox, d_q, len(q), ref)
+            torch.cuda.synchronize()
+            assert torch.equal(out.view(-1, 4)[:, :3], ref.view(-1, 4)[:, :3])
+            if median:
+                assert torch.equal(out.view(-1, 4)[:, 3], ref.view(-1, 4)[:, 3])
+    finally:
+        ctx.set_median(True)
+        ctx.set_path(0)
