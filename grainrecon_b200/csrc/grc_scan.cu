@@ -152,6 +152,7 @@ __global__ void __launch_bounds__(kThreads, GRC_SCAN_BLOCKS)
     __syncthreads();
     const int nv = s_nv;
     const int64_t pw = b.plane_words;
+    const uint32_t pw32 = (uint32_t)pw;
 
     for (int w0 = 0; w0 < g.nrot; w0 += WIN) {
         const int nw = min(WIN, g.nrot - w0);
@@ -225,7 +226,9 @@ __global__ void __launch_bounds__(kThreads, GRC_SCAN_BLOCKS)
             }
             __syncwarp();
             const RowF *vr = sm.rows + sm.vloc[s] * WIN;
-            // completeness mode: this trial's counts in this window, packed as the shared counter
+            // completeness mode: the lane's share of this trial's counts in this window, packed as
+            // the shared counter (Nr_simu low, Nr_intersect high 16 bits) and summed over the warp
+            // once per trial and window
             uint32_t cnt = 0;
             // a selected pixel is read when its batch is evaluated and counted after the next batch
             // has been computed, so the gather's latency overlaps the landing arithmetic; pend_bit
@@ -236,7 +239,7 @@ __global__ void __launch_bounds__(kThreads, GRC_SCAN_BLOCKS)
                 if (MODE == kScanComp) {
                     const bool sel = pend_bit >= 0;
                     const bool hit = sel && ((pend_val >> pend_bit) & 1u);
-                    cnt += (uint32_t)__popc(__ballot_sync(kAll, sel)) + ((uint32_t)__popc(__ballot_sync(kAll, hit)) << 16);
+                    cnt += (uint32_t)sel + ((uint32_t)hit << 16);
                 } else if (pend_bit >= 0) {
                     atomicAdd(&sm.hist[s * kHistWords + (pend_val >> 1)], 1u << ((pend_val & 1u) * 16));
                 }
@@ -250,16 +253,19 @@ __global__ void __launch_bounds__(kThreads, GRC_SCAN_BLOCKS)
                     const float4 wv = wnt[ih];
                     ip = landing_fp32(g, vr[wl], gv, wv.z, wv.w);
                 }
-                const bool amb = ip == -2;
-                const unsigned m = __ballot_sync(kAll, amb);
-                if (amb) fq[fn + __popc(m & lt)] = ((uint32_t)s << 16) | item;
-                fn += __popc(m);
+                const unsigned m = __ballot_sync(kAll, ip == -2);
+                if (m) {  // ambiguous items (rare) join the FP64 queue
+                    if (ip == -2) fq[fn + __popc(m & lt)] = ((uint32_t)s << 16) | item;
+                    fn += __popc(m);
+                }
                 uint32_t val = 0;
                 if (ip >= 0) {
+                    // offsets within the window fit 32 bits: WIN * plane < 2^31 for the codes
+                    // (launch_scan_t) and 8 * plane < 2^31 for the words (scan_round_trials)
                     if (MODE == kScanComp)
-                        val = __ldg(wbits + (int64_t)wl * pw + (ip >> 5));
+                        val = __ldg(wbits + ((uint32_t)wl * pw32 + ((uint32_t)ip >> 5)));
                     else
-                        val = __ldg(wcodes + (int64_t)wl * g.plane + ip);
+                        val = __ldg(wcodes + ((uint32_t)wl * (uint32_t)g.plane + (uint32_t)ip));
                 }
                 apply_pending();
                 pend_bit = ip >= 0 ? (MODE == kScanComp ? (ip & 31) : 0) : -1;
@@ -295,7 +301,11 @@ __global__ void __launch_bounds__(kThreads, GRC_SCAN_BLOCKS)
                 drain_exact(false);
             }
             apply_pending();
-            if (MODE == kScanComp && lane == 0) atomicAdd(&sm.hist[s], cnt);
+            if (MODE == kScanComp) {
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(kAll, cnt, o);
+                if (lane == 0) atomicAdd(&sm.hist[s], cnt);
+            }
         }
         drain_exact(true);
         __syncthreads();  // rows are rebuilt for the next window
