@@ -44,6 +44,8 @@ struct grc_ctx {
     std::vector<float> h_vals;
     DevBuf fgeo, fne, ftrial, fcost0, fcost1, fimp, fhw, geo_dev, rot_cs, hkl, pos, U, res, tvoxel, rlist, in1, in2, in3, out, items, torient, counts, offsets, tmp, counter, p1, bad, nm, sp_keys, sp_ids, sp_keys2, sp_ids2, cell_cnt, cell_off, pr_raw, pr_keys, pr_keys2, pr_ids, pr_ids2, pcount;
     grc::Geo *geo_pinned = nullptr;  // staging of the per-launch geometry copy
+    grc::Geo geo_up{};               // the geometry geo_dev holds (valid when geo_up_ok)
+    bool geo_up_ok = false;
     int *nm_active = nullptr;        // pinned: seeds still running in the orientation fit
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     bool timing = false;
@@ -328,9 +330,14 @@ grc::ScoreBufs bufs(grc_ctx *ctx) {
 
 int stage_geo(grc_ctx *ctx) {
     TRY(ensure(ctx, ctx->geo_dev, sizeof(grc::Geo)));
+    // unchanged since the last upload (byte for byte): the device copy is current, and the
+    // kernels of this call are ordered after that upload on the same stream
+    if (ctx->geo_up_ok && std::memcmp(&ctx->geo_up, &ctx->geo, sizeof(grc::Geo)) == 0) return GRC_OK;
     CU(cudaStreamSynchronize(ctx->stream));  // the pinned staging copy may still be read by an earlier call
     *ctx->geo_pinned = ctx->geo;
     CU(cudaMemcpyAsync(ctx->geo_dev.p, ctx->geo_pinned, sizeof(grc::Geo), cudaMemcpyHostToDevice, ctx->stream));
+    std::memcpy(&ctx->geo_up, &ctx->geo, sizeof(grc::Geo));
+    ctx->geo_up_ok = true;
     return GRC_OK;
 }
 
