@@ -448,6 +448,24 @@ def run_grow(args):
     ev1.record(stream)
     ctx.sync()
     chunked_ms = ev0.elapsed_time(ev1) / args.steps
+    # the same chunks through the MEX-shaped host entry (cuda_forward_comp_compete): host rows, the
+    # full neighbour and Euler arrays and the geometry every call, host output; the resident map
+    # stands for the shim's content-keyed upload.  Wall clock, copies included.
+    S9, B9, hkl, rot, R9, p = s.mex_arrays()
+    rows5_h = np.ascontiguousarray(rows5, np.float32)
+    ids_h = np.ascontiguousarray(ids, np.float32)
+    eul_h = np.ascontiguousarray(eul, np.float32).reshape(-1)
+    out_h = np.empty(8 * m, np.float32)
+    p1_14 = s.vol.param14(0, 0, 0)
+    for c0 in range(0, min(m, chunk), chunk):
+        ctx.forward_comp_compete(rows5_h[c0:c0 + chunk], ids_h, eul_h, S9, B9, hkl, None, rot, R9, p, p1_14,
+                                 out=out_h[8 * c0:8 * (c0 + chunk)])
+    t0 = time.perf_counter()
+    for c0 in range(0, m, chunk):
+        c1 = min(m, c0 + chunk)
+        ctx.forward_comp_compete(rows5_h[c0:c1], ids_h, eul_h, S9, B9, hkl, None, rot, R9, p, p1_14,
+                                 out=out_h[8 * c0:8 * c1])
+    host_chunked_ms = (time.perf_counter() - t0) * 1e3
     # one scorer call per voxel (the launch-bound extreme)
     nb = min(args.plain_voxels, m)
     one = torch.empty(8, dtype=torch.float32, device="cuda")
@@ -475,6 +493,9 @@ def run_grow(args):
                                  "note": (f"one grc_compete_device call per {chunk} voxels "
                                           "(revise_all_unindexed_voxel_cuda.m:77), CSR planned per call")},
             "speedup_vs_reference_chunks": chunked_ms / graph_ms,
+            "reference_chunks_host": {"trials_per_s": T / (host_chunked_ms / 1e3), "ms_per_iteration": host_chunked_ms,
+                                      "note": (f"one grc_forward_comp_compete call per {chunk} voxels with host "
+                                               "buffers (the MEX entry), wall clock, one iteration")},
             "plain_per_voxel": {"trials_per_s": plain, "voxels_sampled": nb,
                                 "note": "one grc_compete_device call (one scoring launch set) per voxel"},
             "speedup_vs_plain": batched / plain, "autotune": tune}
