@@ -10,6 +10,7 @@
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <new>
 #include <vector>
 
 #include "grainrecon_b200.h"
@@ -1278,13 +1279,31 @@ int grc_load_packed_masks(grc_ctx *ctx, const char *path) {
         std::fclose(f);
         return fail(ctx, GRC_EINVAL, "load: %s is not a packed-mask file (version 1)", path);
     }
+    // the same limits as a map given to grc_upload_masks (set_geometry: 10^6 pixels per side,
+    // 2^31 - 1 per projection), checked before anything is allocated
     if (hd.detzsize < 1 || hd.detysize < 1 || hd.nrot < 1 || hd.detzsize > 1000000 || hd.detysize > 1000000 ||
-        hd.nrot > GRC_MAX_NROT || hd.plane_words != (hd.detzsize * hd.detysize + 127) / 128 * 4) {
+        hd.detzsize * hd.detysize > 2147483647LL || hd.nrot > GRC_MAX_NROT ||
+        hd.plane_words != (hd.detzsize * hd.detysize + 127) / 128 * 4) {
         std::fclose(f);
         return fail(ctx, GRC_EINVAL, "load: %s has an inconsistent header", path);
     }
     const int64_t nw = hd.plane_words * hd.nrot, plane = hd.detzsize * hd.detysize;
-    std::vector<uint32_t> h((size_t)nw);
+    // the file must hold exactly the header and the words it announces
+    const long here = std::ftell(f);
+    const bool sized = here >= 0 && std::fseek(f, 0, SEEK_END) == 0 &&
+                       (int64_t)std::ftell(f) == (int64_t)sizeof(PackedHeader) + 4 * nw &&
+                       std::fseek(f, here, SEEK_SET) == 0;
+    if (!sized) {
+        std::fclose(f);
+        return fail(ctx, GRC_EINVAL, "load: %s is truncated or longer than its header says", path);
+    }
+    std::vector<uint32_t> h;
+    try {
+        h.resize((size_t)nw);
+    } catch (const std::bad_alloc &) {
+        std::fclose(f);
+        return fail(ctx, GRC_ECAPACITY, "load: %lld words do not fit in host memory", (long long)nw);
+    }
     const bool full = std::fread(h.data(), sizeof(uint32_t), (size_t)nw, f) == (size_t)nw;
     std::fclose(f);
     if (!full) return fail(ctx, GRC_EINVAL, "load: %s is truncated", path);

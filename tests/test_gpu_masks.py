@@ -4,7 +4,8 @@
   bwdist map uploaded with grc_upload_masks;
 * grc_save_packed_masks writes the documented layout (checked here by decoding the file with
   numpy alone), and grc_load_packed_masks restores a context that scores identically;
-* a truncated, altered or foreign file is refused with GRC_EINVAL."""
+* a truncated, lengthened, altered or foreign file, or a header announcing more pixels per
+  projection than a map may hold, is refused with GRC_EINVAL before anything is allocated."""
 import numpy as np
 import pytest
 
@@ -63,7 +64,10 @@ def test_packed_mask_file_round_trip(sample, tmp_path):
     with Context(0) as b:
         b.load_packed_masks(path)
         np.testing.assert_array_equal(_scan(b, s), ref)
-        for bad in (raw[:-4], raw[:100] + bytes([raw[100] ^ 1]) + raw[101:], b"NOTAMASK" + raw[8:]):
+        big = bytearray(raw[:80])  # a consistent header announcing 10^6 x 10^6 pixels per projection
+        big[16:48] = np.array([10**6, 10**6, g.nrot, (10**12 + 127) // 128 * 4], "<i8").tobytes()
+        for bad in (raw[:-4], raw + b"\0\0\0\0", raw[:100] + bytes([raw[100] ^ 1]) + raw[101:],
+                    b"NOTAMASK" + raw[8:], bytes(big) + raw[80:]):
             p2 = str(tmp_path / "bad.grcmask")
             open(p2, "wb").write(bad)
             with pytest.raises(GrcError) as e:
