@@ -83,8 +83,8 @@ int grc_upload_spot_masks(grc_ctx *ctx, const uint8_t *proj_bin, int64_t detzsiz
  * endian).  1 bit per pixel: 189 MB for 361 projections of 2048^2.  grc_load_packed_masks checks
  * the header, the file length and the key (GRC_EINVAL for a truncated, lengthened, altered or
  * foreign file, or a header beyond the map limits of grc_upload_masks, before anything is
- * allocated) and makes the map resident through the device EDT.  (No counterpart in the reference, which keeps the masks in
- * MATLAB .mat files and recomputes bwdist per run.)
+ * allocated) and makes the map resident through the device EDT.  (No counterpart in the
+ * reference, which keeps the masks in MATLAB .mat files and recomputes bwdist per run.)
  */
 int grc_save_packed_masks(grc_ctx *ctx, const char *path);
 int grc_load_packed_masks(grc_ctx *ctx, const char *path);
