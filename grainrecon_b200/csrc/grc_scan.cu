@@ -13,6 +13,8 @@
 //     of the warp (completeness-only mode: one bit of the packed hit mask per pixel) or in the
 //     trial's 8-bit code histogram (full mode: Nr_simu, Nr_intersect and the exact median).
 // Ambiguous items keep their trial in the FP64 queue, which is drained at the end of the window.
+// Windows: up to 32 projections of 8-bit codes (full mode), up to 128 of the bit mask
+// (completeness mode), each within the limits of shared memory and L2 (launch_scan_t).
 // The decisions are those of the sweep and of the oracle: same prefilter margins, same FP32
 // chain and band, same FP64 path.
 #include <cuda_runtime.h>
@@ -372,14 +374,37 @@ cudaError_t launch_scan_t(const Geo &g, const ScoreBufs &b, const Work &w, int64
     int slots = (int)((n_trials + rounds * grid - 1) / (rounds * grid));
     if (slots < 1) slots = 1;
     const int rows_cap = rows_for(slots);
-    // the widest projection window (32 or 16, else 8) whose rows keep the grid's CTAs per SM
+    // the widest projection window whose rows keep the grid's CTAs per SM: up to 128 projections
+    // for the bit mask (one-seed Al rounds 1.641 / 1.567 / 1.573 ms at 32 / 64 / 128, 64-seed calls
+    // 103.9 / 98.7 / 97.1 ms), 32 or 16 for the 8-bit codes (32 projections of 2048^2 codes are
+    // already about the size of L2), else 8
     ScanFn kern = k8;
     size_t smem = scan_smem_layout(MODE, g.nhkl, rows_cap, slots, kScanWinMin, offs);
     bool refused = false;
-    const int cands[2] = {32, 16};
-    for (int cand : cands) {
+    auto window_kernel = [](int cand) -> ScanFn {
+        if constexpr (MODE == kScanComp) {
+            if (cand == 128) return scan_kernel<MODE, HPL, 128>;
+            if (cand == 64) return scan_kernel<MODE, HPL, 64>;
+        }
+        return cand == 32 ? (ScanFn)scan_kernel<MODE, HPL, 32> : (ScanFn)scan_kernel<MODE, HPL, 16>;
+    };
+    constexpr int kCands = MODE == kScanComp ? 4 : 2;
+    const int cands_comp[4] = {128, 64, 32, 16}, cands_full[2] = {32, 16};
+    const int *cands = MODE == kScanComp ? cands_comp : cands_full;
+    // the bit-mask window stays within 3/4 of L2 (Al 2048^2 on 126 MB: 128 projections = 67 MB,
+    // fastest; 256 = 134 MB ran 30% slower)
+    int64_t l2_budget = 0;
+    if (MODE == kScanComp) {
+        int dev = 0, l2 = 0;
+        if (cudaGetDevice(&dev) == cudaSuccess && cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, dev) == cudaSuccess)
+            l2_budget = (int64_t)l2 * 3 / 4;
+        cudaGetLastError();
+    }
+    for (int ci = 0; ci < kCands; ++ci) {
+        const int cand = cands[ci];
+        if (MODE == kScanComp && cand > 32 && (int64_t)cand * b.plane_words * 4 > l2_budget) continue;
         if (MODE == kScanFull && (int64_t)cand * g.plane > 2147483647LL) continue;
-        const ScanFn kc = cand == 32 ? (ScanFn)scan_kernel<MODE, HPL, 32> : (ScanFn)scan_kernel<MODE, HPL, 16>;
+        const ScanFn kc = window_kernel(cand);
         const size_t smem_c = scan_smem_layout(MODE, g.nhkl, rows_cap, slots, cand, offs);
         int per_c = 0;
         if (cudaFuncSetAttribute(kc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_c) != cudaSuccess ||
