@@ -375,9 +375,9 @@ cudaError_t launch_scan_t(const Geo &g, const ScoreBufs &b, const Work &w, int64
     if (slots < 1) slots = 1;
     const int rows_cap = rows_for(slots);
     // the widest projection window whose rows keep the grid's CTAs per SM: up to 128 projections
-    // for the bit mask (one-seed Al rounds 1.641 / 1.567 / 1.573 ms at 32 / 64 / 128, 64-seed calls
-    // 103.9 / 98.7 / 97.1 ms), 32 or 16 for the 8-bit codes (32 projections of 2048^2 codes are
-    // already about the size of L2), else 8
+    // for the bit mask of a seeding scan (one-seed Al rounds 1.641 / 1.567 / 1.573 ms at 32 / 64 /
+    // 128, 64-seed calls 103.9 / 98.7 / 97.1 ms), 32 or 16 for the 8-bit codes (32 projections of
+    // 2048^2 codes are already about the size of L2; 16 ran 6-8 % slower), else 8
     ScanFn kern = k8;
     size_t smem = scan_smem_layout(MODE, g.nhkl, rows_cap, slots, kScanWinMin, offs);
     bool refused = false;
@@ -388,9 +388,12 @@ cudaError_t launch_scan_t(const Geo &g, const ScoreBufs &b, const Work &w, int64
         }
         return cand == 32 ? (ScanFn)scan_kernel<MODE, HPL, 32> : (ScanFn)scan_kernel<MODE, HPL, 16>;
     };
-    constexpr int kCands = MODE == kScanComp ? 4 : 2;
-    const int cands_comp[4] = {128, 64, 32, 16}, cands_full[2] = {32, 16};
-    const int *cands = MODE == kScanComp ? cands_comp : cands_full;
+    // Explicit trial lists (the seeding refine's grids, grow and compete rows) keep 32: the refine
+    // of 16 Al seeds took 0.234 s with 32-projection windows against 0.246-0.255 s with 128.
+    const bool wide = MODE == kScanComp && !explicit_voxels;
+    const int kCands = wide ? 4 : 2;
+    const int cands_wide[4] = {128, 64, 32, 16}, cands_narrow[2] = {32, 16};
+    const int *cands = wide ? cands_wide : cands_narrow;
     // the bit-mask window stays within 3/4 of L2 (Al 2048^2 on 126 MB: 128 projections = 67 MB,
     // fastest; 256 = 134 MB ran 30% slower)
     int64_t l2_budget = 0;
