@@ -6,6 +6,9 @@
 
 #include "grc_internal.h"
 
+#include <mutex>
+#include <vector>
+
 namespace grc {
 namespace {
 
@@ -290,6 +293,65 @@ __global__ void edt_cols_k(const float *g, int64_t nz, int64_t ny, int64_t nrot,
 }
 
 }  // namespace
+
+namespace {
+struct OccEntry {
+    int device;
+    const void *fn;
+    size_t smem;
+    int per_sm;
+};
+struct SmemEntry {
+    int device;
+    const void *fn;
+    size_t allowed;
+};
+std::mutex g_launch_mu;
+std::vector<OccEntry> g_occ;
+std::vector<SmemEntry> g_smem;
+
+// caller holds g_launch_mu
+cudaError_t allow_smem_locked(int dev, const void *fn, size_t smem) {
+    for (SmemEntry &e : g_smem)
+        if (e.device == dev && e.fn == fn) {
+            if (e.allowed >= smem) return cudaSuccess;
+            const cudaError_t r = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            if (r == cudaSuccess) e.allowed = smem;
+            return r;
+        }
+    const cudaError_t r = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (r == cudaSuccess) g_smem.push_back({dev, fn, smem});
+    return r;
+}
+}  // namespace
+
+cudaError_t allow_smem(const void *fn, size_t smem) {
+    int dev = 0;
+    cudaError_t r = cudaGetDevice(&dev);
+    if (r != cudaSuccess) return r;
+    std::lock_guard<std::mutex> g(g_launch_mu);
+    return allow_smem_locked(dev, fn, smem);
+}
+
+cudaError_t occupancy_for(const void *fn, size_t smem, int *per_sm) {
+    int dev = 0;
+    cudaError_t r = cudaGetDevice(&dev);
+    if (r != cudaSuccess) return r;
+    std::lock_guard<std::mutex> g(g_launch_mu);
+    for (const OccEntry &e : g_occ)
+        if (e.device == dev && e.fn == fn && e.smem == smem) {
+            *per_sm = e.per_sm;
+            return cudaSuccess;
+        }
+    r = allow_smem_locked(dev, fn, smem);
+    if (r != cudaSuccess) return r;
+    int n = 0;
+    r = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, kThreads, smem);
+    if (r != cudaSuccess) return r;
+    g_occ.push_back({dev, fn, smem, n});
+    *per_sm = n;
+    return cudaSuccess;
+}
 
 cudaError_t launch_quat_to_u(const float *q, int64_t n, double *U, cudaStream_t s) {
     quat_to_u_k<<<blocks_for(n), kB, 0, s>>>(q, n, U);

@@ -99,6 +99,13 @@ cudaError_t launch_refine_list(const Geo &g, const ScoreBufs &b, const Work &w, 
 // b.group_size consecutive trials is folded into group_key (group_key_of).
 constexpr int kScanFull = 0, kScanComp = 1;
 int64_t scan_round_trials(const Geo &g, int num_sms);
+
+// Launch-configuration helpers shared by the window kernels' launchers.  occupancy_for: resident
+// CTAs per SM of `fn` with 256 threads and `smem` bytes of dynamic shared memory, cached per
+// (device, kernel, size); allow_smem: raises the kernel's dynamic shared-memory limit to at least
+// `smem` (each only calls the runtime the first time it meets a kernel and size).
+cudaError_t occupancy_for(const void *fn, size_t smem, int *per_sm);
+cudaError_t allow_smem(const void *fn, size_t smem);
 cudaError_t launch_scan(const Geo &g, const ScoreBufs &b, const Work &w, int64_t n_trials, int num_sms, int mode,
                         cudaStream_t s, cudaEvent_t ev0, cudaEvent_t ev1, int *launches, int max_slots = 0);
 // Seeding-stage ordering (grc_select.cu).  top_rows: per group of gsize rows, the indices of the

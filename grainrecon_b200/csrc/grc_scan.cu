@@ -355,19 +355,15 @@ cudaError_t launch_scan_t(const Geo &g, const ScoreBufs &b, const Work &w, int64
     using ScanFn = void (*)(Geo, ScoreBufs, Work, int64_t, int64_t, int, int);
     const ScanFn k8 = scan_kernel<MODE, HPL, kScanWinMin>;
     const size_t smem_max = scan_smem_layout(MODE, g.nhkl, rows_for(max_slots), max_slots, kScanWinMin, offs);
-    cudaError_t e = cudaFuncSetAttribute(k8, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_max);
-    if (e != cudaSuccess) return e;
     int per_sm = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k8, kThreads, smem_max);
+    cudaError_t e = occupancy_for((const void *)k8, smem_max, &per_sm);
     if (e != cudaSuccess) return e;
     if (per_sm < 1) return cudaErrorInvalidConfiguration;
     const int64_t grid = (int64_t)per_sm * num_sms;
     if (!caller_tile && !explicit_voxels && n_trials > grid * max_slots && n_trials <= grid * kScanSlots) {
         int per_sm1 = 0;
         const size_t smem1 = scan_smem_layout(MODE, g.nhkl, rows_for(kScanSlots), kScanSlots, kScanWinMin, offs);
-        if (cudaFuncSetAttribute(k8, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem1) == cudaSuccess &&
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm1, k8, kThreads, smem1) == cudaSuccess &&
-            per_sm1 == per_sm)
+        if (occupancy_for((const void *)k8, smem1, &per_sm1) == cudaSuccess && per_sm1 == per_sm)
             max_slots = kScanSlots;
     }
     const int64_t rounds = (n_trials + grid * max_slots - 1) / (grid * max_slots);
@@ -410,8 +406,7 @@ cudaError_t launch_scan_t(const Geo &g, const ScoreBufs &b, const Work &w, int64
         const ScanFn kc = window_kernel(cand);
         const size_t smem_c = scan_smem_layout(MODE, g.nhkl, rows_cap, slots, cand, offs);
         int per_c = 0;
-        if (cudaFuncSetAttribute(kc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_c) != cudaSuccess ||
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_c, kc, kThreads, smem_c) != cudaSuccess) {
+        if (occupancy_for((const void *)kc, smem_c, &per_c) != cudaSuccess) {
             refused = true;
             continue;
         }
@@ -422,7 +417,7 @@ cudaError_t launch_scan_t(const Geo &g, const ScoreBufs &b, const Work &w, int64
         }
     }
     if (refused) cudaGetLastError();  // a refused window query is not an error of this launch
-    e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    e = allow_smem((const void *)kern, smem);
     if (e != cudaSuccess) return e;
     const int64_t per_round = grid * slots;
     e = cudaMemsetAsync(b.work_counter, 0, 8 * sizeof(int), s);

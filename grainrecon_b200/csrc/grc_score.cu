@@ -827,10 +827,8 @@ __global__ void __launch_bounds__(kThreads, 2) refine_list_kernel(Geo g, ScoreBu
 
 template <typename K>
 cudaError_t prep_launch(K kern, size_t smem, int num_sms, int64_t n_items, int *grid_out) {
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
     int per_sm = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kThreads, smem);
+    const cudaError_t e = occupancy_for((const void *)kern, smem, &per_sm);
     if (e != cudaSuccess) return e;
     if (per_sm < 1) return cudaErrorInvalidConfiguration;
     int64_t grid = (int64_t)per_sm * num_sms;
@@ -888,9 +886,7 @@ cudaError_t launch_sweep_t(const Geo &g, const ScoreBufs &b, const Work &w, int6
     int per_sm = 0;
     using SweepFn = void (*)(Geo, ScoreBufs, Work, int64_t, int64_t, int, int);
     const SweepFn k8 = sweep_kernel<HPL, kWinMin, MODE>;
-    cudaError_t e = cudaFuncSetAttribute(k8, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_max);
-    if (e != cudaSuccess) return e;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k8, kThreads, smem_max);
+    cudaError_t e = occupancy_for((const void *)k8, smem_max, &per_sm);
     if (e != cudaSuccess) return e;
     if (per_sm < 1) return cudaErrorInvalidConfiguration;
     int grid_r = 0;
@@ -901,9 +897,7 @@ cudaError_t launch_sweep_t(const Geo &g, const ScoreBufs &b, const Work &w, int6
         // one round of up to kSlots trials per CTA, if the larger tile keeps the same CTAs per SM
         int per_sm1 = 0;
         const size_t smem1 = sweep_smem_layout(g.nhkl, rows_for(kSlots), kSlots, kWinMin, offs, MODE);
-        if (cudaFuncSetAttribute(k8, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem1) == cudaSuccess &&
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm1, k8, kThreads, smem1) == cudaSuccess &&
-            per_sm1 == per_sm) {
+        if (occupancy_for((const void *)k8, smem1, &per_sm1) == cudaSuccess && per_sm1 == per_sm) {
             max_slots = kSlots;
         }
     }
@@ -922,8 +916,7 @@ cudaError_t launch_sweep_t(const Geo &g, const ScoreBufs &b, const Work &w, int6
         const SweepFn kc = cand == 32 ? (SweepFn)sweep_kernel<HPL, 32, MODE> : (SweepFn)sweep_kernel<HPL, 16, MODE>;
         const size_t smem_c = sweep_smem_layout(g.nhkl, rows_cap, slots, cand, offs, MODE);
         int per_c = 0;
-        if (cudaFuncSetAttribute(kc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_c) != cudaSuccess ||
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_c, kc, kThreads, smem_c) != cudaSuccess) {
+        if (occupancy_for((const void *)kc, smem_c, &per_c) != cudaSuccess) {
             refused = true;  // more shared memory than a CTA may have: not this window
             continue;
         }
@@ -934,7 +927,7 @@ cudaError_t launch_sweep_t(const Geo &g, const ScoreBufs &b, const Work &w, int6
         }
     }
     if (refused) cudaGetLastError();  // the refused query is not an error of this launch
-    e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    e = allow_smem((const void *)kern, smem);
     if (e != cudaSuccess) return e;
     const int64_t per_round = grid * slots;
     e = cudaMemsetAsync(b.work_counter, 0, 8 * sizeof(int), s);
