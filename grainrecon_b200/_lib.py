@@ -56,7 +56,7 @@ class GrcError(RuntimeError):
 class Stats(C.Structure):
     _fields_ = [("trials", C.c_int64), ("refined", C.c_int64), ("kernel_launches", C.c_int64),
                 ("score_ms", C.c_double), ("path", C.c_int64), ("audit_checked", C.c_int64),
-                ("audit_mismatch", C.c_int64)]
+                ("audit_mismatch", C.c_int64), ("device_loop", C.c_int64)]
 
 
 _lib = None
@@ -485,7 +485,7 @@ class Context:
         self._check(self.L.grc_last_stats(self.h, C.byref(s)))
         return {"trials": s.trials, "refined": s.refined, "kernel_launches": s.kernel_launches,
                 "score_ms": s.score_ms, "path": s.path, "audit_checked": s.audit_checked,
-                "audit_mismatch": s.audit_mismatch}
+                "audit_mismatch": s.audit_mismatch, "device_loop": s.device_loop}
 
     def mask_info(self) -> dict:
         nd, nz, ny, nr = C.c_int64(), C.c_int64(), C.c_int64(), C.c_int64()

@@ -43,7 +43,7 @@ struct grc_ctx {
     grc::MapCodes mc{};
     int64_t mz = 0, my = 0, mrot = 0;
     std::vector<float> h_vals;
-    DevBuf fgeo, fne, ftrial, fcost0, fcost1, fimp, fhw, geo_dev, rot_cs, hkl, pos, U, res, tvoxel, rlist, in1, in2, in3, out, items, torient, counts, offsets, tmp, counter, p1, bad, nm, sp_keys, sp_ids, sp_keys2, sp_ids2, cell_cnt, cell_off, pr_raw, pr_keys, pr_keys2, pr_ids, pr_ids2, pcount;
+    DevBuf fgeo, fne, ftrial, fcost0, fcost1, fimp, fhw, geo_dev, rot_cs, hkl, pos, U, res, tvoxel, rlist, in1, in2, in3, out, items, torient, counts, offsets, tmp, counter, p1, bad, nm, sp_keys, sp_ids, sp_keys2, sp_ids2, cell_cnt, cell_off, pr_raw, pr_keys, pr_keys2, pr_ids, pr_ids2, pcount, nmloop;
     grc::Geo *geo_pinned = nullptr;  // staging of the per-launch geometry copy
     grc::Geo geo_up{};               // the geometry geo_dev holds (valid when geo_up_ok)
     bool geo_up_ok = false;
@@ -613,7 +613,7 @@ int grc_ctx_destroy(grc_ctx *ctx) {
                          &ctx->tvoxel, &ctx->rlist, &ctx->geo_dev, &ctx->rot_cs, &ctx->hkl, &ctx->pos, &ctx->U, &ctx->res, &ctx->in1, &ctx->in2,
                          &ctx->in3, &ctx->out, &ctx->items, &ctx->torient, &ctx->counts, &ctx->offsets,
                          &ctx->tmp, &ctx->counter, &ctx->p1, &ctx->bad, &ctx->bits, &ctx->gkey,
-                         &ctx->sgrid, &ctx->sgrid32, &ctx->stv, &ctx->sto, &ctx->sbest};
+                         &ctx->sgrid, &ctx->sgrid32, &ctx->stv, &ctx->sto, &ctx->sbest, &ctx->nmloop};
         for (DevBuf *b : all) cudaFree(b->p);
         if (ctx->has_masks) {
             cudaFree(ctx->mc.codes);
@@ -1380,6 +1380,78 @@ int grc_fit_orientation_nm(grc_ctx *ctx, const double *d_pos, const double *d_x0
         CU(cudaMemcpyAsync(ctx->nm_active, active, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
         return GRC_OK;
     };
+    // Device-side loop: one graph whose conditional WHILE node repeats the kSteps body until no seed
+    // runs (nm_continue_k sets the condition after each body), so the whole fit is one launch with
+    // no host round trip.  Falls back to replaying the body from the host when the runtime cannot
+    // build it.
+    {
+        const int max_bodies = (int)((max_steps + kSteps - 1) / kSteps);
+        TRY(ensure(ctx, ctx->nmloop, sizeof(int)));
+        int *bodies = (int *)ctx->nmloop.p;  // bodies run, zeroed before the launch
+        cudaGraph_t wg = nullptr;
+        cudaGraphExec_t wx = nullptr;
+        cudaGraphConditionalHandle handle = 0;
+        bool built = cudaGraphCreate(&wg, 0) == cudaSuccess &&
+                     cudaGraphConditionalHandleCreate(&handle, wg, 1, cudaGraphCondAssignDefault) == cudaSuccess;
+        cudaGraphNodeParams cp{};
+        cudaGraphNode_t cnode = nullptr;
+        if (built) {
+            cp.type = cudaGraphNodeTypeConditional;
+            cp.conditional.handle = handle;
+            cp.conditional.type = cudaGraphCondTypeWhile;
+            cp.conditional.size = 1;
+            built = cudaGraphAddNode(&cnode, wg, nullptr, 0, &cp) == cudaSuccess;
+        }
+        if (built) {
+            cudaGraph_t body = cp.conditional.phGraph_out[0];
+            built = cudaStreamBeginCaptureToGraph(ctx->stream, body, nullptr, nullptr, 0,
+                                                  cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+            if (built) {
+                int brc = GRC_OK;
+                for (int k = 0; k < kSteps && brc == GRC_OK; ++k) {
+                    if (cudaMemsetAsync(active, 0, sizeof(int), ctx->stream) != cudaSuccess ||
+                        grc::launch_nm_propose((grc::NmSeed *)ctx->nm.p, n, max_evals, max_iter, tol_f, tol_x,
+                                               (double *)ctx->U.p, (longlong4 *)ctx->items.p, active,
+                                               ctx->stream) != cudaSuccess ||
+                        grc::launch_score(ctx->geo, b, w, ctx->num_sms, ctx->stream, nullptr, nullptr, &launches) !=
+                            cudaSuccess ||
+                        grc::launch_nm_accept((grc::NmSeed *)ctx->nm.p, n, (const grc::TrialRes *)ctx->res.p,
+                                              ctx->stream) != cudaSuccess)
+                        brc = GRC_ECUDA;
+                }
+                if (brc == GRC_OK &&
+                    grc::launch_nm_continue((unsigned long long)handle, active, bodies, max_bodies, ctx->stream) !=
+                        cudaSuccess)
+                    brc = GRC_ECUDA;
+                cudaGraph_t captured = nullptr;
+                const bool ended = cudaStreamEndCapture(ctx->stream, &captured) == cudaSuccess;
+                built = brc == GRC_OK && ended && cudaGraphInstantiate(&wx, wg, 0) == cudaSuccess;
+            }
+        }
+        if (built) {
+            int h_bodies = 0;
+            cudaError_t le = cudaMemsetAsync(bodies, 0, sizeof(int), ctx->stream);
+            if (le == cudaSuccess) le = cudaGraphLaunch(wx, ctx->stream);
+            if (le == cudaSuccess)
+                le = cudaMemcpyAsync(&h_bodies, bodies, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream);
+            if (le == cudaSuccess) le = cudaStreamSynchronize(ctx->stream);
+            cudaGraphExecDestroy(wx);
+            cudaGraphDestroy(wg);
+            if (le != cudaSuccess) return fail(ctx, GRC_ECUDA, "orientation fit: %s", cudaGetErrorString(le));
+            CU(grc::launch_nm_final((const grc::NmSeed *)ctx->nm.p, n, d_x, d_fval, d_evals, d_iters, d_flag,
+                                    ctx->stream));
+            CU(cudaStreamSynchronize(ctx->stream));
+            ctx->stats.trials = (int64_t)h_bodies * kSteps * T;
+            ctx->stats.kernel_launches = (int64_t)h_bodies * (kSteps * (2 + launches / kSteps) + 1) + 2;
+            ctx->stats.path = 1;
+            ctx->stats.device_loop = 1;
+            return GRC_OK;
+        }
+        if (wx) cudaGraphExecDestroy(wx);
+        if (wg) cudaGraphDestroy(wg);
+        cudaGetLastError();  // the host-driven replay below does the same work
+        launches = 0;
+    }
     int rc = GRC_OK;
     cudaError_t e = cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal);
     if (e == cudaSuccess) {

@@ -237,6 +237,11 @@ cudaError_t launch_nm_init(NmSeed *st, int64_t n, const double *x0, double half_
 cudaError_t launch_nm_propose(NmSeed *st, int64_t n, int max_evals, int max_iter, double tol_f, double tol_x,
                               double *U, longlong4 *items, int *active, cudaStream_t s);
 cudaError_t launch_nm_accept(NmSeed *st, int64_t n, const TrialRes *res, cudaStream_t s);
+// Loop test of a device-side Nelder-Mead loop (the body of a conditional WHILE graph node): counts
+// one more body in *bodies and keeps the loop going while a seed still runs (*active > 0) and
+// fewer than max_bodies bodies have run.
+cudaError_t launch_nm_continue(unsigned long long handle, const int *active, int *bodies, int max_bodies,
+                               cudaStream_t s);
 cudaError_t launch_nm_final(const NmSeed *st, int64_t n, double *x, double *fval, int32_t *evals, int32_t *iters,
                             int32_t *flag, cudaStream_t s);
 

@@ -371,6 +371,21 @@ cudaError_t launch_nm_accept(NmSeed *st, int64_t n, const TrialRes *res, cudaStr
     return cudaGetLastError();
 }
 
+namespace {
+__global__ void nm_continue_k(cudaGraphConditionalHandle handle, const int *active, int *bodies, int max_bodies) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        const int k = ++*bodies;
+        cudaGraphSetConditional(handle, (*active > 0 && k < max_bodies) ? 1u : 0u);
+    }
+}
+}  // namespace
+
+cudaError_t launch_nm_continue(unsigned long long handle, const int *active, int *bodies, int max_bodies,
+                               cudaStream_t s) {
+    nm_continue_k<<<1, 32, 0, s>>>((cudaGraphConditionalHandle)handle, active, bodies, max_bodies);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_nm_final(const NmSeed *st, int64_t n, double *x, double *fval, int32_t *evals, int32_t *iters,
                             int32_t *flag, cudaStream_t s) {
     nm_final_k<<<blocks_for(n), kB, 0, s>>>(st, n, x, fval, evals, iters, flag);

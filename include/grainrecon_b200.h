@@ -485,6 +485,9 @@ typedef struct {
     int64_t path;            /* 1 = per-trial kernel, 2 = CTA sweep, 3 = warp scan */
     int64_t audit_checked;   /* audit builds only: FP32 decisions re-decided in FP64 */
     int64_t audit_mismatch;  /* audit builds only: of those, decisions that differed */
+    int64_t device_loop;     /* grc_fit_orientation_nm: 1 when its iterations ran as one graph whose
+                                conditional WHILE node stops on the device, 0 when the host replayed
+                                the steps */
 } grc_stats;
 int grc_last_stats(grc_ctx *ctx, grc_stats *out);
 /* 1 = record CUDA events around the scoring kernel of each call (for benchmarks). */

@@ -142,6 +142,8 @@ def test_orientation_fit_matches_oracle_fminsearchbnd(scene):
     fval = torch.empty(n, dtype=torch.float64, device="cuda")
     ev, it, fl = (torch.empty(n, dtype=torch.int32, device="cuda") for _ in range(3))
     ctx.fit_orientation_nm(d(pos), d(x0), n, x, fval, ev, it, fl)
+    # the iterations run as one graph whose conditional WHILE node stops on the device
+    assert ctx.last_stats()["device_loop"] == 1
     x, fval, ev, it, fl = (a.cpu().numpy() for a in (x, fval, ev, it, fl))
     same = 0
     for i in range(n):
