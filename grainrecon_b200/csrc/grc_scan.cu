@@ -384,11 +384,12 @@ cudaError_t launch_scan_t(const Geo &g, const ScoreBufs &b, const Work &w, int64
         }
         return cand == 32 ? (ScanFn)scan_kernel<MODE, HPL, 32> : (ScanFn)scan_kernel<MODE, HPL, 16>;
     };
-    // Explicit trial lists (the seeding refine's grids, grow and compete rows) keep 32: the refine
-    // of 16 Al seeds took 0.234 s with 32-projection windows against 0.246-0.255 s with 128.
-    const bool wide = MODE == kScanComp && !explicit_voxels;
+    // Explicit trial lists in completeness mode (the seeding refine's grids) take at most 64: the
+    // refine of 16 Al seeds took 0.223 s with 64-projection windows, 0.234 s with 32 and
+    // 0.246-0.255 s with 128.
+    const bool wide = MODE == kScanComp;
     const int kCands = wide ? 4 : 2;
-    const int cands_wide[4] = {128, 64, 32, 16}, cands_narrow[2] = {32, 16};
+    const int cands_wide[4] = {explicit_voxels ? 64 : 128, 64, 32, 16}, cands_narrow[2] = {32, 16};
     const int *cands = wide ? cands_wide : cands_narrow;
     // the bit-mask window stays within 3/4 of L2 (Al 2048^2 on 126 MB: 128 projections = 67 MB,
     // fastest; 256 = 134 MB ran 30% slower)
