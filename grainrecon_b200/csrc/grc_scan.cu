@@ -398,7 +398,8 @@ cudaError_t launch_scan_t(const Geo &g, const ScoreBufs &b, const Work &w, int64
         int dev = 0, l2 = 0;
         if (cudaGetDevice(&dev) == cudaSuccess && cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, dev) == cudaSuccess)
             l2_budget = (int64_t)l2 * 3 / 4;
-        cudaGetLastError();
+        else
+            cudaGetLastError();  // no L2 size: windows of at most 32 projections
     }
     for (int ci = 0; ci < kCands; ++ci) {
         const int cand = cands[ci];
