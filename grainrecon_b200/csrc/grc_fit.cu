@@ -19,6 +19,7 @@
 #include <stdint.h>
 
 #include "grc_fit.h"
+#include "grc_internal.h"
 
 namespace grc {
 namespace {
@@ -316,35 +317,37 @@ __device__ __forceinline__ void block_sum(double (&a)[N], double *scratch) {
 constexpr int kNE6 = 21 + 6 + 2;
 __global__ void grain_normal_k(FitFixed fx, const double *grains, const double *geo10, SpotList sp,
                                const int64_t *offsets, int64_t n_grains, double *ne) {
-    __shared__ double scratch[32 * kNE6];
+    // the thread's 29 accumulators in shared memory (column k of thread t at k * 128 + t), so one
+    // pass carries all 6 tangents
+    extern __shared__ double acc_s[];
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
     for (int64_t gi = blockIdx.x; gi < n_grains; gi += gridDim.x) {
-        double acc[kNE6];
-        for (int k = 0; k < kNE6; ++k) acc[k] = 0;
+        for (int k = 0; k < kNE6; ++k) acc_s[k * 128 + t] = 0;
         const double *g6 = grains + 6 * gi;
         for (int64_t i = offsets[gi] + threadIdx.x; i < offsets[gi + 1]; i += blockDim.x) {
-            double ru, rv, ju[6], jv[6], t0[3], t1[3];
-            const bool ok1 = spot_eval<3>(fx, 0, 0, g6, geo10, sp.iw[i], sp.ih[i], ru, rv, t0, t1);
-            for (int k = 0; k < 3; ++k) {
-                ju[k] = t0[k];
-                jv[k] = t1[k];
-            }
-            const bool ok2 = spot_eval<3>(fx, 0, 3, g6, geo10, sp.iw[i], sp.ih[i], ru, rv, t0, t1);
-            for (int k = 0; k < 3; ++k) {
-                ju[3 + k] = t0[k];
-                jv[3 + k] = t1[k];
-            }
-            if (!(ok1 && ok2)) continue;  // spot left the detector: not part of this residual
+            double ru, rv, ju[6], jv[6];
+            // spot left the detector: not part of this residual
+            if (!spot_eval<6>(fx, 0, 0, g6, geo10, sp.iw[i], sp.ih[i], ru, rv, ju, jv)) continue;
             const double eu = ru - sp.uv[2 * i], ev = rv - sp.uv[2 * i + 1];
             int q = 0;
+#pragma unroll
             for (int a = 0; a < 6; ++a)
-                for (int b = a; b < 6; ++b) acc[q++] += ju[a] * ju[b] + jv[a] * jv[b];
-            for (int a = 0; a < 6; ++a) acc[21 + a] += ju[a] * eu + jv[a] * ev;
-            acc[27] += eu * eu + ev * ev;
-            acc[28] += 1.0;
+#pragma unroll
+                for (int b = a; b < 6; ++b) acc_s[(q++) * 128 + t] += ju[a] * ju[b] + jv[a] * jv[b];
+#pragma unroll
+            for (int a = 0; a < 6; ++a) acc_s[(21 + a) * 128 + t] += ju[a] * eu + jv[a] * ev;
+            acc_s[27 * 128 + t] += eu * eu + ev * ev;
+            acc_s[28 * 128 + t] += 1.0;
         }
-        block_sum<kNE6>(acc, scratch);
-        if (threadIdx.x == 0)
-            for (int k = 0; k < kNE6; ++k) ne[gi * kNE6 + k] = acc[k];
+        __syncthreads();
+        for (int k = warp; k < kNE6; k += 4) {
+            double v = acc_s[k * 128 + lane] + acc_s[k * 128 + lane + 32] + acc_s[k * 128 + lane + 64] +
+                       acc_s[k * 128 + lane + 96];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+            if (lane == 0) ne[gi * kNE6 + k] = v;
+        }
+        __syncthreads();  // the next grain clears the accumulators
     }
 }
 
@@ -607,34 +610,39 @@ __global__ void grain_nm_k(FitFixed fx, double *grains, const double *geo10, Spo
 // atomically into the start's 66 accumulators (55 upper J^T J, 10 J^T r, r^T r).
 constexpr int kNE10 = 55 + 10 + 2;
 __global__ void geo_normal_k(FitFixed fx, const double *grains, const double *starts, SpotList sp, double *ne) {
-    __shared__ double scratch[32 * kNE10];
-    const int st = blockIdx.y;
+    // Each thread's 67 accumulators live in shared memory (column k of thread t at k * 128 + t),
+    // which leaves the registers to one pass of all 10 tangent directions: against 67 register
+    // accumulators and five passes of 2 tangents, an LM iteration of the 64-start Al fit runs
+    // 2.5x faster (0.132 s against 0.331 s to 0.1 px).
+    extern __shared__ double acc_s[];
+    const int st = blockIdx.y, t = threadIdx.x;
     const double *geo = starts + 10 * st;
-    double acc[kNE10];
-    for (int k = 0; k < kNE10; ++k) acc[k] = 0;
+    for (int k = 0; k < kNE10; ++k) acc_s[k * 128 + t] = 0;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < sp.n; i += (int64_t)gridDim.x * blockDim.x) {
-        double ju[10], jv[10], ru = 0, rv = 0, t0[2], t1[2];
-        bool ok = true;
+        double ju[10], jv[10], ru = 0, rv = 0;
         const double *g6 = grains + 6 * (int64_t)sp.grain[i];
-        for (int c0 = 0; c0 < 10; c0 += 2) {
-            ok = spot_eval<2>(fx, 1, c0, g6, geo, sp.iw[i], sp.ih[i], ru, rv, t0, t1) && ok;
-            ju[c0] = t0[0];
-            ju[c0 + 1] = t0[1];
-            jv[c0] = t1[0];
-            jv[c0 + 1] = t1[1];
-        }
-        if (!ok) continue;
+        if (!spot_eval<10>(fx, 1, 0, g6, geo, sp.iw[i], sp.ih[i], ru, rv, ju, jv)) continue;
         const double eu = ru - sp.uv[2 * i], ev = rv - sp.uv[2 * i + 1];
         int q = 0;
+#pragma unroll
         for (int a = 0; a < 10; ++a)
-            for (int b = a; b < 10; ++b) acc[q++] += ju[a] * ju[b] + jv[a] * jv[b];
-        for (int a = 0; a < 10; ++a) acc[55 + a] += ju[a] * eu + jv[a] * ev;
-        acc[65] += eu * eu + ev * ev;
-        acc[66] += 1.0;
+#pragma unroll
+            for (int b = a; b < 10; ++b) acc_s[(q++) * 128 + t] += ju[a] * ju[b] + jv[a] * jv[b];
+#pragma unroll
+        for (int a = 0; a < 10; ++a) acc_s[(55 + a) * 128 + t] += ju[a] * eu + jv[a] * ev;
+        acc_s[65 * 128 + t] += eu * eu + ev * ev;
+        acc_s[66 * 128 + t] += 1.0;
     }
-    block_sum<kNE10>(acc, scratch);
-    if (threadIdx.x == 0)
-        for (int k = 0; k < kNE10; ++k) atomicAdd(&ne[st * kNE10 + k], acc[k]);
+    __syncthreads();
+    // column sums: warp w sums columns w, w + 4, ...
+    const int lane = t & 31, warp = t >> 5;
+    for (int k = warp; k < kNE10; k += 4) {
+        double v = acc_s[k * 128 + lane] + acc_s[k * 128 + lane + 32] + acc_s[k * 128 + lane + 64] +
+                   acc_s[k * 128 + lane + 96];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+        if (lane == 0) atomicAdd(&ne[st * kNE10 + k], v);
+    }
 }
 
 __global__ void geo_cost_k(FitFixed fx, const double *grains, const double *starts, SpotList sp, double *cost) {
@@ -793,7 +801,10 @@ cudaError_t fit_spots_fill(const FitFixed &fx, const double *grains, const doubl
 
 cudaError_t fit_grain_normal(const FitFixed &fx, const double *grains, const double *geo10, const SpotList &sp,
                              const int64_t *offsets, int64_t n_grains, double *ne, cudaStream_t s) {
-    grain_normal_k<<<grid_for(n_grains, 1), 128, 0, s>>>(fx, grains, geo10, sp, offsets, n_grains, ne);
+    const size_t smem = sizeof(double) * kNE6 * 128;
+    const cudaError_t e = allow_smem((const void *)grain_normal_k, smem);
+    if (e != cudaSuccess) return e;
+    grain_normal_k<<<grid_for(n_grains, 1), 128, smem, s>>>(fx, grains, geo10, sp, offsets, n_grains, ne);
     return cudaGetLastError();
 }
 
@@ -834,7 +845,10 @@ cudaError_t fit_geo_normal(const FitFixed &fx, const double *grains, const doubl
     cudaError_t e = cudaMemsetAsync(ne, 0, sizeof(double) * kNE10 * n_starts, s);
     if (e != cudaSuccess) return e;
     const int gx = grid_for(sp.n, 128) < num_sms * 4 ? grid_for(sp.n, 128) : num_sms * 4;
-    geo_normal_k<<<dim3(gx, n_starts), 128, 0, s>>>(fx, grains, starts, sp, ne);
+    const size_t smem = sizeof(double) * kNE10 * 128;
+    e = allow_smem((const void *)geo_normal_k, smem);
+    if (e != cudaSuccess) return e;
+    geo_normal_k<<<dim3(gx, n_starts), 128, smem, s>>>(fx, grains, starts, sp, ne);
     return cudaGetLastError();
 }
 

@@ -78,3 +78,18 @@ def test_map_key_follows_content_not_address():
         c = small.copy()
         c[i] = -c[i]
         assert _lib.map_key(c, 4096) != _lib.map_key(small, 4096)
+
+
+def _struct_fields(name):
+    """(type, field) pairs of a typedef struct in the header."""
+    src = re.sub(r"/\*.*?\*/", "", open(HEADER).read(), flags=re.S)
+    body = re.search(r"typedef struct\s*\{(.*?)\}\s*" + name + r"\s*;", src, flags=re.S).group(1)
+    return [tuple(m) for m in re.findall(r"(\w+)\s+(\w+)\s*;", body)]
+
+
+def test_stats_struct_matches_binding():
+    """grc_stats is read through ctypes: same fields, same order, same widths."""
+    widths = {"int64_t": 8, "double": 8, "int32_t": 4, "int": 4}
+    fields = _struct_fields("grc_stats")
+    assert [f for _, f in fields] == [f for f, _ in _lib.Stats._fields_]
+    assert sum(widths[t] for t, _ in fields) == C.sizeof(_lib.Stats)
