@@ -607,7 +607,7 @@ __global__ void grain_nm_k(FitFixed fx, double *grains, const double *geo10, Spo
 
 // ---- geometry fit: normal equations of every start ------------------------------------
 // Spots are split across CTAs (blockIdx.x) for start blockIdx.y; partial sums are added
-// atomically into the start's 66 accumulators (55 upper J^T J, 10 J^T r, r^T r).
+// atomically into the start's 67 accumulators (55 upper J^T J, 10 J^T r, r^T r, n).
 constexpr int kNE10 = 55 + 10 + 2;
 __global__ void geo_normal_k(FitFixed fx, const double *grains, const double *starts, SpotList sp, double *ne) {
     // Each thread's 67 accumulators live in shared memory (column k of thread t at k * 128 + t),
