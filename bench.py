@@ -116,16 +116,20 @@ def build_problem(config: str, seed: int, sample=None):
     return s, pos, q
 
 
-def workload_desc(s, seeds_per_step):
+def workload_desc(s, seeds_per_step, output="completeness"):
     g = s.geom
+    npx = g.nrot * g.detysize * g.detzsize
+    read = (f"the packed hit mask ({npx / 8 / 1e6:.0f} MB, one bit per pixel)" if output == "completeness"
+            else f"the distance map as 8-bit rank codes ({npx / 1e9:.2f} GB)")
+    big = (npx / 8 if output == "completeness" else npx) > 126e6
     return {"workload": (f"seeding scan: {'FCC Al' if s.space_group == 225 else 'BCC Fe'} "
                          f"{len(s.grain_q)} grains, {int((s.grain_id > 0).sum())} voxels, "
                          f"{g.detysize}x{g.detzsize} detector, {g.nrot} projections, {s.nhkl} reflections; "
                          f"{seeds_per_step} seed voxels x {N_ORIENT} orientations per step per GPU"),
             "trials_per_step_per_gpu": seeds_per_step * N_ORIENT,
             "reflections_per_trial": g.nrot * s.nhkl,
-            "l2": "inputs larger than L2: the resident rank-coded distance map "
-                  f"({g.nrot * g.detysize * g.detzsize * 2 / 1e9:.2f} GB) is read by every step",
+            "l2": (f"inputs larger than L2 (126 MB): {read} is read by every step" if big else
+                   f"{read} fits in L2 (126 MB) and stays resident across steps (no flush)"),
             "parallelism": "replicas: seeds sharded across ranks, no collective on the data path"}
 
 
@@ -345,7 +349,7 @@ def run_ours(args):
         torch.cuda.synchronize()
         cpu = cpu_baseline(s, host_map, seeds, q, args.cpu_trials)
     if rank == 0:
-        cfg = workload_desc(s, S)
+        cfg = workload_desc(s, S, args.output)
         cfg["output"] = (("completeness only: Nr_simu, Nr_intersect and completeness from the bit-packed hit "
                           "mask (column 4 NaN), and each seed's first maximum over its orientations; the "
                           "seeding engine reads column 3 only (GrainMapping_engine_gpu_comp.m:103)") if comp else
