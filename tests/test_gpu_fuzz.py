@@ -7,7 +7,8 @@ per lane in the window kernels); six more push to 1-2 reflections, 1-12 projecti
 tilts and a beam stop over the detector centre.  Odd seeds use a distance map with a few
 distinct values (8-bit codes), even seeds one with millions (32-bit codes and the radix refine
 of the median).  On the per-trial kernel, the CTA sweep and the warp scan, with and without the median,
-every trial without a tight edge reflection equals the oracle in every column it returns."""
+every trial without a tight edge reflection equals the oracle in every column it returns.  Seven of
+the geometries also run the grow and compete entries against the oracle's grow and compete."""
 import numpy as np
 import pytest
 
@@ -89,3 +90,68 @@ def test_random_geometry_matches_oracle(seed, nhkl, extreme):
                         assert np.isnan(gpu[:, 3]).all()
         ctx.set_path(0)
         ctx.set_median(True)
+
+
+def _volume_param1(rng, simap, dim=60):
+    """param1[:11] of a dim^3 volume of 5 um voxels around a random centre (the positions span
+    about +-0.15 mm, like the seed positions above); simap 1 flips x and y."""
+    centre = rng.uniform(-0.02, 0.02, 3)
+    return np.array([1, 1, 1, simap, 0.005, *centre, dim, dim, dim, 0, 0, 0], np.float32), dim
+
+
+@pytest.mark.parametrize("seed,nhkl,extreme", [CASES[i] for i in (0, 1, 4, 5, 8, 9, 12)])
+def test_random_geometry_grow_and_compete_match_oracle(seed, nhkl, extreme):
+    """cuda_grow_indexed_region and cuda_forward_comp_compete on the same random geometries, on
+    every kernel: trials without a tight edge reflection equal the oracle in every column
+    (dis_median to float32 rounding, as in the fixed-geometry parity tests)."""
+    geom, dmap, (S9, B9, hk, rot, R9, p), _, q = _case(seed, nhkl, extreme)
+    rng = np.random.default_rng(seed + 1000)
+    p1, dim = _volume_param1(rng, seed % 2)
+    m = 256
+    idx = rng.integers(1, dim + 1, (m, 3)).astype(np.float32)
+    # grow rows [x y z I mask dmed]; about 0.12-0.15 of the random map's pixels are hits
+    rows6 = np.zeros((m, 6), np.float32)
+    rows6[:, :3] = idx
+    rows6[:, 3] = rng.uniform(0, 0.3, m)
+    rows6[:, 4] = rng.random(m) > 0.2
+    rows6[:, 5] = rng.uniform(0, 10, m)
+    p1g = p1.copy()
+    p1g[11:14] = (0.15, 0.1, 6.0)  # flag: C >= 0.135, about the random map's hit fraction
+    U = G.flat_rowmajor(G.quat_to_u(q[0]))
+    g_ref, _, g_tight = O.grow(rows6, U, S9, B9, hk, dmap, rot, R9, p, p1g, tight=True)
+    g_ref = g_ref.reshape(-1, 7)
+    g_ok = g_tight == 0
+    assert g_ok.sum() >= m - 8
+    # compete: 1-16 candidates per voxel among 40 orientations, one voxel without any
+    ng = 40
+    eul = (np.degrees([G.u_to_euler(G.quat_to_u(x)) for x in q[:ng]]) % 360).astype(np.float32)
+    counts = np.minimum(rng.geometric(0.3, m), 16)
+    counts[7] = 0
+    ids, rows5 = [], np.zeros((m, 5), np.float32)
+    rows5[:, :3] = idx
+    for i, c in enumerate(counts):
+        rows5[i, 3] = len(ids) + 1
+        ids.extend(rng.integers(1, ng + 1, c).tolist())
+        rows5[i, 4] = len(ids)
+    ids = np.array(ids, np.float32)
+    c_ref, _, c_tight = O.compete(rows5, ids, eul, S9, B9, hk, dmap, rot, R9, p, p1, tight=True)
+    c_ref = c_ref.reshape(-1, 8)
+    c_ok = c_tight == 0
+    assert c_ok.sum() >= m - 16
+    with Context(0) as ctx:
+        ctx.set_geometry(S9, B9, hk, rot, R9, p)
+        ctx.upload_masks(dmap, geom.detzsize, geom.detysize, geom.nrot)
+        for path in (1, 2, 3):
+            ctx.set_path(path)
+            msg = f"seed {seed} path {path}"
+            gg = ctx.grow_indexed_region(rows6, U, S9, B9, hk, None, rot, R9, p, p1g).reshape(-1, 7)
+            assert ctx.last_stats()["path"] == path
+            np.testing.assert_array_equal(gg[g_ok][:, [0, 1, 2, 3, 4, 6]], g_ref[g_ok][:, [0, 1, 2, 3, 4, 6]],
+                                          err_msg=msg + " grow")
+            np.testing.assert_allclose(gg[g_ok, 5], g_ref[g_ok, 5], rtol=1e-6, err_msg=msg + " grow median")
+            gc = ctx.forward_comp_compete(rows5, ids, eul, S9, B9, hk, None, rot, R9, p, p1).reshape(-1, 8)
+            assert ctx.last_stats()["path"] == path
+            np.testing.assert_array_equal(gc[c_ok][:, :7], c_ref[c_ok][:, :7], err_msg=msg + " compete")
+            np.testing.assert_allclose(gc[c_ok, 7], c_ref[c_ok, 7], rtol=1e-6, err_msg=msg + " compete median")
+            assert gc[7, 4] == 0 and gc[7, 7] == 2000
+        ctx.set_path(0)
