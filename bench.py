@@ -784,6 +784,92 @@ def verify_fitted_completeness(ctx, fitted_geo10, seed, n_vox=64, n_or=1024):
             "unchanged_trials": same / (n_vox * n_or), "true_orientation_C>0.9_voxels": hit_true}
 
 
+def run_pair(args):
+    """Spot pairing (forward_comp_pair_spots.m:73-80, grc_pair_spots) on the fe6 sample: each grain's
+    orientation at 256 voxels of that grain, against the measured centroid list of all six grains
+    (each grain's landings at its mean position, 0.5 px Gaussian noise, area 10 px) plus 20 spurious
+    spots per projection.  Each call is synchronous (it returns the pair count); the device time
+    of the K calls comes from CUDA events on the library's stream."""
+    import ctypes as C
+
+    import torch
+    from grainrecon_b200 import fit as F
+    from grainrecon_b200 import synth
+    from grainrecon_b200._lib import PAIR_DTYPE, Context, _ptr
+
+    rank, world, local = env_rank()
+    torch.cuda.set_device(local)
+    s = synth.make_sample("fe6", seed=args.seed)
+    ctx = Context(local)
+    synth.device_maps(s, ctx)
+    g = s.geom
+    S9, B9, hkl, rot, R9, p = s.mex_arrays()
+    ctx.set_geometry(S9, B9, hkl, rot, R9, p)
+    idx = s.voxel_indices()
+    gid = s.grain_id[tuple((idx - 1).T)]
+    ng = len(s.grain_q)
+    q = np.asarray(s.grain_q, np.float64)
+    centre = np.stack([s.vol.pos_of_index(idx[gid == k + 1]).mean(0) for k in range(ng)])
+    d_grains = torch.from_numpy(np.concatenate([F.quat_to_rod(q), centre], 1).reshape(-1).copy()).cuda()
+    spots = F.simulate_spots(ctx, F.geo10_of(g), d_grains, 0.5, args.seed + 1)
+    rng = np.random.default_rng(args.seed + 2)
+    n_fake = 20 * g.nrot
+    sp_iw = torch.cat([spots.iw.long(), torch.arange(g.nrot, device="cuda").repeat_interleave(20)])
+    fake = np.stack([rng.uniform(1, g.detysize, n_fake), rng.uniform(1, g.detzsize, n_fake)], 1)
+    sp_uv = torch.cat([spots.uv.view(-1, 2), torch.from_numpy(fake).cuda()])
+    sp = torch.cat([sp_uv, torch.full((len(sp_iw), 1), 10.0, dtype=torch.float64, device="cuda")], 1)
+    order = torch.argsort(sp_iw, stable=True)
+    d_sp = sp[order].contiguous().view(-1)
+    n_sp = len(sp_iw)
+    d_off = torch.zeros(g.nrot + 1, dtype=torch.int64, device="cuda")
+    d_off[1:] = torch.cumsum(torch.bincount(sp_iw, minlength=g.nrot), 0)
+    per = 256
+    pos, quat = [], []
+    for k in range(ng):
+        mine = idx[gid == k + 1]
+        pick = mine[rng.choice(len(mine), per, replace=len(mine) < per)]
+        pos.append(s.vol.pos_of_index(pick))
+        quat.append(np.repeat(q[k][None], per, 0))
+    d_pos = torch.from_numpy(np.concatenate(pos).reshape(-1).copy()).cuda()
+    d_q = torch.from_numpy(np.concatenate(quat).reshape(-1).copy()).cuda()
+    n = ng * per
+    pairs = ctx.pair_spots(d_pos, d_q, n, d_sp, n_sp, d_off)
+    cap = max(len(pairs), 1)
+    buf = torch.empty(cap * PAIR_DTYPE.itemsize, dtype=torch.uint8, device="cuda")
+    npairs = C.c_int64()
+    torch.cuda.synchronize()
+
+    def call():
+        ctx._check(ctx.L.grc_pair_spots(ctx.h, _ptr(d_pos), _ptr(d_q), n, _ptr(d_sp), n_sp, _ptr(d_off),
+                                        _ptr(buf), cap, C.byref(npairs)))
+
+    for _ in range(args.warmup):
+        call()
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0 = time.perf_counter()
+    ev0.record(stream)
+    for _ in range(args.steps):
+        call()
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    wall = (time.perf_counter() - t0) / args.steps
+    dev_ms = ev0.elapsed_time(ev1) / args.steps
+    assert npairs.value == len(pairs)
+    line = {"metric": "spot pairing trials/s", "value": n / (dev_ms / 1e3), "unit": "trials/s", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": dev_ms, "higher_is_better": True,
+            "dtype": "f64", "data": "synthetic",
+            "config": {"workload": (f"fe6-pair: BCC Fe {ng} grains, {g.detysize}x{g.detzsize} detector, "
+                                    f"{g.nrot} projections, {s.nhkl} reflections; {n} trials (each grain's "
+                                    f"orientation at {per} of its voxels) against {n_sp} measured spots"),
+                       "spots": n_sp, "trials": n},
+            "pairs_per_step": int(npairs.value), "pairs_per_s": npairs.value / (dev_ms / 1e3),
+            "wall_ms_per_step": wall * 1e3}
+    print(json.dumps(line), flush=True)
+    ctx.close()
+    return 0
+
+
 def run_fit(args):
     """Fit benchmarks: 5,000-grain orientation+centre fit (BCC Fe, 1024^2, 181 projections) or the
     10-parameter geometry fit (FCC Al, 2048^2, 361 projections, 2,000 grains, 64 starts)."""
@@ -830,7 +916,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="al400", choices=["al400", "fe6", "al400-grow", "fe-fit", "al-geofit",
-                                                                "al400-seed", "fe6-map", "al400-walk"])
+                                                                "al400-seed", "fe6-map", "al400-walk", "fe6-pair"])
     ap.add_argument("--map-iters", type=int, default=4, help="fe6-map: mapping iterations at most")
     ap.add_argument("--nr-seed", type=int, default=400, help="al400-seed: candidates refined per seed")
     ap.add_argument("--seed-batch", type=int, default=16, help="al400-seed: seeds per step")
@@ -863,6 +949,8 @@ def main():
         return run_map(args)
     if args.config == "al400-walk":
         return run_walk(args)
+    if args.config == "fe6-pair":
+        return run_pair(args)
     return run_ours(args)
 
 

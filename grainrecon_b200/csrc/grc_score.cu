@@ -966,66 +966,135 @@ cudaError_t launch_mark_t(const Geo &g, const ScoreBufs &b, const Work &w, int n
 // centroid of that projection (first in list order among equal distances) is paired when it
 // lies closer than min(sqrt(area), 15) pixels.  The spot index holds, per projection, the spots
 // of each cell of cell_px x cell_px pixels in list order.
+// One selected (projection, reflection) item of a trial: the FP64 landing, the hit test and the
+// nearest centroid.
 template <typename CodeT>
-__global__ void __launch_bounds__(128) pair_kernel(Geo g, ScoreBufs b, int64_t n, SpotIndex si, PairRec *out,
-                                                   int64_t cap, unsigned long long *count) {
-    __shared__ double sub[9];
+__device__ __forceinline__ void pair_item(const Geo &g, const ScoreBufs &b, const SpotIndex &si, int64_t t,
+                                          const OmegaRow &r, const double4 gv, int iw, int ih, PairRec *out,
+                                          int64_t cap, unsigned long long *count) {
     const CodeT *codes = (const CodeT *)b.codes;
-    for (int64_t t = blockIdx.x; t < n; t += gridDim.x) {
-        __syncthreads();
-        if (threadIdx.x == 0) sub_matrix(g, b.U + 9 * t, sub);
-        __syncthreads();
-        const double *vp = b.vpos + 3 * t;
-        for (int iw = threadIdx.x; iw < g.nrot; iw += blockDim.x) {
-            const OmegaRow r = omega_row(g, b.rot_cs[iw], vp);
-            for (int ih = 0; ih < g.nhkl; ++ih) {
-                const double h = b.hkl[3 * ih], k = b.hkl[3 * ih + 1], l = b.hkl[3 * ih + 2];
-                const double x = sub[0] * h + sub[1] * k + sub[2] * l;
-                const double y = sub[3] * h + sub[4] * k + sub[5] * l;
-                const double z = sub[6] * h + sub[7] * k + sub[8] * l;
-                double lam = 0.0;
-                const int64_t idx = landing_fp64(g, r, x, y, z, iw, &lam);
-                if (idx < 0) continue;
-                const uint32_t code = (uint32_t)codes[idx];
-                if (code >= g.n_hit) continue;
-                const int64_t in_plane = idx - (int64_t)iw * g.plane;
-                const int dety = (int)(in_plane / g.detzsize) + 1, detz = (int)(in_plane % g.detzsize) + 1;
-                const int cy0 = max(0, (dety - 16) / si.cell_px), cy1 = min(si.ncy - 1, (dety + 14) / si.cell_px);
-                const int cz0 = max(0, (detz - 16) / si.cell_px), cz1 = min(si.ncz - 1, (detz + 14) / si.cell_px);
-                int best = -1;
-                double bd = 0.0;
-                for (int cy = cy0; cy <= cy1; ++cy)
-                    for (int cz = cz0; cz <= cz1; ++cz) {
-                        const int64_t cell = ((int64_t)iw * si.ncy + cy) * si.ncz + cz;
-                        for (int64_t q = si.cell_off[cell]; q < si.cell_off[cell + 1]; ++q) {
-                            const int id = si.cell_ids[q];
-                            const double dy = __dsub_rn(si.yza[3 * id], (double)dety);
-                            const double dz = __dsub_rn(si.yza[3 * id + 1], (double)detz);
-                            const double d = sqrt(__dadd_rn(__dmul_rn(dy, dy), __dmul_rn(dz, dz)));
-                            if (best < 0 || d < bd || (d == bd && id < best)) {
-                                best = id;
-                                bd = d;
-                            }
-                        }
-                    }
-                if (best < 0 || !(bd < fmin(sqrt(si.yza[3 * best + 2]), 15.0))) continue;
-                const unsigned long long slot = atomicAdd(count, 1ull);
-                if ((int64_t)slot < cap) {
-                    PairRec p;
-                    p.trial = (int32_t)t;
-                    p.iw = iw;
-                    p.ih = ih;
-                    p.spot = best;
-                    p.dety = dety;
-                    p.detz = detz;
-                    p.exp_y = si.yza[3 * best];
-                    p.exp_z = si.yza[3 * best + 1];
-                    p.area = si.yza[3 * best + 2];
-                    p.energy_kev = 12.398 / lam;
-                    p.dis = (double)b.vals[min(code, g.n_vals - 1u)];
-                    out[slot] = p;
+    double lam = 0.0;
+    const int64_t idx = landing_fp64(g, r, gv.x, gv.y, gv.z, iw, &lam);
+    if (idx < 0) return;
+    const uint32_t code = (uint32_t)codes[idx];
+    if (code >= g.n_hit) return;
+    const int64_t in_plane = idx - (int64_t)iw * g.plane;
+    const int dety = (int)(in_plane / g.detzsize) + 1, detz = (int)(in_plane % g.detzsize) + 1;
+    const int cy0 = max(0, (dety - 16) / si.cell_px), cy1 = min(si.ncy - 1, (dety + 14) / si.cell_px);
+    const int cz0 = max(0, (detz - 16) / si.cell_px), cz1 = min(si.ncz - 1, (detz + 14) / si.cell_px);
+    int best = -1;
+    double bd = 0.0;
+    for (int cy = cy0; cy <= cy1; ++cy)
+        for (int cz = cz0; cz <= cz1; ++cz) {
+            const int64_t cell = ((int64_t)iw * si.ncy + cy) * si.ncz + cz;
+            for (int64_t q = si.cell_off[cell]; q < si.cell_off[cell + 1]; ++q) {
+                const int id = si.cell_ids[q];
+                const double dy = __dsub_rn(si.yza[3 * id], (double)dety);
+                const double dz = __dsub_rn(si.yza[3 * id + 1], (double)detz);
+                const double d = sqrt(__dadd_rn(__dmul_rn(dy, dy), __dmul_rn(dz, dz)));
+                if (best < 0 || d < bd || (d == bd && id < best)) {
+                    best = id;
+                    bd = d;
                 }
             }
+        }
+    if (best < 0 || !(bd < fmin(sqrt(si.yza[3 * best + 2]), 15.0))) return;
+    const unsigned long long slot = atomicAdd(count, 1ull);
+    if ((int64_t)slot < cap) {
+        PairRec p;
+        p.trial = (int32_t)t;
+        p.iw = iw;
+        p.ih = ih;
+        p.spot = best;
+        p.dety = dety;
+        p.detz = detz;
+        p.exp_y = si.yza[3 * best];
+        p.exp_z = si.yza[3 * best + 1];
+        p.area = si.yza[3 * best + 2];
+        p.energy_kev = 12.398 / lam;
+        p.dis = (double)b.vals[min(code, g.n_vals - 1u)];
+        out[slot] = p;
+    }
+}
+
+constexpr int kPairThreads = 128, kPairWarps = kPairThreads / 32, kPairQueue = 64;
+
+__host__ __device__ inline size_t pair_smem_bytes(int nrot, int nhkl) {
+    return sizeof(double4) * nhkl + sizeof(double) * 10 + sizeof(OmegaRow) * nrot +
+           sizeof(uint32_t) * kPairWarps * kPairQueue;
+}
+
+// One CTA per trial (grid-stride).  The trial's omega rows and G vectors (S*U*B*h with |G|) go to
+// shared memory; each warp tests 32 (projection, reflection) pairs at a time against a window
+// slightly wider than the landing's own (a superset: landing_fp64 makes the decision), queues
+// the passing items and runs the FP64 landing and the centroid search on full batches of 32.
+template <typename CodeT>
+__global__ void __launch_bounds__(kPairThreads) pair_kernel(Geo g, ScoreBufs b, int64_t n, SpotIndex si,
+                                                            PairRec *out, int64_t cap,
+                                                            unsigned long long *count) {
+    extern __shared__ __align__(16) unsigned char pair_smem[];
+    double4 *gws = (double4 *)pair_smem;
+    double *sub = (double *)(gws + g.nhkl);
+    OmegaRow *rows = (OmegaRow *)(sub + 10);
+    uint32_t *queue = (uint32_t *)(rows + g.nrot);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const unsigned lt = (1u << lane) - 1u;
+    uint32_t *wq = queue + warp * kPairQueue;
+    const int nh = g.nhkl, P = g.nrot * g.nhkl;
+    for (int64_t t = blockIdx.x; t < n; t += gridDim.x) {
+        __syncthreads();  // the previous trial's tables are no longer read
+        if (tid == 0) sub_matrix(g, b.U + 9 * t, sub);
+        const double *vp = b.vpos + 3 * t;
+        for (int iw = tid; iw < g.nrot; iw += kPairThreads) rows[iw] = omega_row(g, b.rot_cs[iw], vp);
+        __syncthreads();
+        for (int ih = tid; ih < nh; ih += kPairThreads) {
+            const double h = b.hkl[3 * ih], k = b.hkl[3 * ih + 1], l = b.hkl[3 * ih + 2];
+            const double x = sub[0] * h + sub[1] * k + sub[2] * l;
+            const double y = sub[3] * h + sub[4] * k + sub[5] * l;
+            const double z = sub[6] * h + sub[7] * k + sub[8] * l;
+            gws[ih] = make_double4(x, y, z, sqrt(x * x + y * y + z * z));
+        }
+        __syncthreads();
+        int qn = 0;
+        auto drain = [&](int take) {
+            const bool valid = lane < take;
+            const uint32_t it = valid ? wq[qn + lane] : 0u;
+            __syncwarp();
+            if (valid) {
+                const int iw = (int)(it >> 8), ih = (int)(it & 255u);
+                pair_item<CodeT>(g, b, si, t, rows[iw], gws[ih], iw, ih, out, cap, count);
+            }
+            __syncwarp();
+        };
+        for (int base = warp * 32; base < P; base += kPairThreads) {
+            const int p = base + lane;
+            bool pass = false;
+            uint32_t item = 0;
+            if (p < P) {
+                const int iw = p / nh, ih = p - iw * nh;
+                const OmegaRow &r = rows[iw];
+                const double4 gv = gws[ih];
+                // cos(beta) and 2 d sin(theta) as landing_fp64 forms them, tested with a margin
+                const double Gtx = r.c * gv.x - r.s * gv.y, Gty = r.s * gv.x + r.c * gv.y;
+                const double x = (r.kx * Gtx + r.ky * Gty + r.kz * gv.z) / gv.w;
+                const double lam = 2.0 * (2.0 * CUDART_PI / gv.w) * (-x);
+                pass = x < 1e-9 && x > g.cbmax - 1e-9 && lam > g.lmin * (1.0 - 1e-9) &&
+                       lam < g.lmax * (1.0 + 1e-9);
+                item = ((uint32_t)iw << 8) | (uint32_t)ih;
+            }
+            const unsigned bm = __ballot_sync(kFull, pass);
+            if (pass) wq[qn + __popc(bm & lt)] = item;
+            qn += __popc(bm);
+            __syncwarp();
+            if (qn >= 32) {
+                qn -= 32;
+                drain(32);
+            }
+        }
+        if (qn > 0) {
+            const int take = qn;
+            qn = 0;
+            drain(take);
         }
     }
 }
@@ -1134,11 +1203,19 @@ cudaError_t launch_refine_list(const Geo &g, const ScoreBufs &b, const Work &w, 
 cudaError_t launch_pair(const Geo &g, const ScoreBufs &b, int64_t n, const SpotIndex &si, PairRec *out, int64_t cap,
                         unsigned long long *count, int num_sms, cudaStream_t s) {
     if (n <= 0) return cudaSuccess;
-    const int grid = (int)(n < (int64_t)num_sms * 16 ? n : (int64_t)num_sms * 16);
+    const size_t smem = pair_smem_bytes(g.nrot, g.nhkl);
+    const void *fn = g.code_bits <= 16 ? (const void *)pair_kernel<uint16_t> : (const void *)pair_kernel<uint32_t>;
+    cudaError_t e = allow_smem(fn, smem);
+    if (e != cudaSuccess) return e;
+    int per_sm = 0;  // CTAs of kPairThreads (occupancy_for counts kThreads-thread CTAs)
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kPairThreads, smem);
+    if (e != cudaSuccess) return e;
+    const int64_t resident = (int64_t)num_sms * (per_sm > 0 ? per_sm : 1);
+    const int grid = (int)(n < resident ? n : resident);
     if (g.code_bits <= 16)
-        pair_kernel<uint16_t><<<grid, 128, 0, s>>>(g, b, n, si, out, cap, count);
+        pair_kernel<uint16_t><<<grid, kPairThreads, smem, s>>>(g, b, n, si, out, cap, count);
     else
-        pair_kernel<uint32_t><<<grid, 128, 0, s>>>(g, b, n, si, out, cap, count);
+        pair_kernel<uint32_t><<<grid, kPairThreads, smem, s>>>(g, b, n, si, out, cap, count);
     return cudaGetLastError();
 }
 
