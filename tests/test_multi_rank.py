@@ -56,3 +56,27 @@ def test_single_process_time_is_identity():
     import bench
     assert bench.max_over_ranks(3.5) == 3.5
     assert bench.seed_range(2, 0, 1, 64) == (128, 192)
+
+
+def test_workload_note_says_whether_the_read_array_exceeds_l2():
+    """The timing rule for the bench line: inputs larger than L2 between timed steps, or the
+    line says they are not.  The Al seeding scan reads a 189 MB hit mask (and 1.51 GB of 8-bit
+    codes with the four columns); the Fe mask (24 MB) stays in L2 and the note says so."""
+    import sys
+    from types import SimpleNamespace as NS
+
+    import numpy as np
+    sys.path.insert(0, ROOT)
+    import bench
+
+    def sample(nrot, n, sg, ngr, nhkl):
+        return NS(geom=NS(nrot=nrot, detysize=n, detzsize=n), space_group=sg, grain_q=[0] * ngr, nhkl=nhkl,
+                  grain_id=np.ones(4))
+
+    al = sample(361, 2048, 225, 400, 64)
+    fe = sample(181, 1024, 229, 6, 86)
+    assert bench.workload_desc(al, 64)["l2"].startswith("inputs larger than L2 (126 MB): the packed hit mask (189 MB")
+    assert "(1.51 GB)" in bench.workload_desc(al, 64, "full")["l2"]
+    assert "fits in L2" in bench.workload_desc(fe, 64)["l2"]
+    assert bench.workload_desc(fe, 64, "full")["l2"].startswith("inputs larger than L2")
+    assert bench.workload_desc(al, 64)["trials_per_step_per_gpu"] == 64 * bench.N_ORIENT
