@@ -8,7 +8,8 @@ tilts and a beam stop over the detector centre.  Odd seeds use a distance map wi
 distinct values (8-bit codes), even seeds one with millions (32-bit codes and the radix refine
 of the median).  On the per-trial kernel, the CTA sweep and the warp scan, with and without the median,
 every trial without a tight edge reflection equals the oracle in every column it returns.  Seven of
-the geometries also run the grow and compete entries against the oracle's grow and compete."""
+the geometries also run the grow and compete entries against the oracle's grow and compete, and
+six run the spot pairing against the oracle's forward_comp_pair_spots."""
 import numpy as np
 import pytest
 
@@ -155,3 +156,56 @@ def test_random_geometry_grow_and_compete_match_oracle(seed, nhkl, extreme):
             np.testing.assert_allclose(gc[c_ok, 7], c_ref[c_ok, 7], rtol=1e-6, err_msg=msg + " compete median")
             assert gc[7, 4] == 0 and gc[7, 7] == 2000
         ctx.set_path(0)
+
+
+def _pairing_spots(rng, geom, trials, S9, B9, hk, dmap, rot, R9, p):
+    """Measured spots of a random geometry: the landings of the given (U, pos) trials with 0.4 px
+    centroid noise and random areas, plus 10 spurious spots per projection."""
+    per = [[] for _ in range(geom.nrot)]
+    for U, pos in trials:
+        rec, _ = O.landings(U, pos, S9, B9, hk, dmap, rot, R9, p)
+        for j in np.nonzero(rec["sel"])[0]:
+            per[rec["iw"][j]].append((rec["u"][j] + rng.normal(0, 0.4), rec["v"][j] + rng.normal(0, 0.4),
+                                      rng.uniform(4, 40)))
+    for iw in range(geom.nrot):
+        for _ in range(10):
+            per[iw].append((rng.uniform(1, geom.detysize), rng.uniform(1, geom.detzsize), 10.0))
+    return [np.array(a, np.float64).reshape(-1, 3) for a in per]
+
+
+@pytest.mark.parametrize("seed,nhkl,extreme", [CASES[i] for i in (0, 1, 4, 5, 10, 12)])
+def test_random_geometry_pairing_matches_oracle(seed, nhkl, extreme):
+    """grc_pair_spots on random geometries against the oracle's forward_comp_pair_spots.m: six
+    trials, three of them with their own noisy spots in the list; every trial whose hits carry
+    no edge reflection has the oracle's pair list (projection, reflection, spot, pixel, centroid,
+    area and distance exact, energy to 1e-12)."""
+    from grainrecon_b200 import seeding as S
+    from oracle import seed_oracle as SO
+    geom, dmap, (S9, B9, hk, rot, R9, p), pos, q = _case(seed, nhkl, extreme)
+    rng = np.random.default_rng(seed + 2000)
+    tp = pos[[0, 1, 0, 1, 0, 1]].astype(np.float64)
+    tq = q[:6].astype(np.float64)
+    Us = [G.quat_to_u(x) for x in tq]
+    spots = _pairing_spots(rng, geom, [(Us[t], tp[t]) for t in range(3)], S9, B9, hk, dmap, rot, R9, p)
+    off = np.concatenate([[0], np.cumsum([len(a) for a in spots])])
+    sc = SO.Scene(S9, B9, hk, rot, R9, p, dmap)
+    with Context(0) as ctx:
+        ctx.set_geometry(S9, B9, hk, rot, R9, p)
+        ctx.upload_masks(dmap, geom.detzsize, geom.detysize, geom.nrot)
+        pairs = S.pair_spots(ctx, tp, tq, spots, geom.nrot)
+    n_clean = n_pairs = 0
+    for t in range(len(tp)):
+        ref, edges = SO.pair_spots(sc, Us[t], tp[t], spots)
+        if edges:
+            continue
+        n_clean += 1
+        got = pairs[pairs["trial"] == t]
+        assert len(got) == len(ref), (seed, t, len(got), len(ref))
+        n_pairs += len(ref)
+        for a, r in zip(got, ref):
+            iw, ih, j, dety, detz, ey, ez, area, ekev, dis = r
+            assert (a["iw"], a["ih"], a["spot"]) == (iw, ih, off[iw] + j)
+            assert (a["dety"], a["detz"], a["exp_y"], a["exp_z"], a["area"]) == (dety, detz, ey, ez, area)
+            assert a["dis"] == np.float32(dis)
+            np.testing.assert_allclose(a["energy_kev"], ekev, rtol=1e-12)
+    assert n_clean >= 4 and n_pairs > 0
