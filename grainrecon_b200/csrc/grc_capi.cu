@@ -1568,12 +1568,18 @@ int grc_pair_spots(grc_ctx *ctx, const double *d_pos, const double *d_q, int64_t
         TRY(ensure(ctx, ctx->pr_ids2, sizeof(int32_t) * m));
         CU(grc::launch_pair_keys((const grc::PairRec *)ctx->pr_raw.p, m, g.nrot, g.nhkl, (int64_t *)ctx->pr_keys.p,
                                  (int32_t *)ctx->pr_ids.p, s));
+        // keys (trial * nrot + iw) * nhkl + ih are below n * nrot * nhkl: sort only those bits
+        const uint64_t key_end = (uint64_t)n * (uint64_t)g.nrot * (uint64_t)g.nhkl;
+        int key_bits = 1;
+        while (key_bits < 63 && (uint64_t(1) << key_bits) < key_end) ++key_bits;
         size_t tb = 0;
         CU(cub::DeviceRadixSort::SortPairs(nullptr, tb, (const int64_t *)ctx->pr_keys.p, (int64_t *)ctx->pr_keys2.p,
-                                           (const int32_t *)ctx->pr_ids.p, (int32_t *)ctx->pr_ids2.p, m, 0, 64, s));
+                                           (const int32_t *)ctx->pr_ids.p, (int32_t *)ctx->pr_ids2.p, m, 0, key_bits,
+                                           s));
         TRY(ensure(ctx, ctx->tmp, tb));
         CU(cub::DeviceRadixSort::SortPairs(ctx->tmp.p, tb, (const int64_t *)ctx->pr_keys.p, (int64_t *)ctx->pr_keys2.p,
-                                           (const int32_t *)ctx->pr_ids.p, (int32_t *)ctx->pr_ids2.p, m, 0, 64, s));
+                                           (const int32_t *)ctx->pr_ids.p, (int32_t *)ctx->pr_ids2.p, m, 0, key_bits,
+                                           s));
         CU(grc::launch_pair_gather((const grc::PairRec *)ctx->pr_raw.p, (const int32_t *)ctx->pr_ids2.p, m,
                                    (grc::PairRec *)d_pairs, s));
         CU(cudaStreamSynchronize(s));
