@@ -977,27 +977,34 @@ __device__ __forceinline__ void pair_item(const Geo &g, const ScoreBufs &b, cons
     const int64_t idx = landing_fp64(g, r, gv.x, gv.y, gv.z, iw, &lam);
     if (idx < 0) return;
     const uint32_t code = (uint32_t)codes[idx];
-    if (code >= g.n_hit) return;
     const int64_t in_plane = idx - (int64_t)iw * g.plane;
     const int dety = (int)(in_plane / g.detzsize) + 1, detz = (int)(in_plane % g.detzsize) + 1;
     const int cy0 = max(0, (dety - 16) / si.cell_px), cy1 = min(si.ncy - 1, (dety + 14) / si.cell_px);
     const int cz0 = max(0, (detz - 16) / si.cell_px), cz1 = min(si.ncz - 1, (detz + 14) / si.cell_px);
+    // cells cz0..cz1 of one cell row are consecutive in the index, so a row's spots are one range
+    // of cell_ids; the first row's bounds are read before the hit test, beside the code
+    const int64_t row0 = ((int64_t)iw * si.ncy + cy0) * si.ncz;
+    int64_t q0 = si.cell_off[row0 + cz0], q1 = si.cell_off[row0 + cz1 + 1];
+    if (code >= g.n_hit) return;
     int best = -1;
     double bd = 0.0;
-    for (int cy = cy0; cy <= cy1; ++cy)
-        for (int cz = cz0; cz <= cz1; ++cz) {
-            const int64_t cell = ((int64_t)iw * si.ncy + cy) * si.ncz + cz;
-            for (int64_t q = si.cell_off[cell]; q < si.cell_off[cell + 1]; ++q) {
-                const int id = si.cell_ids[q];
-                const double dy = __dsub_rn(si.yza[3 * id], (double)dety);
-                const double dz = __dsub_rn(si.yza[3 * id + 1], (double)detz);
-                const double d = sqrt(__dadd_rn(__dmul_rn(dy, dy), __dmul_rn(dz, dz)));
-                if (best < 0 || d < bd || (d == bd && id < best)) {
-                    best = id;
-                    bd = d;
-                }
+    for (int cy = cy0; cy <= cy1; ++cy) {
+        if (cy > cy0) {
+            const int64_t row = ((int64_t)iw * si.ncy + cy) * si.ncz;
+            q0 = si.cell_off[row + cz0];
+            q1 = si.cell_off[row + cz1 + 1];
+        }
+        for (int64_t q = q0; q < q1; ++q) {
+            const int id = si.cell_ids[q];
+            const double dy = __dsub_rn(si.yza[3 * id], (double)dety);
+            const double dz = __dsub_rn(si.yza[3 * id + 1], (double)detz);
+            const double d = sqrt(__dadd_rn(__dmul_rn(dy, dy), __dmul_rn(dz, dz)));
+            if (best < 0 || d < bd || (d == bd && id < best)) {
+                best = id;
+                bd = d;
             }
         }
+    }
     if (best < 0 || !(bd < fmin(sqrt(si.yza[3 * best + 2]), 15.0))) return;
     const unsigned long long slot = atomicAdd(count, 1ull);
     if ((int64_t)slot < cap) {
